@@ -1,0 +1,195 @@
+/*
+ * mhd_b200.h -- C ABI of the B200 (sm_100a) SPMHD particle-update library.
+ *
+ * The library replaces the CUDA kernels that PySPH generates at run time for
+ * the reference's equation groups (src/scheme.py:66-81) and its integrator
+ * step (src/integrator.py), plus the PySPH neighbour search
+ * (src/application.py:63-78, periodic_mode="minimum_image") that feeds them.
+ *
+ * Conventions
+ *  - Every function returns MHD_OK (0) or a negative MHD_ERR_* code; no C++
+ *    exception crosses the ABI.  mhd_last_error() gives a message.
+ *  - Particle memory belongs to the caller (one device array per reference
+ *    property name, structure of arrays).  A context owns only workspace.
+ *  - All calls are ordered on the CUDA stream passed in (cudaStream_t as
+ *    void*; NULL = legacy default stream).  One host thread per context.
+ *  - Device-side failures (non-finite dt, neighbour capacity) are recorded in
+ *    a device status word and reported at the next synchronising call.
+ */
+#ifndef MHD_B200_H
+#define MHD_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MHD_ABI_VERSION 1
+
+#define MHD_OK 0
+#define MHD_ERR_INVALID (-1)        /* bad argument, null required pointer, n > n_max */
+#define MHD_ERR_CUDA (-2)           /* a CUDA runtime call failed */
+#define MHD_ERR_NOT_CONVERGED (-3)  /* density iteration hit max_iter with unconverged particles */
+#define MHD_ERR_NONFINITE (-4)      /* NaN/Inf met in the timestep reduction */
+#define MHD_ERR_CAPACITY (-5)       /* cell grid larger than the supported maximum */
+#define MHD_ERR_NO_DEVICE (-6)      /* no CUDA device, or not sm_100 */
+
+/* Kernel ids: the reference's kernel map, src/scheme.py:48-56. */
+#define MHD_KERNEL_CUBIC 0
+#define MHD_KERNEL_QUINTIC 1
+#define MHD_KERNEL_WENDLAND_C2 2
+#define MHD_KERNEL_WENDLAND_C4 3
+#define MHD_KERNEL_WENDLAND_C6 4
+#define MHD_KERNEL_GAUSSIAN 5
+#define MHD_KERNEL_SUPER_GAUSSIAN 6
+
+/* Pair-sum precision of the force and density passes. */
+#define MHD_PRECISION_FP64 0
+#define MHD_PRECISION_FP32 1
+
+/*
+ * Scheme parameters.  Fields map to the reference's configuration
+ * (src/config.py:8-57) and MHDScheme (src/scheme.py:32-44); dim, alpha_min,
+ * alpha_max and precision are extensions whose defaults (3, 0, 1, FP64)
+ * reproduce the reference.
+ */
+typedef struct MhdParams {
+  int32_t dim;             /* 2 or 3 (reference: always 3, src/scheme.py:57) */
+  int32_t kernel;          /* MHD_KERNEL_* */
+  int32_t iterate;         /* numerics.density == "iterate" (src/scheme.py:69) */
+  int32_t min_iter;        /* 2 (src/scheme.py:71) */
+  int32_t max_iter;        /* 250, MAX_DENSITY_ITERATIONS (src/scheme.py:28) */
+  int32_t precision;       /* MHD_PRECISION_* */
+  int32_t periodic[3];     /* periodic_mode "minimum_image" per axis */
+  int32_t reserved;
+  double hfact;            /* numerics.hfact, the k of DensityIteration */
+  double gamma;            /* physics.gamma */
+  double mu0;              /* physics.mu0 */
+  double av;               /* physics.artificial_viscosity */
+  double ac;               /* physics.artificial_thermal_conductivity */
+  double ar;               /* physics.artificial_magnetic_dissipation */
+  double clean_speed;      /* numerics.cleaning_speed_factor */
+  double clean_damp;       /* numerics.cleaning_damping_factor */
+  double timestep_factor;  /* solver.timestep_factor */
+  double alpha_min;        /* Cullen-Dehnen clip, reference literal 0 (src/equations.py:428) */
+  double alpha_max;        /* reference literal 1 */
+  double tf;               /* solver.tf: the last step is clipped to reach it */
+  double lo[3];            /* periodic box (src/application.py:66-78) */
+  double hi[3];
+} MhdParams;
+
+/*
+ * Particle state: one device pointer per reference property name
+ * (src/particles.py).  The X-macro lists the fields in layout order; all are
+ * double except itype (int32).  "Required" fields must be non-null for the
+ * step and RHS calls; "optional" ones are written only when non-null.
+ */
+#define MHD_STATE_REQUIRED(X)                                                                       \
+  X(x) X(y) X(z) X(gid) X(u) X(v) X(w) X(rho) X(rho_sum) X(h) X(m) X(cs) X(p) X(e) X(au) X(av) X(aw) \
+  X(ae) X(ah) X(upred) X(vpred) X(wpred) X(epred) X(h0) X(div) X(dt_cfl) X(dt_adapt) X(omega)       \
+  X(converged) X(alpha1) X(Bx) X(By) X(Bz) X(Bevolx) X(Bevoly) X(Bevolz) X(psi) X(Bevolxpred)        \
+  X(Bevolypred) X(Bevolzpred) X(psipred) X(Bxpred) X(Bypred) X(Bzpred) X(aBevolx) X(aBevoly)         \
+  X(aBevolz) X(apsi) X(divBsymm) X(divBdiff) X(div_for_psi) X(alphaloc)
+#define MHD_STATE_OPTIONAL(X)                                                                       \
+  X(x0) X(y0) X(z0) X(u0) X(v0) X(w0) X(e0) X(alpha10) X(Bevolx0) X(Bevoly0) X(Bevolz0) X(psi0)      \
+  X(xilimiter) X(divvdt) X(arho) X(grhox) X(grhoy) X(grhoz) X(dwdh)                                 \
+  X(cd_rxx) X(cd_rxy) X(cd_rxz) X(cd_ryy) X(cd_ryz) X(cd_rzz) X(cd_vxx) X(cd_vxy) X(cd_vxz)           \
+  X(cd_vyx) X(cd_vyy) X(cd_vyz) X(cd_vzx) X(cd_vzy) X(cd_vzz) X(cd_axx) X(cd_axy) X(cd_axz)           \
+  X(cd_ayx) X(cd_ayy) X(cd_ayz) X(cd_azx) X(cd_azy) X(cd_azz) X(dvdx_xx) X(dvdx_xy) X(dvdx_xz)        \
+  X(dvdx_yx) X(dvdx_yy) X(dvdx_yz) X(dvdx_zx) X(dvdx_zy) X(dvdx_zz)
+
+typedef struct MhdState {
+#define MHD_FIELD_(n) double* n;
+  MHD_STATE_REQUIRED(MHD_FIELD_)
+  MHD_STATE_OPTIONAL(MHD_FIELD_)
+#undef MHD_FIELD_
+  int32_t* itype; /* 1 = integrated fluid; other values are frozen (src/integrator.py:39,69) */
+} MhdState;
+
+/* Per-call statistics of a right-hand side (host memory). */
+typedef struct MhdRhsStats {
+  int32_t density_passes;   /* passes of the iterated DensityIteration group */
+  int32_t grid_rebuilds;    /* neighbour grids built (1 + re-plans when h outgrew the cells) */
+  int64_t n_unconverged;    /* particles unconverged when the group stopped */
+  int64_t n_cells;          /* cells of the last grid */
+} MhdRhsStats;
+
+/* ---- library and context ---- */
+
+int mhd_abi_version(void);
+/* Names of the MhdState fields in layout order (for binding checks). */
+int mhd_state_field_count(void);
+const char* mhd_state_field_name(int32_t i);
+/* Names of the fields mhd_cells_build permutes from src into dst (the
+   caller needs distinct src/dst buffers for exactly these, itype last). */
+int mhd_sorted_field_count(void);
+const char* mhd_sorted_field_name(int32_t i);
+
+/* Creates a context for up to n_max particles on the current CUDA device.
+   Replaces PySPH's solver set-up of the generated kernels
+   (MHDScheme.configure_solver, src/scheme.py:46-59). */
+int mhd_ctx_create(const MhdParams* params, int64_t n_max, void** ctx);
+int mhd_ctx_destroy(void* ctx);
+int mhd_ctx_set_params(void* ctx, const MhdParams* params);
+const char* mhd_last_error(void* ctx);
+/* Number of this library's kernels launched through the context so far. */
+int64_t mhd_launch_count(void* ctx);
+
+/* ---- neighbour search ----
+   Sort the particles of `src` by cell of the neighbour grid (Morton-free
+   linear cell order, stable LSD radix sort + prefix scan) and write the
+   permuted persistent fields into `dst`: PySPH's NNPS update plus
+   Solver.reorder_particles (src/solver.py:30-32).  `src` and `dst` may not
+   alias.  The grid is kept in the context for the passes that follow. */
+int mhd_cells_build(void* ctx, const MhdState* src, MhdState* dst, int64_t n, void* stream);
+
+/* ---- equation groups (src/scheme.py:71-80) ----
+   G1, DensityIteration with its iterated Group (src/equations.py:14-94,
+   src/scheme.py:71); neighbours follow the current h in every pass. */
+int mhd_density_iterate(void* ctx, MhdState* s, int64_t n, MhdRhsStats* stats, void* stream);
+/* G2-G10 fused: SmoothingLengthRateFromDensityRelation, DensityFromSmoothingLength,
+   IdealGasEOS, CullenDehnenAlphaDiagnostics, StrainDiagnostics,
+   MagneticStateReconstruction, MHDAccelerations,
+   SmoothingLengthRateFromForceDivergence, MagneticStressAccelerations,
+   MagneticStateRates, EnergyLimiter, DivBCorrection, AdaptiveTimestep
+   (src/equations.py:97-624) as one neighbour pass with prologue/epilogue. */
+int mhd_force_pass(void* ctx, MhdState* s, int64_t n, void* stream);
+/* One full right-hand side on `src` (grid build into `dst`, G1..G10 on
+   `dst`): PySPH's Integrator.compute_accelerations. */
+int mhd_rhs(void* ctx, const MhdState* src, MhdState* dst, int64_t n, MhdRhsStats* stats, void* stream);
+
+/* ---- timestep (src/solver.py:40,61; src/application.py:134-147) ----
+   dt = min_i dt_adapt_i, clipped so that t + dt <= tf.  Writes dt to the
+   device scalar the corrector reads and to *dt_host (synchronising) when
+   dt_host is non-null. */
+int mhd_timestep(void* ctx, const MhdState* s, int64_t n, double t, double* dt_host, void* stream);
+
+/* Device clock of the fused loop: t = start of the current step, dt = its
+   size.  mhd_corrector_predictor with device dt advances it. */
+int mhd_clock_set(void* ctx, double t, double dt, void* stream);
+int mhd_clock_get(void* ctx, double* t, double* dt, void* stream); /* synchronising */
+
+/* ---- integrator (MHDStep, src/integrator.py:12-82) ----
+   The literal stages: every property the reference writes is written. */
+int mhd_step_initialize(void* ctx, MhdState* s, int64_t n, void* stream);
+int mhd_step_stage1(void* ctx, MhdState* s, int64_t n, double dt, void* stream);
+int mhd_step_stage2(void* ctx, MhdState* s, int64_t n, double dt, void* stream);
+/* Fused corrector-predictor: stage2 of the current step with dt_cur, then
+   initialize + stage1 of the next with dt_next, one pass over HBM.
+   mode: 1 = stage2 only, 2 = initialize+stage1 only, 3 = both.
+   A negative dt reads the value mhd_timestep left on the device.  The
+   x0..psi0 copies are not materialised (they are consumed in registers). */
+int mhd_corrector_predictor(void* ctx, MhdState* s, int64_t n, int32_t mode, double dt_cur, double dt_next,
+                            void* stream);
+
+/* One PEC step (PECIntegrator.one_timestep order: initialize, stage1, wrap,
+   RHS, stage2, wrap) on `src`; the result is in `dst` (particle order
+   changes with the neighbour sort).  dt < 0 uses the device dt. */
+int mhd_step(void* ctx, MhdState* src, MhdState* dst, int64_t n, double dt, MhdRhsStats* stats, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MHD_B200_H */

@@ -1,0 +1,299 @@
+// mhd_cells.cu -- neighbour grid for the SPMHD particle update (sm_100a).
+//
+// Replaces PySPH's NNPS update (src/application.py:63-78) and its
+// Solver.reorder_particles (src/solver.py:30-32,69-70): particles are
+// binned into a uniform grid whose cells are at least R*h_max wide, sorted
+// by linear cell index (x fastest) with a stable LSD radix sort, and the
+// persistent particle fields are gathered into the sorted order.  A prefix
+// table cell_start[ncells+1] then makes every x-row of three neighbouring
+// cells one contiguous index range.
+#include <cuda_runtime.h>
+#include <string.h>
+
+#include "mhd_common.cuh"
+#include "mhd_internal.h"
+
+namespace mhd {
+
+// ---------------------------------------------------------------- reductions
+// h_max over all particles and the bounding box of positions (for axes that
+// are not periodic).  Order-mapped integer atomics; sc->h_max_bits etc. must
+// be reset by the caller.
+__global__ void __launch_bounds__(256) k_reduce_hbox(int n, const double* __restrict__ x,
+                                                     const double* __restrict__ y, const double* __restrict__ z,
+                                                     const double* __restrict__ h, DevScalars* sc) {
+  double hm = 0.0;
+  double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  const double* pos[3] = {x, y, z};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double hv = h[i];
+    hm = hv > hm ? hv : hm;
+    if (!(hv > 0.0) || !isfinite(hv)) set_status(sc, MHD_ERR_NONFINITE);
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      const double v = pos[a][i];
+      lo[a] = fmin(lo[a], v);
+      hi[a] = fmax(hi[a], v);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    hm = fmax(hm, __shfl_xor_sync(0xffffffffu, hm, o));
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      lo[a] = fmin(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], o));
+      hi[a] = fmax(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], o));
+    }
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(&sc->h_max_bits, dbl_order(hm));
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      atomicMin(&sc->lo_bits[a], dbl_order(lo[a]));
+      atomicMax(&sc->hi_bits[a], dbl_order(hi[a]));
+    }
+  }
+}
+
+// --------------------------------------------------------------- cell keys
+template <int DIM>
+__global__ void __launch_bounds__(256) k_cell_keys(int n, Grid g, const double* __restrict__ x,
+                                                   const double* __restrict__ y, const double* __restrict__ z,
+                                                   uint32_t* __restrict__ keys, int32_t* __restrict__ vals) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int cx = cell_coord(g, 0, x[i]);
+  const int cy = cell_coord(g, 1, y[i]);
+  const int cz = DIM == 3 ? cell_coord(g, 2, z[i]) : 0;
+  keys[i] = (uint32_t)((cz * g.nc[1] + cy) * g.nc[0] + cx);
+  vals[i] = i;
+}
+
+// -------------------------------------------------------------- radix sort
+constexpr int RS_THREADS = 256;
+constexpr int RS_WARPS = RS_THREADS / 32;
+constexpr int RS_ITERS = 16;                    // per warp
+constexpr int RS_TILE = RS_THREADS * RS_ITERS;  // keys per block
+
+__global__ void __launch_bounds__(RS_THREADS) k_radix_hist(const uint32_t* __restrict__ keys, int n, int shift,
+                                                           uint32_t* __restrict__ hist, int nblocks) {
+  __shared__ uint32_t h[256];
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  const int base = blockIdx.x * RS_TILE;
+#pragma unroll 4
+  for (int it = 0; it < RS_ITERS; it++) {
+    const int idx = base + it * RS_THREADS + threadIdx.x;
+    if (idx < n) atomicAdd(&h[(keys[idx] >> shift) & 255u], 1u);
+  }
+  __syncthreads();
+  hist[threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
+}
+
+// Stable scatter: warp w owns the contiguous sub-tile [w*512, (w+1)*512) of
+// the block tile and walks it in order; equal digits inside one 32-key step
+// are ranked by lane (match_any), steps and warps in order, so the pass is
+// stable.
+__global__ void __launch_bounds__(RS_THREADS) k_radix_scatter(const uint32_t* __restrict__ kin,
+                                                              const int32_t* __restrict__ vin,
+                                                              uint32_t* __restrict__ kout, int32_t* __restrict__ vout,
+                                                              int n, int shift, const uint32_t* __restrict__ offs,
+                                                              int nblocks) {
+  __shared__ uint32_t wh[RS_WARPS][256];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int k = threadIdx.x; k < RS_WARPS * 256; k += RS_THREADS) (&wh[0][0])[k] = 0;
+  __syncthreads();
+  const int base = blockIdx.x * RS_TILE + warp * (RS_ITERS * 32);
+  const unsigned lt = (1u << lane) - 1u;
+  for (int it = 0; it < RS_ITERS; it++) {
+    const int idx = base + it * 32 + lane;
+    const bool valid = idx < n;
+    const uint32_t d = valid ? ((kin[idx] >> shift) & 255u) : 256u;
+    const unsigned peers = __match_any_sync(0xffffffffu, d);
+    if (valid && lane == __ffs(peers) - 1) wh[warp][d] += __popc(peers);
+  }
+  __syncthreads();
+  {
+    const int d = threadIdx.x;  // RS_THREADS == 256 digits
+    uint32_t run = offs[d * nblocks + blockIdx.x];
+#pragma unroll
+    for (int w = 0; w < RS_WARPS; w++) {
+      const uint32_t c = wh[w][d];
+      wh[w][d] = run;
+      run += c;
+    }
+  }
+  __syncthreads();
+  for (int it = 0; it < RS_ITERS; it++) {
+    const int idx = base + it * 32 + lane;
+    const bool valid = idx < n;
+    uint32_t key = 0;
+    int32_t val = 0;
+    if (valid) {
+      key = kin[idx];
+      val = vin[idx];
+    }
+    const uint32_t d = valid ? ((key >> shift) & 255u) : 256u;
+    const unsigned peers = __match_any_sync(0xffffffffu, d);
+    if (valid) {
+      const uint32_t pos = wh[warp][d] + __popc(peers & lt);
+      kout[pos] = key;
+      vout[pos] = val;
+    }
+    __syncwarp();
+    if (valid && lane == __ffs(peers) - 1) wh[warp][d] += __popc(peers);
+    __syncwarp();
+  }
+}
+
+// ------------------------------------------------------------ prefix scan
+constexpr int SCAN_THREADS = 256;
+constexpr int SCAN_ITEMS = 4;
+constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* total) {
+  __shared__ uint32_t warp_sums[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  uint32_t incl = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) warp_sums[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t s = lane < nwarps ? warp_sums[lane] : 0;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += t;
+    }
+    warp_sums[lane] = s;
+  }
+  __syncthreads();
+  const uint32_t warp_off = warp > 0 ? warp_sums[warp - 1] : 0;
+  *total = warp_sums[nwarps - 1];
+  __syncthreads();
+  return warp_off + incl - v;
+}
+
+// Exclusive scan of tiles of SCAN_TILE elements; tile totals to `sums`.
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_tiles(const uint32_t* in, uint32_t* out, int m,
+                                                             uint32_t* sums) {
+  const int base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
+  uint32_t v[SCAN_ITEMS], s = 0;
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; k++) {
+    v[k] = base + k < m ? in[base + k] : 0u;
+    s += v[k];
+  }
+  uint32_t total;
+  uint32_t run = block_exclusive_scan(s, &total);
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; k++) {
+    if (base + k < m) out[base + k] = run;
+    run += v[k];
+  }
+  if (threadIdx.x == 0 && sums) sums[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_add(uint32_t* __restrict__ out, int m,
+                                                           const uint32_t* __restrict__ sums) {
+  const int base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
+  const uint32_t add = sums[blockIdx.x];
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; k++)
+    if (base + k < m) out[base + k] += add;
+}
+
+// --------------------------------------------------------------- cell table
+// cell_start[c] = first sorted slot whose key >= c, for c in [0, ncells].
+__global__ void __launch_bounds__(256) k_cell_starts(int n, int ncells, const uint32_t* __restrict__ skeys,
+                                                     int* __restrict__ cell_start) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s > n) return;
+  const int kcur = s < n ? (int)skeys[s] : ncells;
+  const int kprev = s > 0 ? (int)skeys[s - 1] : -1;
+  for (int c = kprev + 1; c <= kcur; c++) cell_start[c] = s;
+}
+
+// ------------------------------------------------------------------ gather
+__global__ void __launch_bounds__(256) k_gather(int n, const int32_t* __restrict__ perm, GatherSet gs) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const int o = perm[s];
+  for (int f = 0; f < gs.nf; f++) gs.dst[f][s] = __ldg(gs.src[f] + o);
+  if (gs.isrc) gs.idst[s] = __ldg(gs.isrc + o);
+}
+
+// ------------------------------------------------------------- host driver
+static int ceil_div(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
+
+// Exclusive scan of m elements, in place allowed; `scratch` holds the tile
+// sums of every level (sized by scan_sums_needed).
+static void exclusive_scan(Ctx* c, const uint32_t* in, uint32_t* out, int m, uint32_t* scratch, cudaStream_t st) {
+  const int tiles = ceil_div(m, SCAN_TILE);
+  if (tiles <= 1) {
+    k_scan_tiles<<<1, SCAN_THREADS, 0, st>>>(in, out, m, nullptr);
+    c->launches++;
+    return;
+  }
+  k_scan_tiles<<<tiles, SCAN_THREADS, 0, st>>>(in, out, m, scratch);
+  exclusive_scan(c, scratch, scratch, tiles, scratch + tiles, st);
+  k_scan_add<<<tiles, SCAN_THREADS, 0, st>>>(out, m, scratch);
+  c->launches += 2;
+}
+
+int max_sort_blocks(int64_t n_max) { return ceil_div(n_max > 0 ? n_max : 1, RS_TILE); }
+int64_t scan_sums_needed(int64_t n_max) {
+  int64_t m = (int64_t)256 * max_sort_blocks(n_max), total = 0;
+  while (m > 1) {
+    m = ceil_div(m, SCAN_TILE);
+    total += m;
+  }
+  return total + 16;
+}
+
+void launch_reduce_hbox(Ctx* c, const MhdState* s, int n, cudaStream_t st) {
+  const int blocks = n > 0 ? (ceil_div(n, 256) < 1184 ? ceil_div(n, 256) : 1184) : 1;
+  k_reduce_hbox<<<blocks, 256, 0, st>>>(n, s->x, s->y, s->z, s->h, c->d_sc);
+  c->launches++;
+}
+
+// Sort the particles by cell of `c->grid`; leaves perm (sorted slot ->
+// source index) in c->perm and the cell table in c->cell_start.
+void launch_sort_cells(Ctx* c, const MhdState* s, int n, cudaStream_t st) {
+  const Grid& g = c->grid;
+  const int nb = ceil_div(n, 256);
+  if (n > 0) {
+    if (c->P.dim == 3)
+      k_cell_keys<3><<<nb, 256, 0, st>>>(n, g, s->x, s->y, s->z, c->keys[0], c->vals[0]);
+    else
+      k_cell_keys<2><<<nb, 256, 0, st>>>(n, g, s->x, s->y, s->z, c->keys[0], c->vals[0]);
+    c->launches++;
+  }
+  int bits = 1;
+  while ((1LL << bits) < (int64_t)g.ncells) bits++;
+  const int passes = (bits + 7) / 8;
+  const int sb = max_sort_blocks(n);
+  int cur = 0;
+  for (int p = 0; p < passes && n > 0; p++) {
+    const int shift = 8 * p;
+    k_radix_hist<<<sb, RS_THREADS, 0, st>>>(c->keys[cur], n, shift, c->hist, sb);
+    exclusive_scan(c, c->hist, c->hist, 256 * sb, c->scan_sums, st);
+    k_radix_scatter<<<sb, RS_THREADS, 0, st>>>(c->keys[cur], c->vals[cur], c->keys[cur ^ 1], c->vals[cur ^ 1], n,
+                                               shift, c->hist, sb);
+    c->launches += 2;
+    cur ^= 1;
+  }
+  c->sorted_keys = c->keys[cur];
+  c->perm = c->vals[cur];
+  k_cell_starts<<<ceil_div(n + 1, 256), 256, 0, st>>>(n, g.ncells, c->sorted_keys, c->cell_start);
+  c->launches++;
+}
+
+void launch_gather(Ctx* c, const GatherSet& gs, int n, cudaStream_t st) {
+  if (n <= 0) return;
+  k_gather<<<ceil_div(n, 256), 256, 0, st>>>(n, c->perm, gs);
+  c->launches++;
+}
+
+}  // namespace mhd

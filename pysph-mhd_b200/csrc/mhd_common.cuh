@@ -1,0 +1,259 @@
+// mhd_common.cuh -- device-side parameters, SPH kernels and neighbour-test
+// helpers shared by the sm_100a kernels of the SPMHD particle update.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+
+#include "mhd_b200.h"
+
+namespace mhd {
+
+constexpr double kDensityTolerance = 1.0e-4;          // src/equations.py:6
+constexpr double kCourantFactor = 0.3;                // src/equations.py:7
+constexpr double kForceFactor = 0.25;                 // src/equations.py:8
+constexpr double kPairDistanceEpsilon = 1.0e-12;      // src/equations.py:9
+constexpr double kInteractionDistanceEpsilon = 1.0e-8;  // src/equations.py:10
+constexpr double kFloatTiny = 2.2250738585072014e-308;  // src/equations.py:11
+constexpr double kMachineEps = 2.220446049250313e-16;   // src/equations.py:67
+constexpr double kBigNumber = 1.0e29;                 // src/equations.py:574
+
+// Uniform cell grid over the box; cells along x are contiguous in the sorted
+// particle order, so a row of neighbouring cells is one index range.
+struct Grid {
+  int nc[3];
+  int ncells;
+  double lo[3];
+  double inv_cs[3];
+  double cs[3];
+  double h_plan;  // every h must stay <= h_plan for the grid to be valid
+};
+
+// Everything a kernel needs, passed by value.
+struct DevParams {
+  int dim;
+  int kernel;
+  int iterate;
+  int min_iter;
+  int max_iter;
+  int periodic[3];
+  double L[3];
+  double half[3];
+  double lo[3];
+  double hi[3];
+  double R;  // kernel radius scale
+  double hfact, gamma, gamma1, mu0, inv_mu0, av, ac, ar, clean_speed, clean_damp, clean_active;
+  double c_cour, c_force, alpha_min, alpha_max, tf;
+  double norm;  // kernel normalisation sigma_d
+};
+
+// Device-resident scalars of one context (status, reductions, step clock).
+struct DevScalars {
+  double dt;         // step size in use (stage2 of the current step)
+  double dt_next;    // next step size (min dt_adapt, clipped to tf)
+  double t;          // time at the start of the current step
+  double t_next;     // time at the start of the next step
+  unsigned long long dt_min_bits;  // atomicMin target (positive doubles order as integers)
+  unsigned long long h_max_bits;
+  unsigned long long lo_bits[3];   // bounding box (non-periodic axes), order-mapped
+  unsigned long long hi_bits[3];
+  int status;        // first device error, MHD_OK if none
+  int replan;        // an h outgrew the grid's h_plan during the density passes
+  int passes_done;   // density passes executed in the current group evaluation
+  unsigned int ticket;  // last-block counter of the dt reduction
+  int n_unconverged[256 + 8];  // per density pass
+};
+
+// ------------------------------------------------------------ kernels (SPH)
+// w(q) and dw/dq, unnormalised; forms and branch conditions follow PySPH's
+// pysph.base.kernels (restated): cubic spline (Monaghan), quintic spline
+// (Morris), Wendland C2/C4/C6, Gaussian, super-Gaussian.
+template <int K>
+__device__ __forceinline__ void w_dw(double q, int dim, double& w, double& dw) {
+  if constexpr (K == MHD_KERNEL_CUBIC) {
+    if (q > 2.0) {
+      w = 0.0; dw = 0.0;
+    } else if (q > 1.0) {
+      const double t = 2.0 - q;
+      w = 0.25 * t * t * t; dw = -0.75 * t * t;
+    } else {
+      w = 1.0 - 1.5 * q * q * (1.0 - 0.5 * q); dw = -3.0 * q * (1.0 - 0.75 * q);
+    }
+  } else if constexpr (K == MHD_KERNEL_QUINTIC) {
+    if (q > 3.0) { w = 0.0; dw = 0.0; return; }
+    const double t3 = 3.0 - q, t2 = 2.0 - q, t1 = 1.0 - q;
+    const double t3s = t3 * t3, t2s = t2 * t2, t1s = t1 * t1;
+    w = t3s * t3s * t3;
+    dw = -5.0 * t3s * t3s;
+    if (q <= 2.0) {
+      w -= 6.0 * t2s * t2s * t2;
+      dw += 30.0 * t2s * t2s;
+      if (q <= 1.0) {
+        w += 15.0 * t1s * t1s * t1;
+        dw -= 75.0 * t1s * t1s;
+      }
+    }
+  } else if constexpr (K == MHD_KERNEL_WENDLAND_C2) {
+    if (q >= 2.0) { w = 0.0; dw = 0.0; return; }
+    const double s = 1.0 - 0.5 * q, s3 = s * s * s;
+    w = s3 * s * (2.0 * q + 1.0); dw = -5.0 * q * s3;
+  } else if constexpr (K == MHD_KERNEL_WENDLAND_C4) {
+    if (q >= 2.0) { w = 0.0; dw = 0.0; return; }
+    const double s = 1.0 - 0.5 * q, s2 = s * s, s5 = s2 * s2 * s;
+    w = s5 * s * (35.0 / 12.0 * q * q + 3.0 * q + 1.0);
+    dw = -14.0 / 3.0 * q * (1.0 + 2.5 * q) * s5;
+  } else if constexpr (K == MHD_KERNEL_WENDLAND_C6) {
+    if (q >= 2.0) { w = 0.0; dw = 0.0; return; }
+    const double s = 1.0 - 0.5 * q, s2 = s * s, s4 = s2 * s2, s7 = s4 * s2 * s;
+    w = s7 * s * (4.0 * q * q * q + 6.25 * q * q + 4.0 * q + 1.0);
+    dw = -5.5 * q * (1.0 + 3.5 * q + 4.0 * q * q) * s7;
+  } else if constexpr (K == MHD_KERNEL_GAUSSIAN) {
+    if (q >= 3.0) { w = 0.0; dw = 0.0; return; }
+    const double e = exp(-q * q);
+    w = e; dw = -2.0 * q * e;
+  } else {
+    if (q >= 3.0) { w = 0.0; dw = 0.0; return; }
+    const double e = exp(-q * q), d2 = 0.5 * dim;
+    w = e * (d2 + 1.0 - q * q); dw = -2.0 * q * e * (d2 + 2.0 - q * q);
+  }
+}
+
+template <int K>
+__host__ __device__ constexpr double radius_scale() {
+  return (K == MHD_KERNEL_QUINTIC || K == MHD_KERNEL_GAUSSIAN || K == MHD_KERNEL_SUPER_GAUSSIAN) ? 3.0 : 2.0;
+}
+
+inline double radius_scale_of(int k) {
+  return (k == MHD_KERNEL_QUINTIC || k == MHD_KERNEL_GAUSSIAN || k == MHD_KERNEL_SUPER_GAUSSIAN) ? 3.0 : 2.0;
+}
+
+double kernel_norm(int kernel, int dim);  // host, mhd_abi.cu
+
+template <int DIM>
+__device__ __forceinline__ double pow_dim(double a) {
+  if constexpr (DIM == 2) return a * a;
+  else return a * a * a;
+}
+
+// sigma_d / h^d
+template <int DIM>
+__device__ __forceinline__ double hfac(double norm, double h1) {
+  return norm * pow_dim<DIM>(h1);
+}
+
+// Minimum-image displacement along one periodic axis.
+__device__ __forceinline__ double min_image(double d, double L, double half, int periodic) {
+  if (periodic) {
+    if (d > half) d = d - L;
+    if (d < -half) d = d + L;
+  }
+  return d;
+}
+
+// Squared distance evaluated without FMA contraction, in the oracle's order
+// ((dx*dx + dy*dy) + dz*dz), so neighbour sets are bit-identical to it.
+__device__ __forceinline__ double r2_exact(double dx, double dy, double dz) {
+  return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+}
+
+// (R*h)^2 without contraction.
+__device__ __forceinline__ double rh2_exact(double R, double h) {
+  const double rh = __dmul_rn(R, h);
+  return __dmul_rn(rh, rh);
+}
+
+__device__ __forceinline__ unsigned long long dbl_order(double v) {
+  // Monotone map of doubles to unsigned integers.
+  unsigned long long b = __double_as_longlong(v);
+  return (b & 0x8000000000000000ULL) ? ~b : (b | 0x8000000000000000ULL);
+}
+__host__ __device__ inline double dbl_unorder(unsigned long long b) {
+  unsigned long long v = (b & 0x8000000000000000ULL) ? (b & 0x7fffffffffffffffULL) : ~b;
+  double d;
+  memcpy(&d, &v, sizeof d);
+  return d;
+}
+
+__device__ __forceinline__ void set_status(DevScalars* sc, int code) { atomicCAS(&sc->status, MHD_OK, code); }
+
+// Cell coordinate of a position along axis a.
+__device__ __forceinline__ int cell_coord(const Grid& g, int a, double x) {
+  int c = (int)floor((x - g.lo[a]) * g.inv_cs[a]);
+  c = c < 0 ? 0 : c;
+  c = c >= g.nc[a] ? g.nc[a] - 1 : c;
+  return c;
+}
+
+// Up to two index ranges covering the x-row of cells (cx-1..cx+1) at (cy, cz).
+struct RowRanges {
+  int b0, e0, b1, e1;
+};
+
+__device__ __forceinline__ RowRanges row_ranges(const Grid& g, const int* __restrict__ cell_start, int row, int cx,
+                                                int periodic_x) {
+  RowRanges r;
+  const int nx = g.nc[0];
+  const int base = row * nx;
+  r.b1 = 0;
+  r.e1 = 0;
+  if (nx < 3) {
+    r.b0 = cell_start[base];
+    r.e0 = cell_start[base + nx];
+    return r;
+  }
+  int lo = cx - 1, hi = cx + 1;
+  if (lo < 0) {
+    if (periodic_x) {
+      r.b1 = cell_start[base + nx - 1];
+      r.e1 = cell_start[base + nx];
+    }
+    lo = 0;
+  }
+  if (hi >= nx) {
+    if (periodic_x) {
+      r.b1 = cell_start[base];
+      r.e1 = cell_start[base + 1];
+    }
+    hi = nx - 1;
+  }
+  r.b0 = cell_start[base + lo];
+  r.e0 = cell_start[base + hi + 1];
+  return r;
+}
+
+}  // namespace mhd
+
+namespace mhd {
+
+// Visits every particle index j in the 3^DIM cells around (xi, yi, zi):
+// per (y, z) row one or two contiguous ranges of the cell-sorted order.
+template <int DIM, class F>
+__device__ __forceinline__ void for_each_candidate(const Grid& G, const DevParams& P, const int* __restrict__ cell_start,
+                                                   double xi, double yi, double zi, F&& f) {
+  const int cx = cell_coord(G, 0, xi);
+  const int cy = cell_coord(G, 1, yi);
+  const int cz = DIM == 3 ? cell_coord(G, 2, zi) : 0;
+  const int ny = G.nc[1], nz = G.nc[2];
+  const int zlo = (DIM == 3 && nz > 1) ? -1 : 0, zhi = (DIM == 3 && nz > 1) ? 1 : 0;
+  const int ylo = ny > 1 ? -1 : 0, yhi = ny > 1 ? 1 : 0;
+  for (int oz = zlo; oz <= zhi; oz++) {
+    int zc = cz + oz;
+    if (zc < 0 || zc >= nz) {
+      if (!P.periodic[2]) continue;
+      zc = zc < 0 ? zc + nz : zc - nz;
+    }
+    for (int oy = ylo; oy <= yhi; oy++) {
+      int yc = cy + oy;
+      if (yc < 0 || yc >= ny) {
+        if (!P.periodic[1]) continue;
+        yc = yc < 0 ? yc + ny : yc - ny;
+      }
+      const RowRanges r = row_ranges(G, cell_start, zc * ny + yc, cx, P.periodic[0]);
+      for (int j = r.b0; j < r.e0; j++) f(j);
+      for (int j = r.b1; j < r.e1; j++) f(j);
+    }
+  }
+}
+
+}  // namespace mhd

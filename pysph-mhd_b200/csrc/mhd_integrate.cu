@@ -1,0 +1,277 @@
+// mhd_integrate.cu -- MHDStep stages, fused corrector-predictor and the
+// FP64 timestep reduction (sm_100a).
+//
+// k_stage_initialize / k_stage1 / k_stage2 restate MHDStep.initialize,
+// stage1 and stage2 (src/integrator.py:12-82) field for field; the periodic
+// wrap of PySPH's update_domain follows stage1 in the same kernel.
+// k_corrector_predictor fuses stage2 of step n with initialize + stage1 of
+// step n+1, so the integrator reads and writes each field once per step.
+// k_dt_reduce computes min(dt_adapt) (src/equations.py:570-585 with the
+// adaptive rule of src/application.py:134-147) and clips to tf.
+#include <cuda_runtime.h>
+
+#include "mhd_common.cuh"
+#include "mhd_internal.h"
+
+namespace mhd {
+
+__device__ __forceinline__ double wrap_axis(double v, double lo, double hi, double L) {
+  if (v < lo) v = v + L;
+  if (v > hi) v = v - L;
+  return v;
+}
+
+__device__ __forceinline__ void wrap_position(const DevParams& P, double& x, double& y, double& z) {
+  if (P.periodic[0]) x = wrap_axis(x, P.lo[0], P.hi[0], P.L[0]);
+  if (P.periodic[1]) y = wrap_axis(y, P.lo[1], P.hi[1], P.L[1]);
+  if (P.dim == 3 && P.periodic[2]) z = wrap_axis(z, P.lo[2], P.hi[2], P.L[2]);
+}
+
+// MHDStep.initialize (src/integrator.py:12-35)
+__global__ void __launch_bounds__(256) k_stage_initialize(int n, MhdState s) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  s.x0[i] = s.x[i];
+  s.y0[i] = s.y[i];
+  s.z0[i] = s.z[i];
+  s.u0[i] = s.u[i];
+  s.v0[i] = s.v[i];
+  s.w0[i] = s.w[i];
+  s.upred[i] = s.u[i];
+  s.vpred[i] = s.v[i];
+  s.wpred[i] = s.w[i];
+  s.e0[i] = s.e[i];
+  s.epred[i] = s.e[i];
+  s.h0[i] = s.h[i];
+  s.converged[i] = 0.0;
+  s.omega[i] = 1.0;
+  s.alpha10[i] = s.alpha1[i];
+  s.Bevolx0[i] = s.Bevolx[i];
+  s.Bevoly0[i] = s.Bevoly[i];
+  s.Bevolz0[i] = s.Bevolz[i];
+  s.psi0[i] = s.psi[i];
+  s.Bevolxpred[i] = s.Bevolx[i];
+  s.Bevolypred[i] = s.Bevoly[i];
+  s.Bevolzpred[i] = s.Bevolz[i];
+  s.psipred[i] = s.psi[i];
+}
+
+// MHDStep.stage1 (src/integrator.py:38-65) + periodic wrap.  In dim 2 the
+// z coordinate is not integrated (w is a field component only).
+__global__ void __launch_bounds__(256) k_stage1(int n, MhdState s, DevParams P, double dt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || s.itype[i] != 1) return;
+  const double dtb2 = 0.5 * dt;
+  const double u = s.u0[i] + dtb2 * s.au[i];
+  const double v = s.v0[i] + dtb2 * s.av[i];
+  const double w = s.w0[i] + dtb2 * s.aw[i];
+  s.u[i] = u;
+  s.v[i] = v;
+  s.w[i] = w;
+  s.upred[i] = s.u0[i] + dt * s.au[i];
+  s.vpred[i] = s.v0[i] + dt * s.av[i];
+  s.wpred[i] = s.w0[i] + dt * s.aw[i];
+  double x = s.x0[i] + dt * u, y = s.y0[i] + dt * v, z = P.dim == 3 ? s.z0[i] + dt * w : s.z[i];
+  wrap_position(P, x, y, z);
+  s.x[i] = x;
+  s.y[i] = y;
+  s.z[i] = z;
+  s.e[i] = s.e0[i] + dtb2 * s.ae[i];
+  s.epred[i] = s.e0[i] + dt * s.ae[i];
+  const double h = s.h0[i] + dt * s.ah[i];
+  s.h[i] = h;
+  const double decay = 0.1 * s.cs[i] / h;
+  const double a10 = s.alpha10[i], aloc = s.alphaloc[i];
+  s.alpha1[i] = a10 < aloc ? aloc : (a10 + dt * aloc * decay) / (1.0 + dt * decay);
+  s.Bevolx[i] = s.Bevolx0[i] + dtb2 * s.aBevolx[i];
+  s.Bevoly[i] = s.Bevoly0[i] + dtb2 * s.aBevoly[i];
+  s.Bevolz[i] = s.Bevolz0[i] + dtb2 * s.aBevolz[i];
+  s.psi[i] = s.psi0[i] + dtb2 * s.apsi[i];
+  s.Bevolxpred[i] = s.Bevolx0[i] + dt * s.aBevolx[i];
+  s.Bevolypred[i] = s.Bevoly0[i] + dt * s.aBevoly[i];
+  s.Bevolzpred[i] = s.Bevolz0[i] + dt * s.aBevolz[i];
+  s.psipred[i] = s.psi0[i] + dt * s.apsi[i];
+}
+
+// MHDStep.stage2 (src/integrator.py:68-82); positions do not change.
+__global__ void __launch_bounds__(256) k_stage2(int n, MhdState s, DevParams P, double dt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || s.itype[i] != 1) return;
+  const double dtb2 = 0.5 * dt;
+  s.u[i] += dtb2 * s.au[i];
+  s.v[i] += dtb2 * s.av[i];
+  s.w[i] += dtb2 * s.aw[i];
+  const double e = s.e[i] + dtb2 * s.ae[i];
+  s.e[i] = e;
+  const double rho = s.rho[i];
+  s.p[i] = P.gamma1 * rho * e;
+  const double bx = s.Bevolx[i] + dtb2 * s.aBevolx[i];
+  const double by = s.Bevoly[i] + dtb2 * s.aBevoly[i];
+  const double bz = s.Bevolz[i] + dtb2 * s.aBevolz[i];
+  s.Bevolx[i] = bx;
+  s.Bevoly[i] = by;
+  s.Bevolz[i] = bz;
+  s.psi[i] += dtb2 * s.apsi[i];
+  s.Bx[i] = bx * rho;
+  s.By[i] = by * rho;
+  s.Bz[i] = bz * rho;
+}
+
+// stage2(dt_cur) of this step, then initialize + stage1(dt_next) of the next.
+// mode bit 1: corrector; bit 2: predictor.  dev_dt: read both steps from sc.
+__global__ void __launch_bounds__(256) k_corrector_predictor(int n, MhdState s, DevParams P, int mode, double dt_cur,
+                                                             double dt_next, int dev_dt, const DevScalars* sc) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (dev_dt) {
+    dt_cur = sc->dt;
+    dt_next = sc->dt_next;
+  }
+  const bool fluid = s.itype[i] == 1;
+  double u = s.u[i], v = s.v[i], w = s.w[i], e = s.e[i];
+  double bx = s.Bevolx[i], by = s.Bevoly[i], bz = s.Bevolz[i], psi = s.psi[i];
+  const double au = s.au[i], av = s.av[i], aw = s.aw[i], ae = s.ae[i];
+  const double abx = s.aBevolx[i], aby = s.aBevoly[i], abz = s.aBevolz[i], apsi = s.apsi[i];
+  if ((mode & 1) && fluid) {
+    const double dtb2 = 0.5 * dt_cur;
+    u += dtb2 * au;
+    v += dtb2 * av;
+    w += dtb2 * aw;
+    e += dtb2 * ae;
+    const double rho = s.rho[i];
+    s.p[i] = P.gamma1 * rho * e;
+    bx += dtb2 * abx;
+    by += dtb2 * aby;
+    bz += dtb2 * abz;
+    psi += dtb2 * apsi;
+    s.Bx[i] = bx * rho;
+    s.By[i] = by * rho;
+    s.Bz[i] = bz * rho;
+  }
+  if (!(mode & 2)) {
+    if (fluid) {
+      s.u[i] = u; s.v[i] = v; s.w[i] = w; s.e[i] = e;
+      s.Bevolx[i] = bx; s.Bevoly[i] = by; s.Bevolz[i] = bz; s.psi[i] = psi;
+    }
+    return;
+  }
+  // initialize: the *0 copies live in registers
+  const double h0 = s.h[i];
+  s.h0[i] = h0;
+  s.converged[i] = 0.0;
+  s.omega[i] = 1.0;
+  if (!fluid) {
+    s.upred[i] = u; s.vpred[i] = v; s.wpred[i] = w; s.epred[i] = e;
+    s.Bevolxpred[i] = bx; s.Bevolypred[i] = by; s.Bevolzpred[i] = bz; s.psipred[i] = psi;
+    return;
+  }
+  const double dt = dt_next, dtb2 = 0.5 * dt;
+  const double un = u + dtb2 * au, vn = v + dtb2 * av, wn = w + dtb2 * aw;
+  s.u[i] = un;
+  s.v[i] = vn;
+  s.w[i] = wn;
+  s.upred[i] = u + dt * au;
+  s.vpred[i] = v + dt * av;
+  s.wpred[i] = w + dt * aw;
+  double x = s.x[i] + dt * un, y = s.y[i] + dt * vn, z = P.dim == 3 ? s.z[i] + dt * wn : s.z[i];
+  wrap_position(P, x, y, z);
+  s.x[i] = x;
+  s.y[i] = y;
+  s.z[i] = z;
+  s.e[i] = e + dtb2 * ae;
+  s.epred[i] = e + dt * ae;
+  const double h = h0 + dt * s.ah[i];
+  s.h[i] = h;
+  const double decay = 0.1 * s.cs[i] / h;
+  const double a10 = s.alpha1[i], aloc = s.alphaloc[i];
+  s.alpha1[i] = a10 < aloc ? aloc : (a10 + dt * aloc * decay) / (1.0 + dt * decay);
+  s.Bevolx[i] = bx + dtb2 * abx;
+  s.Bevoly[i] = by + dtb2 * aby;
+  s.Bevolz[i] = bz + dtb2 * abz;
+  s.psi[i] = psi + dtb2 * apsi;
+  s.Bevolxpred[i] = bx + dt * abx;
+  s.Bevolypred[i] = by + dt * aby;
+  s.Bevolzpred[i] = bz + dt * abz;
+  s.psipred[i] = psi + dt * apsi;
+}
+
+// min(dt_adapt) with the tf clip; the last block finishes the reduction.
+// t_host < 0: the step starts at the device clock's t + dt.
+__global__ void __launch_bounds__(256) k_dt_reduce(int n, const double* __restrict__ dt_adapt, double t_host,
+                                                   DevScalars* sc, unsigned int* ticket, double tf) {
+  double m = INFINITY;
+  bool bad = false;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double v = dt_adapt[i];
+    bad |= !(v > 0.0) || !isfinite(v);
+    m = fmin(m, v);
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) set_status(sc, MHD_ERR_NONFINITE);
+  if ((threadIdx.x & 31) == 0) atomicMin(&sc->dt_min_bits, dbl_order(m));
+  __shared__ bool last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    const double dmin = dbl_unorder(atomicAdd(&sc->dt_min_bits, 0ULL));
+    const double t_next = t_host >= 0.0 ? t_host : sc->t + sc->dt;
+    double dt = dmin;
+    if (t_next + dt > tf) dt = tf - t_next;
+    sc->dt_next = dt;
+    sc->t_next = t_next;
+    sc->dt_min_bits = ~0ULL;
+    *ticket = 0u;
+  }
+}
+
+__global__ void k_clock_advance(DevScalars* sc) {
+  sc->t = sc->t_next;
+  sc->dt = sc->dt_next;
+}
+
+__global__ void k_clock_set(DevScalars* sc, double t, double dt) {
+  sc->t = t;
+  sc->dt = dt;
+}
+
+static int blocks_for(int n) { return n > 0 ? (n + 255) / 256 : 1; }
+
+void launch_stage(Ctx* c, MhdState* s, int n, int which, double dt, cudaStream_t st) {
+  if (n <= 0) return;
+  if (which == 0) k_stage_initialize<<<blocks_for(n), 256, 0, st>>>(n, *s);
+  else if (which == 1) k_stage1<<<blocks_for(n), 256, 0, st>>>(n, *s, c->P, dt);
+  else k_stage2<<<blocks_for(n), 256, 0, st>>>(n, *s, c->P, dt);
+  c->launches++;
+}
+
+void launch_corrector_predictor(Ctx* c, MhdState* s, int n, int mode, double dt_cur, double dt_next,
+                                cudaStream_t st) {
+  const int dev = (mode & 1 ? dt_cur < 0.0 : false) || (mode & 2 ? dt_next < 0.0 : false);
+  if (n > 0) {
+    k_corrector_predictor<<<blocks_for(n), 256, 0, st>>>(n, *s, c->P, mode, dt_cur, dt_next, dev, c->d_sc);
+    c->launches++;
+  }
+  if (dev && (mode & 2)) {
+    k_clock_advance<<<1, 1, 0, st>>>(c->d_sc);
+    c->launches++;
+  }
+}
+
+void launch_dt_reduce(Ctx* c, const MhdState* s, int n, double t, cudaStream_t st) {
+  int blocks = blocks_for(n);
+  if (blocks > 1184) blocks = 1184;
+  k_dt_reduce<<<blocks, 256, 0, st>>>(n, s->dt_adapt, t, c->d_sc, &c->d_sc->ticket, c->P.tf);
+  c->launches++;
+}
+
+void launch_clock_set(Ctx* c, double t, double dt, cudaStream_t st) {
+  k_clock_set<<<1, 1, 0, st>>>(c->d_sc, t, dt);
+  c->launches++;
+}
+
+}  // namespace mhd

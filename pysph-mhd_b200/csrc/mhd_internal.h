@@ -1,0 +1,87 @@
+// mhd_internal.h -- context and launch helpers shared by the .cu files.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "mhd_common.cuh"
+
+namespace mhd {
+
+constexpr int kGatherMax = 48;
+
+// Fields permuted by the neighbour sort (besides itype): everything that
+// persists from one right-hand side to the next, plus the output properties
+// (src/particles.py:53-71) so the caller's view stays consistent.
+#define MHD_SORTED_FIELDS(X)                                                                                 \
+  X(x) X(y) X(z) X(gid) X(m) X(h) X(h0) X(u) X(v) X(w) X(e) X(upred) X(vpred) X(wpred) X(epred) X(Bevolx)      \
+  X(Bevoly) X(Bevolz) X(Bevolxpred) X(Bevolypred) X(Bevolzpred) X(psi) X(psipred) X(alpha1) X(converged)        \
+  X(omega) X(rho) X(rho_sum) X(p) X(cs) X(Bx) X(By) X(Bz)
+
+// Arrays gathered by the neighbour sort: dst[f][s] = src[f][perm[s]].
+struct GatherSet {
+  const double* src[kGatherMax];
+  double* dst[kGatherMax];
+  int nf;
+  const int32_t* isrc;
+  int32_t* idst;
+};
+
+struct Ctx {
+  MhdParams params;
+  DevParams P;
+  Grid grid;
+  bool have_grid = false;
+  int64_t n_max = 0;
+  int device = 0;
+  int64_t launches = 0;
+  std::string err;
+
+  // sort workspace
+  uint32_t* keys[2] = {nullptr, nullptr};
+  int32_t* vals[2] = {nullptr, nullptr};
+  uint32_t* sorted_keys = nullptr;
+  int32_t* perm = nullptr;
+  uint32_t* hist = nullptr;
+  uint32_t* scan_sums = nullptr;
+  int* cell_start = nullptr;
+  int64_t cell_cap = 0;
+
+  // density / force workspace
+  double* h_alt = nullptr;
+  double* au_prev = nullptr;
+  double* av_prev = nullptr;
+  double* aw_prev = nullptr;
+  double* vwave = nullptr;
+  double* inv_rho = nullptr;
+  double* inv_h = nullptr;
+  double* psich = nullptr;
+  float* f32_work = nullptr;  // packed single-precision neighbour records
+
+  double* spare[kGatherMax] = {};  // replan buffers, allocated on first use
+  double grid_margin = 1.05;       // cells are R * h_max * grid_margin wide
+
+  DevScalars* d_sc = nullptr;
+  DevScalars* h_sc = nullptr;  // pinned mirror
+};
+
+int max_sort_blocks(int64_t n_max);
+int64_t scan_sums_needed(int64_t n_max);
+void launch_reduce_hbox(Ctx* c, const MhdState* s, int n, cudaStream_t st);
+void launch_sort_cells(Ctx* c, const MhdState* s, int n, cudaStream_t st);
+void launch_gather(Ctx* c, const GatherSet& gs, int n, cudaStream_t st);
+
+// density pass `pass` (0-based) reading h_in, writing h_out
+void launch_density_pass(Ctx* c, MhdState* s, int n, int pass, const double* h_in, double* h_out, cudaStream_t st);
+void launch_force_prologue(Ctx* c, MhdState* s, int n, cudaStream_t st);
+void launch_force_pass(Ctx* c, MhdState* s, int n, cudaStream_t st);
+
+void launch_dt_reduce(Ctx* c, const MhdState* s, int n, double t, cudaStream_t st);
+void launch_stage(Ctx* c, MhdState* s, int n, int which, double dt, cudaStream_t st);
+void launch_clock_set(Ctx* c, double t, double dt, cudaStream_t st);
+void launch_corrector_predictor(Ctx* c, MhdState* s, int n, int mode, double dt_cur, double dt_next,
+                                cudaStream_t st);
+
+}  // namespace mhd

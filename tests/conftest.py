@@ -9,6 +9,7 @@ import sys
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 PKG = os.path.join(ROOT, "pysph-mhd_b200")
+BUILD_DIR = PKG
 for p in (ROOT, PKG):
     if p not in sys.path:
         sys.path.insert(0, p)
