@@ -1,0 +1,394 @@
+#!/usr/bin/env python
+"""Benchmark: particle-steps/s of the SPMHD particle update on B200.
+
+Workload (default): 3-D MHD blast, 128^3 = 2,097,152 particles on a cubic
+lattice in the periodic unit cube [-0.5, 0.5]^3, rho = 1, p = 0.1 except
+p = 10 for r < 0.1, B = (1/sqrt2, 1/sqrt2, 0), gamma = 5/3, cubic spline
+kernel with hfact 1.2 (configs/mhdblast.toml), Cullen-Dehnen alpha in
+[0.1, 1], artificial viscosity / conduction / resistivity 1, cleaning 1/1.
+Synthetic seeded inputs of that shape; no dataset is involved.
+
+One "step" is one predictor-evaluate-corrector step of the whole particle
+set (neighbour sort, iterated density, fused force pass, FP64 dt reduction,
+fused corrector-predictor), after the reference's 3-RHS warm-up.  Inputs
+(state 35 fields x 2.1M x 8 B ~ 590 MB) exceed the 126 MB L2, so no flush
+is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Multi-GPU: "replicas only" -- every rank advances its own independent blast
+(the per-instance update does not shard without a halo exchange); value is
+the particle-steps of all ranks over the max-over-ranks time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "pysph-mhd_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "particle-steps/s on 1 B200, FP32/batched vs plain FP64 at stated L2 error"
+UNIT = "particle-steps/s"
+
+# Algorithmic bytes per particle of the fused force pass (FP64): reads 25
+# doubles (x y z h m rho omega p epred u v w Bx By Bz alpha1 au' av' aw'
+# 1/h 1/rho v_wave psi*c_h psi cs), writes 16 (au av aw ae ah div div_psi
+# dt_cfl dt_adapt dB/dt x3 dpsi/dt divBsymm divBdiff alphaloc).
+FORCE_BYTES_PER_PARTICLE = {"fp64": (25 + 16) * 8}
+# FP64 operations per neighbour pair of the force pass and per distance
+# test (add, sub, mul, div, sqrt count 1; fma counts 2), counted from
+# csrc/mhd_pairs.cu.
+FORCE_FLOPS_PER_PAIR = 300
+FORCE_FLOPS_PER_CANDIDATE = 12
+
+
+def blast_case(n: int, precision: str = "fp64"):
+    dx = 1.0 / n
+    ax = -0.5 + (np.arange(n) + 0.5) * dx
+    x, y, z = np.meshgrid(ax, ax, ax, indexing="ij")
+    x, y, z = x.ravel(), y.ravel(), z.ravel()
+    cnt = x.size
+    gamma = 5.0 / 3.0
+    p = np.where(x * x + y * y + z * z < 0.1 * 0.1, 10.0, 0.1)
+    b = 1.0 / math.sqrt(2.0)
+    ic = dict(x=x, y=y, z=z, u=np.zeros(cnt), v=np.zeros(cnt), w=np.zeros(cnt), rho=np.ones(cnt),
+              h=np.full(cnt, 1.2 * dx), m=np.full(cnt, dx ** 3), e=p / (gamma - 1.0), Bx=np.full(cnt, b),
+              By=np.full(cnt, b), Bz=np.zeros(cnt), alpha1=np.full(cnt, 0.1), gid=np.arange(cnt, dtype=np.float64))
+    prm = dict(dim=3, kernel="cubic", hfact=1.2, density="iterate", gamma=gamma, mu0=1.0, av=1.0, ac=1.0, ar=1.0,
+               clean_speed=1.0, clean_damp=1.0, timestep_factor=1.0, tf=1e30, lo=[-0.5] * 3, hi=[0.5] * 3,
+               periodic=[True] * 3, alpha_min=0.1, alpha_max=1.0, precision=precision)
+    return ic, prm
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.idx = device_index
+        self.samples = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.idx), "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.samples.append(parts)
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread is not None:
+            self.thread.join(timeout=5)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if s[5 + k].lower() == "active"})
+        pw = [float(s[3]) for s in self.samples if s[3].replace(".", "").isdigit()]
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples), "power_w_max": max(pw) if pw else None}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "of measured"
+    return 6650.0, "of fallback"
+
+
+def profiled_traffic(n):
+    """DRAM bytes per force-pass launch from the committed ncu summary, scaled
+    to n particles (traffic grows in proportion to the particles processed)."""
+    path = os.path.join(ROOT, "profiles", "force_pass_traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        d = json.load(f)
+    return float(d["dram_bytes_per_particle"]) * n
+
+
+def cpu_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def oracle_rate(n_side, steps, warm_steps=0):
+    """Particle-steps/s of the C oracle (the reference restated, OpenMP over all
+    host threads) on the blast at n_side^3: warm-up untimed, then `steps`."""
+    import oracle
+
+    oracle.build()
+    ic, prm = blast_case(n_side)
+    s = oracle.State(ic)
+    o = oracle.Oracle(prm, exact_order=False, nthreads=cpu_cores())
+    o.warmup(s)
+    dt = o.initial_dt(s)
+    for _ in range(warm_steps):
+        o.step(s, dt)
+        dt = o.min_dt(s)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        o.step(s, dt)
+        dt = o.min_dt(s)
+    el = time.perf_counter() - t0
+    return s.n * steps / el, el, s.n
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    n_side = args.ref_n
+    rate, el, n = oracle_rate(n_side, args.steps, args.warmup)
+    ic_n = args.n ** 3
+    sample = (f"C oracle (reference equations restated, FP64, OpenMP {cpu_cores()} threads): 3-D blast at {n_side}^3 "
+              f"= {n} particles (same physics and spacing law as the {args.n}^3 workload), {args.warmup} untimed + "
+              f"{args.steps} timed PEC steps after the 3-RHS warm-up")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"3-D MHD blast {args.n}^3 = {ic_n} particles, cubic kernel hfact 1.2, alpha [0.1, 1]",
+                   "sample_particles": n},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cpu_cores(), "kind": "port", "sample": sample},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_b200(args, rank, world):
+    import ctypes
+
+    import torch
+
+    from src import _abi
+    from src.engine import Engine, params_from_dict
+    from src.particle_array import ParticleArray
+
+    dist = world > 1
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if dist:
+        import datetime
+
+        import torch.distributed as tdist
+
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+
+    def barrier():
+        if dist:
+            import torch.distributed as tdist
+
+            tdist.barrier()
+
+    ic, prm = blast_case(args.n, args.precision)
+    n = args.n ** 3
+    lib = _abi.load()
+    eng = Engine(params_from_dict(prm), ParticleArray("fluid", ic, device=dev))
+    eng.warmup()
+    dt0 = eng.initial_dt()
+    eng.begin(dt0)
+    eng.advance(args.warmup, finish=False)
+    torch.cuda.synchronize()
+
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    ms_k = (ctypes.c_double * 6)()
+    cnt_k = (ctypes.c_int64 * 6)()
+    lib.mhd_timing_enable(eng.ctx, 1)
+    lib.mhd_timing_read(eng.ctx, ms_k, cnt_k)
+    pairs, cands = ctypes.c_int64(), ctypes.c_int64()
+    lib.mhd_pair_counts(eng.ctx, ctypes.byref(pairs), ctypes.byref(cands), st)
+    passes0 = len(eng.density_passes)
+    launches0 = eng.launches()
+    clocks = ClockSampler(local)
+
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    eng.advance(args.steps, finish=False)
+    e1.record()
+    torch.cuda.synchronize()
+    barrier()
+    clocks.stop()
+    ms = e0.elapsed_time(e1)
+    launches = eng.launches() - launches0
+    ms_max = ms
+    if dist:
+        import torch.distributed as tdist
+
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    lib.mhd_timing_read(eng.ctx, ms_k, cnt_k)
+    lib.mhd_pair_counts(eng.ctx, ctypes.byref(pairs), ctypes.byref(cands), st)
+    lib.mhd_timing_enable(eng.ctx, 0)
+    kern = {k: {"ms_total": ms_k[i], "launches": int(cnt_k[i])} for i, k in enumerate(_abi.TIMING_KINDS)}
+    passes = eng.density_passes[passes0:]
+
+    value = world * n * args.steps / (ms_max * 1e-3)
+    force_ms = kern["force"]["ms_total"] / max(kern["force"]["launches"], 1)
+    bytes_per_launch = FORCE_BYTES_PER_PARTICLE.get(args.precision, 328) * n
+    hbm_peak, peak_src = measured_peaks()
+    achieved_gbs = bytes_per_launch / (force_ms * 1e-3) / 1e9
+    nb_mean = pairs.value / (n * args.steps)
+    cand_mean = cands.value / (n * args.steps)
+    flops = (FORCE_FLOPS_PER_PAIR * pairs.value + FORCE_FLOPS_PER_CANDIDATE * cands.value) / args.steps
+    fp64_peak = ctypes.c_double()
+    lib.mhd_probe_fma_peak(0, ctypes.byref(fp64_peak), st)
+    achieved_tf = flops / (force_ms * 1e-3) / 1e12
+    eng.close()
+
+    # ---- end-to-end through the public API: host state -> device, PEC steps
+    # with the host-side dt each step (src/solver.py loop), output pulls every
+    # pfreq = 20 steps and at the end.
+    e2e = run_e2e(args, dev) if rank == 0 or dist else None
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, el, ns = oracle_rate(args.ref_n, args.cpu_steps)
+        cpu = {"value": rate, "unit": UNIT, "cores": cpu_cores(), "kind": "port",
+               "sample": f"C oracle (reference equations restated, FP64, OpenMP) on the blast at {args.ref_n}^3 = "
+                         f"{ns} particles, {args.cpu_steps} PEC steps after the warm-up, {el:.1f} s"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32 pair sums / f64 iteration",
+            "data": "synthetic",
+            "config": {"workload": f"3-D MHD blast {args.n}^3 = {n} particles, cubic kernel hfact 1.2, "
+                                   f"alpha [0.1, 1], periodic unit cube", "precision": args.precision,
+                       "parallelism": "replicas" if world > 1 else "single", "l2_flush": "inputs (~0.6 GB) > L2",
+                       "density_passes_mean": sum(passes) / max(len(passes), 1),
+                       "neighbours_mean": nb_mean, "candidates_mean": cand_mean},
+            "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
+                         "frac": achieved_gbs / hbm_peak, "traffic": profiled_traffic(n), "kernel": "k_force_pass",
+                         "peak_source": peak_src, "bytes_per_launch": bytes_per_launch,
+                         "launch_ms": force_ms},
+            "roofline_compute": {"bound": "fp64_simt", "achieved": achieved_tf, "peak": fp64_peak.value / 1e12,
+                                 "unit": "TFLOP/s", "frac": achieved_tf * 1e12 / fp64_peak.value,
+                                 "peak_source": "measured FMA probe on this GPU", "flops_per_launch": flops},
+            "kernels_ms_per_step": {k: v["ms_total"] / args.steps for k, v in kern.items()},
+            "gpu_launches": launches,
+            "clocks": clocks.summary(),
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        import torch.distributed as tdist
+
+        tdist.barrier()
+        tdist.destroy_process_group()
+
+
+def run_e2e(args, dev):
+    import torch
+
+    from src.engine import Engine, params_from_dict
+    from src.particle_array import ParticleArray
+    from src.particles import OUTPUT_PROPERTIES
+
+    ic, prm = blast_case(args.n, args.precision)
+    n = args.n ** 3
+    # Warm-up on the device is part of start-up (excluded, as in the metric).
+    eng = Engine(params_from_dict(prm), ParticleArray("fluid", ic, device=dev))
+    eng.warmup()
+    dt = eng.initial_dt()
+    host = {k: torch.empty(n, dtype=v.dtype, pin_memory=True) for k, v in eng.pa.properties.items()}
+    for k, v in eng.pa.properties.items():
+        host[k].copy_(v)
+    out = {k: torch.empty(n, dtype=eng.pa.properties[k].dtype, pin_memory=True) for k in OUTPUT_PROPERTIES}
+    torch.cuda.synchronize()
+    pfreq = 20
+    h2d = sum(t.numel() * t.element_size() for t in host.values())
+    d2h = 0
+    t0 = time.perf_counter()
+    for k, t in host.items():
+        eng.pa.properties[k].copy_(t, non_blocking=True)
+    t = 0.0
+    for step in range(args.steps):
+        eng.step(dt)
+        t += dt
+        dt = eng.timestep(t)
+        d2h += 8
+        if (step + 1) % pfreq == 0 or step == args.steps - 1:
+            for k in OUTPUT_PROPERTIES:
+                out[k].copy_(eng.pa.properties[k], non_blocking=True)
+                d2h += out[k].numel() * out[k].element_size()
+            torch.cuda.synchronize()
+    el = time.perf_counter() - t0
+    eng.close()
+    return {"value": n * args.steps / el, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,
+            "d2h_bytes_per_step": d2h / args.steps,
+            "path": "ParticleArray push from pinned host + Engine.step (literal MHDStep stages, host dt per step) "
+                    "+ OUTPUT_PROPERTIES pulled every 20 steps and at the end"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=("b200", "reference"))
+    ap.add_argument("--n", type=int, default=128, help="lattice side of the blast (n^3 particles)")
+    ap.add_argument("--ref-n", type=int, default=64, help="lattice side of the CPU sample")
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--precision", default="fp64", choices=("fp64", "fp32"))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+    else:
+        run_b200(args, rank, world)
+
+
+if __name__ == "__main__":
+    main()

@@ -115,6 +115,15 @@ typedef struct MhdRhsStats {
   int64_t n_cells;          /* cells of the last grid */
 } MhdRhsStats;
 
+/* Kernel families timed with CUDA events when timing is enabled. */
+#define MHD_TIMING_KINDS 6
+#define MHD_TIMING_CELLS 0        /* grid reduction, key, radix sort, cell table, gather */
+#define MHD_TIMING_DENSITY 1      /* density passes */
+#define MHD_TIMING_PROLOGUE 2     /* force prologue (G2, G3, G5) */
+#define MHD_TIMING_FORCE 3        /* fused force pass (G4, G6-G10) */
+#define MHD_TIMING_DT 4           /* timestep reduction */
+#define MHD_TIMING_INTEGRATE 5    /* integrator stages / corrector-predictor */
+
 /* ---- library and context ---- */
 
 int mhd_abi_version(void);
@@ -135,6 +144,20 @@ int mhd_ctx_set_params(void* ctx, const MhdParams* params);
 const char* mhd_last_error(void* ctx);
 /* Number of this library's kernels launched through the context so far. */
 int64_t mhd_launch_count(void* ctx);
+
+/* Per-family device time with CUDA events recorded on the launching stream
+   around each launch.  mhd_timing_read synchronises, returns the totals
+   since the previous read (ms[MHD_TIMING_KINDS], launches[...]) and resets. */
+int mhd_timing_enable(void* ctx, int32_t enable);
+int mhd_timing_read(void* ctx, double* ms, int64_t* launches);
+
+/* Measured FMA throughput (FLOP/s, FMA = 2 flops) of the FP64 or FP32 SIMT
+   pipe on the current device: the compute roof of the pair passes. */
+int mhd_probe_fma_peak(int32_t precision, double* flops_per_second, void* stream);
+
+/* Neighbour pairs (self included) and distance tests of all force passes
+   since the previous call (synchronises, then resets). */
+int mhd_pair_counts(void* ctx, int64_t* pairs, int64_t* candidates, void* stream);
 
 /* ---- neighbour search ----
    Sort the particles of `src` by cell of the neighbour grid (Morton-free

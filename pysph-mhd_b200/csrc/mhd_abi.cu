@@ -180,7 +180,7 @@ int plan_grid(Ctx* c, const MhdState* s, int n, cudaStream_t st) {
   if (h.status != MHD_OK) FAIL(h.status, "non-finite or non-positive smoothing length");
   const double hmax = n > 0 ? dbl_unorder(h.h_max_bits) : 1.0;
   const DevParams& P = c->P;
-  const double cutoff = P.R * hmax * c->grid_margin;
+  const double cutoff = P.R * hmax * c->grid_margin * (1.0 + c->list_margin);
   Grid g;
   memset(&g, 0, sizeof g);
   double extent[3];
@@ -239,61 +239,111 @@ int plan_grid(Ctx* c, const MhdState* s, int n, cudaStream_t st) {
   return MHD_OK;
 }
 
-// Sort src into dst and carry the previous accelerations into au_prev.
+// Allocate (or grow) the neighbour-list storage for `cap` entries per particle.
+int ensure_list_storage(Ctx* c, int cap) {
+  if (cap <= c->list_cap && c->nbr_idx) return MHD_OK;
+  cudaFree(c->nbr_idx);
+  c->nbr_idx = nullptr;
+  c->list_cap = 0;
+  if (dev_alloc(c, &c->nbr_idx, c->n_pad * (int64_t)cap) != MHD_OK) return MHD_ERR_CUDA;
+  c->list_cap = cap;
+  return MHD_OK;
+}
+
+// Sort src into dst, carry the previous accelerations into au_prev and build
+// the neighbour lists of the sorted particles.
 int sort_into(Ctx* c, const MhdState* src, MhdState* dst, int n, cudaStream_t st) {
-  launch_sort_cells(c, src, n, st);
-  GatherSet g;
-  memset(&g, 0, sizeof g);
-  build_gather(src, dst, g);
-  launch_gather(c, g, n, st);
-  GatherSet a;
-  memset(&a, 0, sizeof a);
-  a.src[0] = src->au;
-  a.src[1] = src->av;
-  a.src[2] = src->aw;
-  a.dst[0] = c->au_prev;
-  a.dst[1] = c->av_prev;
-  a.dst[2] = c->aw_prev;
-  a.nf = 3;
-  launch_gather(c, a, n, st);
+  {
+    TimedScope ts(c, MHD_TIMING_CELLS, st);
+    launch_sort_cells(c, src, n, st);
+    GatherSet g;
+    memset(&g, 0, sizeof g);
+    build_gather(src, dst, g);
+    launch_gather(c, g, n, st);
+    GatherSet a;
+    memset(&a, 0, sizeof a);
+    a.src[0] = src->au;
+    a.src[1] = src->av;
+    a.src[2] = src->aw;
+    a.dst[0] = c->au_prev;
+    a.dst[1] = c->av_prev;
+    a.dst[2] = c->aw_prev;
+    a.nf = 3;
+    launch_gather(c, a, n, st);
+  }
+  launch_build_lists(c, dst, n, st);
+  c->lists_checked = false;
   CK(cudaGetLastError());
   return MHD_OK;
 }
 
-// Re-sort `s` in place for a grid planned from its current h (the density
-// iteration grew an h beyond the grid).  Uses the context's spare buffers.
+// Re-sort `s` in place for a grid planned from its current h and rebuild
+// the lists (an h outgrew its list during the density iteration).  Uses the
+// context's spare buffers.
 int resort_in_place(Ctx* c, MhdState* s, int n, cudaStream_t st) {
   int rc = plan_grid(c, s, n, st);
   if (rc != MHD_OK) return rc;
-  launch_sort_cells(c, s, n, st);
-  GatherSet g;
-  memset(&g, 0, sizeof g);
-  MhdState tmp;
-  memset(&tmp, 0, sizeof tmp);
-  build_gather(s, s, g);
-  const int nf = g.nf;
-  // au_prev & co. and the per-particle density diagnostics ride along.
-  g.src[nf] = c->au_prev;
-  g.src[nf + 1] = c->av_prev;
-  g.src[nf + 2] = c->aw_prev;
-  double* home[kGatherMax];
-  for (int f = 0; f < nf; f++) home[f] = g.dst[f];
-  home[nf] = c->au_prev;
-  home[nf + 1] = c->av_prev;
-  home[nf + 2] = c->aw_prev;
-  g.nf = nf + 3;
-  for (int f = 0; f < g.nf; f++) {
-    if (!c->spare[f] && dev_alloc(c, &c->spare[f], c->n_max) != MHD_OK) return MHD_ERR_CUDA;
-    g.dst[f] = c->spare[f];
+  {
+    TimedScope ts(c, MHD_TIMING_CELLS, st);
+    launch_sort_cells(c, s, n, st);
+    GatherSet g;
+    memset(&g, 0, sizeof g);
+    build_gather(s, s, g);
+    const int nf = g.nf;
+    // au_prev & co. ride along.
+    g.src[nf] = c->au_prev;
+    g.src[nf + 1] = c->av_prev;
+    g.src[nf + 2] = c->aw_prev;
+    double* home[kGatherMax];
+    for (int f = 0; f < nf; f++) home[f] = g.dst[f];
+    home[nf] = c->au_prev;
+    home[nf + 1] = c->av_prev;
+    home[nf + 2] = c->aw_prev;
+    g.nf = nf + 3;
+    for (int f = 0; f < g.nf; f++) {
+      if (!c->spare[f] && dev_alloc(c, &c->spare[f], c->n_max) != MHD_OK) return MHD_ERR_CUDA;
+      g.dst[f] = c->spare[f];
+    }
+    int32_t* itmp = (int32_t*)c->keys[c->sorted_keys == c->keys[0] ? 1 : 0];
+    g.idst = itmp;
+    launch_gather(c, g, n, st);
+    for (int f = 0; f < g.nf; f++)
+      CK(cudaMemcpyAsync(home[f], c->spare[f], sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(s->itype, itmp, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, st));
   }
-  int32_t* itmp = (int32_t*)c->keys[c->sorted_keys == c->keys[0] ? 1 : 0];
-  g.idst = itmp;
-  launch_gather(c, g, n, st);
-  for (int f = 0; f < g.nf; f++)
-    CK(cudaMemcpyAsync(home[f], c->spare[f], sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-  CK(cudaMemcpyAsync(s->itype, itmp, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, st));
+  launch_build_lists(c, s, n, st);
+  c->lists_checked = false;
   CK(cudaGetLastError());
   return MHD_OK;
+}
+
+// React to a raised `relist` (h_sc must hold a fresh copy of the device
+// scalars): grow the list capacity after an overflow, then re-plan, re-sort
+// and rebuild.
+int relist(Ctx* c, MhdState* s, int n, cudaStream_t st) {
+  const int need = c->h_sc->list_max;
+  if (need > c->list_cap) {
+    int rc = ensure_list_storage(c, ((need + need / 4) + 7) & ~7);
+    if (rc != MHD_OK) return rc;
+  }
+  CK(cudaMemsetAsync(&c->d_sc->relist, 0, 2 * sizeof(int), st));  // relist, list_max
+  return resort_in_place(c, s, n, st);
+}
+
+// Synchronise and make sure the lists cover the current h of `s`.
+int ensure_lists(Ctx* c, MhdState* s, int n, cudaStream_t st, int* rebuilds) {
+  for (int tries = 0; tries < 16; tries++) {
+    CK(cudaMemcpyAsync(c->h_sc, c->d_sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (!c->h_sc->relist) {
+      c->lists_checked = true;
+      return MHD_OK;
+    }
+    int rc = relist(c, s, n, st);
+    if (rc != MHD_OK) return rc;
+    if (rebuilds) (*rebuilds)++;
+  }
+  FAIL(MHD_ERR_CAPACITY, "neighbour lists rebuilt too often");
 }
 
 int density_iterate(Ctx* c, MhdState* s, int n, MhdRhsStats* stats, cudaStream_t st) {
@@ -303,11 +353,10 @@ int density_iterate(Ctx* c, MhdState* s, int n, MhdRhsStats* stats, cudaStream_t
     if (stats) stats->density_passes = 0;
     return MHD_OK;
   }
-  // reset pass counters
+  // reset pass counters (a relist raised by the list build stays raised)
   {
     DevScalars* d = c->d_sc;
     CK(cudaMemsetAsync(&d->n_unconverged[0], 0, sizeof(d->n_unconverged), st));
-    CK(cudaMemsetAsync(&d->replan, 0, sizeof(int), st));
     CK(cudaMemsetAsync(&d->passes_done, 0, sizeof(int), st));
   }
   double* buf[2] = {s->h, c->h_alt};
@@ -321,23 +370,28 @@ int density_iterate(Ctx* c, MhdState* s, int n, MhdRhsStats* stats, cudaStream_t
     CK(cudaStreamSynchronize(st));
     const DevScalars& h = *c->h_sc;
     const int done = h.passes_done;
-    const bool stopped = done >= P.max_iter || !P.iterate || (done >= P.min_iter && done > 0 && h.n_unconverged[done - 1] == 0);
+    const bool stopped =
+        done >= P.max_iter || (!P.iterate && done > 0) || (done >= P.min_iter && done > 0 && h.n_unconverged[done - 1] == 0);
     unconv = done > 0 ? h.n_unconverged[done - 1] : 0;
-    if (h.replan) {
-      // bring the latest h home, re-sort for a grid that covers it, continue
+    if (h.relist) {
+      // bring the latest h home, re-sort and rebuild the lists for it, go on
       if (done & 1) CK(cudaMemcpyAsync(s->h, c->h_alt, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-      int rc = resort_in_place(c, s, n, st);
+      int rc = relist(c, s, n, st);
       if (rc != MHD_OK) return rc;
       CK(cudaMemcpyAsync(c->h_alt, s->h, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-      CK(cudaMemsetAsync(&c->d_sc->replan, 0, sizeof(int), st));
       rebuilds++;
-      if (rebuilds > 64) FAIL(MHD_ERR_CAPACITY, "neighbour grid re-planned too often");
-      if (stopped) break;
+      if (rebuilds > 64) FAIL(MHD_ERR_CAPACITY, "neighbour lists rebuilt too often");
+      if (stopped) {
+        rc = ensure_lists(c, s, n, st, &rebuilds);
+        if (rc != MHD_OK) return rc;
+        break;
+      }
       pass = done;
       continue;
     }
     if (stopped) {
       if (done & 1) CK(cudaMemcpyAsync(s->h, c->h_alt, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+      c->lists_checked = true;
       break;
     }
     if (done <= pass) FAIL(MHD_ERR_CUDA, "density pass made no progress");
@@ -355,6 +409,10 @@ int density_iterate(Ctx* c, MhdState* s, int n, MhdRhsStats* stats, cudaStream_t
 
 int force_pass(Ctx* c, MhdState* s, int n, cudaStream_t st) {
   if (!c->have_grid) FAIL(MHD_ERR_INVALID, "mhd_cells_build must precede the force pass");
+  if (!c->lists_checked) {
+    int rc = ensure_lists(c, s, n, st, nullptr);
+    if (rc != MHD_OK) return rc;
+  }
   launch_force_prologue(c, s, n, st);
   launch_force_pass(c, s, n, st);
   CK(cudaGetLastError());
@@ -432,6 +490,14 @@ int mhd_ctx_create(const MhdParams* params, int64_t n_max, void** out) {
             dev_alloc(c, &c->aw_prev, N) == MHD_OK && dev_alloc(c, &c->vwave, N) == MHD_OK &&
             dev_alloc(c, &c->inv_rho, N) == MHD_OK && dev_alloc(c, &c->inv_h, N) == MHD_OK &&
             dev_alloc(c, &c->psich, N) == MHD_OK && dev_alloc(c, &c->d_sc, 1) == MHD_OK;
+  c->n_pad = (N + 31) / 32 * 32;
+  {
+    const double rr = radius_scale_of(params->kernel) * params->hfact * (1.0 + c->list_margin);
+    const double vol = params->dim == 3 ? 4.0 / 3.0 * M_PI * rr * rr * rr : M_PI * rr * rr;
+    const int cap = ((int)(1.5 * vol) + 16 + 7) & ~7;
+    ok = ok && dev_alloc(c, &c->nbr_cnt, c->n_pad) == MHD_OK && dev_alloc(c, &c->nbr_hlim, c->n_pad) == MHD_OK &&
+         ensure_list_storage(c, cap) == MHD_OK;
+  }
   if (ok && cudaMallocHost((void**)&c->h_sc, sizeof(DevScalars)) != cudaSuccess) ok = false;
   if (!ok) {
     g_err = c->err.empty() ? "workspace allocation failed" : c->err;
@@ -469,7 +535,14 @@ int mhd_ctx_destroy(void* ctx) {
   cudaFree(c->inv_h);
   cudaFree(c->psich);
   cudaFree(c->f32_work);
+  cudaFree(c->nbr_idx);
+  cudaFree(c->nbr_cnt);
+  cudaFree(c->nbr_hlim);
   for (double* p : c->spare) cudaFree(p);
+  for (auto& e : c->events) {
+    cudaEventDestroy(e.a);
+    cudaEventDestroy(e.b);
+  }
   cudaFree(c->d_sc);
   if (c->h_sc) cudaFreeHost(c->h_sc);
   delete c;
@@ -488,6 +561,48 @@ const char* mhd_last_error(void* ctx) {
 }
 
 int64_t mhd_launch_count(void* ctx) { return ctx ? ((Ctx*)ctx)->launches : 0; }
+
+int mhd_timing_enable(void* ctx, int32_t enable) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return MHD_ERR_INVALID;
+  c->timing = enable != 0;
+  return MHD_OK;
+}
+
+int mhd_timing_read(void* ctx, double* ms, int64_t* launches) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c || !ms || !launches) return MHD_ERR_INVALID;
+  for (int k = 0; k < MHD_TIMING_KINDS; k++) {
+    ms[k] = 0.0;
+    launches[k] = 0;
+  }
+  for (size_t e = 0; e < c->events_used; e++) {
+    CK(cudaEventSynchronize(c->events[e].b));
+    float t = 0.f;
+    CK(cudaEventElapsedTime(&t, c->events[e].a, c->events[e].b));
+    ms[c->events[e].kind] += t;
+    launches[c->events[e].kind] += 1;
+  }
+  c->events_used = 0;
+  return MHD_OK;
+}
+
+int mhd_probe_fma_peak(int32_t precision, double* flops_per_second, void* stream) {
+  if (!flops_per_second) return MHD_ERR_INVALID;
+  return probe_fma_peak(precision, flops_per_second, S(stream));
+}
+
+int mhd_pair_counts(void* ctx, int64_t* pairs, int64_t* candidates, void* stream) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return MHD_ERR_INVALID;
+  const cudaStream_t st = S(stream);
+  CK(cudaMemcpyAsync(c->h_sc, c->d_sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (pairs) *pairs = (int64_t)c->h_sc->n_pairs;
+  if (candidates) *candidates = (int64_t)c->h_sc->n_candidates;
+  CK(cudaMemsetAsync(&c->d_sc->n_pairs, 0, 2 * sizeof(unsigned long long), st));
+  return MHD_OK;
+}
 
 int mhd_cells_build(void* ctx, const MhdState* src, MhdState* dst, int64_t n, void* stream) {
   Ctx* c = (Ctx*)ctx;

@@ -30,6 +30,18 @@ struct Grid {
   double h_plan;  // every h must stay <= h_plan for the grid to be valid
 };
 
+// Compacted neighbour lists: entry k of particle i lives at
+// idx[((i / 32) * cap + k) * 32 + i % 32], so the 32 lanes of a warp read
+// entry k of their particles from one 128-byte line.  A list holds every j
+// with r_ij < R * max(h_i, h_j) * (1 + margin) for the h it was built with;
+// hlim[i] = h_i * (1 + margin) is the largest h_i it stays valid for.
+struct NbrList {
+  const int* idx;
+  const int* cnt;
+  const double* hlim;
+  int cap;
+};
+
 // Everything a kernel needs, passed by value.
 struct DevParams {
   int dim;
@@ -60,8 +72,12 @@ struct DevScalars {
   unsigned long long hi_bits[3];
   int status;        // first device error, MHD_OK if none
   int replan;        // an h outgrew the grid's h_plan during the density passes
+  int relist;        // an h outgrew its neighbour list, or a list overflowed
+  int list_max;      // longest neighbour list met by the last build
   int passes_done;   // density passes executed in the current group evaluation
   unsigned int ticket;  // last-block counter of the dt reduction
+  unsigned long long n_pairs;       // force-pass neighbour pairs (accumulating)
+  unsigned long long n_candidates;  // force-pass distance tests (accumulating)
   int n_unconverged[256 + 8];  // per density pass
 };
 

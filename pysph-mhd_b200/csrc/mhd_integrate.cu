@@ -243,6 +243,7 @@ static int blocks_for(int n) { return n > 0 ? (n + 255) / 256 : 1; }
 
 void launch_stage(Ctx* c, MhdState* s, int n, int which, double dt, cudaStream_t st) {
   if (n <= 0) return;
+  TimedScope ts(c, MHD_TIMING_INTEGRATE, st);
   if (which == 0) k_stage_initialize<<<blocks_for(n), 256, 0, st>>>(n, *s);
   else if (which == 1) k_stage1<<<blocks_for(n), 256, 0, st>>>(n, *s, c->P, dt);
   else k_stage2<<<blocks_for(n), 256, 0, st>>>(n, *s, c->P, dt);
@@ -252,6 +253,7 @@ void launch_stage(Ctx* c, MhdState* s, int n, int which, double dt, cudaStream_t
 void launch_corrector_predictor(Ctx* c, MhdState* s, int n, int mode, double dt_cur, double dt_next,
                                 cudaStream_t st) {
   const int dev = (mode & 1 ? dt_cur < 0.0 : false) || (mode & 2 ? dt_next < 0.0 : false);
+  TimedScope ts(c, MHD_TIMING_INTEGRATE, st);
   if (n > 0) {
     k_corrector_predictor<<<blocks_for(n), 256, 0, st>>>(n, *s, c->P, mode, dt_cur, dt_next, dev, c->d_sc);
     c->launches++;
@@ -265,6 +267,7 @@ void launch_corrector_predictor(Ctx* c, MhdState* s, int n, int mode, double dt_
 void launch_dt_reduce(Ctx* c, const MhdState* s, int n, double t, cudaStream_t st) {
   int blocks = blocks_for(n);
   if (blocks > 1184) blocks = 1184;
+  TimedScope ts(c, MHD_TIMING_DT, st);
   k_dt_reduce<<<blocks, 256, 0, st>>>(n, s->dt_adapt, t, c->d_sc, &c->d_sc->ticket, c->P.tf);
   c->launches++;
 }
@@ -272,6 +275,52 @@ void launch_dt_reduce(Ctx* c, const MhdState* s, int n, double t, cudaStream_t s
 void launch_clock_set(Ctx* c, double t, double dt, cudaStream_t st) {
   k_clock_set<<<1, 1, 0, st>>>(c->d_sc, t, dt);
   c->launches++;
+}
+
+// ---------------------------------------------------------- FMA probe
+// Eight independent FMA chains per thread keep the SIMT pipe saturated.
+template <class T>
+__global__ void __launch_bounds__(256) k_fma_probe(T* out, int iters, T b, T c) {
+  T a0 = (T)threadIdx.x, a1 = a0 + (T)1, a2 = a0 + (T)2, a3 = a0 + (T)3, a4 = a0 + (T)4, a5 = a0 + (T)5,
+    a6 = a0 + (T)6, a7 = a0 + (T)7;
+  for (int k = 0; k < iters; k++) {
+    a0 = fma(a0, b, c); a1 = fma(a1, b, c); a2 = fma(a2, b, c); a3 = fma(a3, b, c);
+    a4 = fma(a4, b, c); a5 = fma(a5, b, c); a6 = fma(a6, b, c); a7 = fma(a7, b, c);
+  }
+  const T s = ((a0 + a1) + (a2 + a3)) + ((a4 + a5) + (a6 + a7));
+  if (s == (T)-1.2345) out[blockIdx.x] = s;  // never true; keeps the chains live
+}
+
+int probe_fma_peak(int precision, double* flops, cudaStream_t st) {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int blocks = sms * 8, threads = 256, iters = 1 << 14;
+  void* out = nullptr;
+  if (cudaMalloc(&out, sizeof(double) * blocks) != cudaSuccess) return MHD_ERR_CUDA;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  float best = 1e30f;
+  for (int rep = 0; rep < 4; rep++) {
+    cudaEventRecord(a, st);
+    if (precision == MHD_PRECISION_FP32)
+      k_fma_probe<float><<<blocks, threads, 0, st>>>((float*)out, iters, 1.0000001f, 1e-7f);
+    else
+      k_fma_probe<double><<<blocks, threads, 0, st>>>((double*)out, iters, 1.0000000001, 1e-12);
+    cudaEventRecord(b, st);
+    cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    if (rep > 0 && ms < best) best = ms;
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(out);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return MHD_ERR_CUDA;
+  *flops = 2.0 * 8.0 * (double)iters * blocks * threads / (best * 1e-3);
+  return MHD_OK;
 }
 
 }  // namespace mhd

@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <vector>
 
 #include "mhd_common.cuh"
 
@@ -61,10 +62,52 @@ struct Ctx {
   float* f32_work = nullptr;  // packed single-precision neighbour records
 
   double* spare[kGatherMax] = {};  // replan buffers, allocated on first use
-  double grid_margin = 1.05;       // cells are R * h_max * grid_margin wide
+  double grid_margin = 1.0;        // cells are R * h_max * grid_margin * (1 + list_margin) wide
+
+  // compacted neighbour lists (NbrList layout), built with every grid
+  double list_margin = 0.05;
+  int list_cap = 0;
+  int* nbr_idx = nullptr;
+  int* nbr_cnt = nullptr;
+  double* nbr_hlim = nullptr;
+  int64_t n_pad = 0;  // n_max rounded up to a multiple of 32
+  bool lists_checked = false;  // the host knows the current lists are valid
+  NbrList lists() const { return NbrList{nbr_idx, nbr_cnt, nbr_hlim, list_cap}; }
 
   DevScalars* d_sc = nullptr;
   DevScalars* h_sc = nullptr;  // pinned mirror
+
+  // CUDA-event timing of kernel families (MHD_TIMING_*)
+  bool timing = false;
+  struct EventPair {
+    cudaEvent_t a, b;
+    int kind;
+  };
+  std::vector<EventPair> events;
+  size_t events_used = 0;
+};
+
+// Records a CUDA event pair around the launches in its scope when timing.
+struct TimedScope {
+  Ctx* c;
+  int kind;
+  cudaStream_t st;
+  size_t slot = (size_t)-1;
+  TimedScope(Ctx* c_, int kind_, cudaStream_t st_) : c(c_), kind(kind_), st(st_) {
+    if (!c->timing) return;
+    if (c->events_used == c->events.size()) {
+      Ctx::EventPair e;
+      cudaEventCreate(&e.a);
+      cudaEventCreate(&e.b);
+      c->events.push_back(e);
+    }
+    slot = c->events_used++;
+    c->events[slot].kind = kind;
+    cudaEventRecord(c->events[slot].a, st);
+  }
+  ~TimedScope() {
+    if (slot != (size_t)-1) cudaEventRecord(c->events[slot].b, st);
+  }
 };
 
 int max_sort_blocks(int64_t n_max);
@@ -73,6 +116,7 @@ void launch_reduce_hbox(Ctx* c, const MhdState* s, int n, cudaStream_t st);
 void launch_sort_cells(Ctx* c, const MhdState* s, int n, cudaStream_t st);
 void launch_gather(Ctx* c, const GatherSet& gs, int n, cudaStream_t st);
 
+void launch_build_lists(Ctx* c, const MhdState* s, int n, cudaStream_t st);
 // density pass `pass` (0-based) reading h_in, writing h_out
 void launch_density_pass(Ctx* c, MhdState* s, int n, int pass, const double* h_in, double* h_out, cudaStream_t st);
 void launch_force_prologue(Ctx* c, MhdState* s, int n, cudaStream_t st);
@@ -81,6 +125,7 @@ void launch_force_pass(Ctx* c, MhdState* s, int n, cudaStream_t st);
 void launch_dt_reduce(Ctx* c, const MhdState* s, int n, double t, cudaStream_t st);
 void launch_stage(Ctx* c, MhdState* s, int n, int which, double dt, cudaStream_t st);
 void launch_clock_set(Ctx* c, double t, double dt, cudaStream_t st);
+int probe_fma_peak(int precision, double* flops, cudaStream_t st);
 void launch_corrector_predictor(Ctx* c, MhdState* s, int n, int mode, double dt_cur, double dt_next,
                                 cudaStream_t st);
 

@@ -24,18 +24,18 @@ namespace mhd {
 
 // ------------------------------------------------------------ density pass
 template <int K, int DIM>
-__global__ void __launch_bounds__(128) k_density_pass(int n, int pass, DevParams P, Grid G,
-                                                      const int* __restrict__ cell_start,
+__global__ void __launch_bounds__(128) k_density_pass(int n, int pass, DevParams P, NbrList L,
                                                       const double* __restrict__ x, const double* __restrict__ y,
                                                       const double* __restrict__ z, const double* __restrict__ m,
                                                       const double* __restrict__ h_in, double* __restrict__ h_out,
                                                       const double* __restrict__ h0, double* __restrict__ rho_sum,
                                                       double* __restrict__ omega, double* __restrict__ converged,
                                                       DevScalars* sc) {
+  // Stop when the iterated group already stopped after pass `pass` (1-based
+  // count), or when the neighbour lists no longer cover the current h.
+  if (sc->relist) return;
   if (pass > 0) {
-    // The iterated group already stopped after pass `pass` (1-based count).
-    const bool stop = sc->replan || !P.iterate || pass >= P.max_iter ||
-                      (pass >= P.min_iter && sc->n_unconverged[pass - 1] == 0);
+    const bool stop = !P.iterate || pass >= P.max_iter || (pass >= P.min_iter && sc->n_unconverged[pass - 1] == 0);
     if (stop) return;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) atomicMax(&sc->passes_done, pass + 1);
@@ -54,7 +54,10 @@ __global__ void __launch_bounds__(128) k_density_pass(int n, int pass, DevParams
   const double rhi2 = rh2_exact(P.R, hi);
   constexpr bool compact = K <= MHD_KERNEL_WENDLAND_C6;
   double rs = 0.0, ds = 0.0;
-  for_each_candidate<DIM>(G, P, cell_start, xi, yi, zi, [&](int j) {
+  const int cnt = L.cnt[i];
+  const int* __restrict__ row = L.idx + (size_t)(i >> 5) * L.cap * 32 + (i & 31);
+  for (int k = 0; k < cnt; k++) {
+    const int j = row[k * 32];
     const double dx = min_image(xi - x[j], P.L[0], P.half[0], P.periodic[0]);
     const double dy = min_image(yi - y[j], P.L[1], P.half[1], P.periodic[1]);
     const double dz = DIM == 3 ? min_image(zi - z[j], P.L[2], P.half[2], P.periodic[2]) : 0.0;
@@ -72,7 +75,7 @@ __global__ void __launch_bounds__(128) k_density_pass(int n, int pass, DevParams
       rs += mj * (w * fac);
       ds += mj * (-fac * h1 * (dw * q + w * (double)DIM));
     }
-  });
+  }
   // post_loop (src/equations.py:53-86)
   const double mi = m[i];
   const double rhoi = mi / pow_dim<DIM>(hi / P.hfact);
@@ -97,7 +100,60 @@ __global__ void __launch_bounds__(128) k_density_pass(int n, int pass, DevParams
   }
   h_out[i] = hout;
   rho_sum[i] = rs;
-  if (!(hout <= G.h_plan)) atomicExch(&sc->replan, 1);
+  // The lists hold every j within R * max(h_i, h_j) of the h they were built
+  // with, enlarged by the list margin; a larger h needs new lists.
+  if (!(hout <= L.hlim[i])) atomicExch(&sc->relist, 1);
+}
+
+// ------------------------------------------------------- neighbour lists
+// One thread per particle scans the 3^DIM cells around it (uniform work per
+// candidate, only the append is predicated) and appends every j within the
+// margin-enlarged symmetric radius.  Counts beyond `cap` are recorded, not
+// stored, and flag a rebuild with a larger capacity.
+template <int DIM>
+__global__ void __launch_bounds__(128) k_build_lists(int n, DevParams P, Grid G, const int* __restrict__ cell_start,
+                                                     const double* __restrict__ x, const double* __restrict__ y,
+                                                     const double* __restrict__ z, const double* __restrict__ h,
+                                                     double grow, int cap, int* __restrict__ idx,
+                                                     int* __restrict__ cnt_out, double* __restrict__ hlim,
+                                                     DevScalars* sc) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double xi = x[i], yi = y[i], zi = DIM == 3 ? z[i] : 0.0;
+  const double hg = h[i] * grow;
+  const double rhi = P.R * hg, rhi2 = rhi * rhi;
+  int* __restrict__ row = idx + (size_t)(i >> 5) * cap * 32 + (i & 31);
+  int cnt = 0;
+  for_each_candidate<DIM>(G, P, cell_start, xi, yi, zi, [&](int j) {
+    const double dx = min_image(xi - x[j], P.L[0], P.half[0], P.periodic[0]);
+    const double dy = min_image(yi - y[j], P.L[1], P.half[1], P.periodic[1]);
+    const double dz = DIM == 3 ? min_image(zi - z[j], P.L[2], P.half[2], P.periodic[2]) : 0.0;
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    const double rhj = P.R * h[j] * grow;
+    if (r2 < rhi2 || r2 < rhj * rhj) {
+      if (cnt < cap) row[cnt * 32] = j;
+      cnt++;
+    }
+  });
+  cnt_out[i] = cnt < cap ? cnt : cap;
+  hlim[i] = hg;
+  if (cnt > cap) {
+    atomicMax(&sc->list_max, cnt);
+    atomicExch(&sc->relist, 1);
+  }
+}
+
+void launch_build_lists(Ctx* c, const MhdState* s, int n, cudaStream_t st) {
+  if (n <= 0) return;
+  TimedScope ts(c, MHD_TIMING_CELLS, st);
+  const double grow = 1.0 + c->list_margin;
+  if (c->P.dim == 3)
+    k_build_lists<3><<<(n + 127) / 128, 128, 0, st>>>(n, c->P, c->grid, c->cell_start, s->x, s->y, s->z, s->h, grow,
+                                                     c->list_cap, c->nbr_idx, c->nbr_cnt, c->nbr_hlim, c->d_sc);
+  else
+    k_build_lists<2><<<(n + 127) / 128, 128, 0, st>>>(n, c->P, c->grid, c->cell_start, s->x, s->y, s->z, s->h, grow,
+                                                     c->list_cap, c->nbr_idx, c->nbr_cnt, c->nbr_hlim, c->d_sc);
+  c->launches++;
 }
 
 // ------------------------------------------------------------ force pass
@@ -144,8 +200,7 @@ __global__ void __launch_bounds__(256) k_force_prologue(int n, DevParams P, MhdS
 }
 
 template <int K, int DIM>
-__global__ void __launch_bounds__(128) k_force_pass(int n, DevParams P, Grid G, const int* __restrict__ cell_start,
-                                                    ForceArgs a, DevScalars* sc) {
+__global__ void __launch_bounds__(128) k_force_pass(int n, DevParams P, NbrList L, ForceArgs a, DevScalars* sc) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double xi = a.x[i], yi = a.y[i], zi = DIM == 3 ? a.z[i] : 0.0;
@@ -172,13 +227,16 @@ __global__ void __launch_bounds__(128) k_force_pass(int n, DevParams P, Grid G, 
   // MHDAccelerations + MagneticStressAccelerations + MagneticStateRates
   double fx = 0, fy = 0, fz = 0, fe = 0, fdiv = 0, dtc = 0;
   double bx_r = 0, by_r = 0, bz_r = 0, dbs = 0, dbd = 0;
+  unsigned npair = 0, ncand = 0;
 
-  for_each_candidate<DIM>(G, P, cell_start, xi, yi, zi, [&](int j) {
+  auto pair = [&](int j) {
+    ncand++;
     const double dx = min_image(xi - a.x[j], P.L[0], P.half[0], P.periodic[0]);
     const double dy = min_image(yi - a.y[j], P.L[1], P.half[1], P.periodic[1]);
     const double dz = DIM == 3 ? min_image(zi - a.z[j], P.L[2], P.half[2], P.periodic[2]) : 0.0;
     const double r2 = r2_exact(dx, dy, dz);
     if (!(r2 < rhi2 || r2 < rh2_exact(P.R, a.h[j]))) return;
+    npair++;
     const double r = sqrt(r2);
     const double h1j = a.inv_h[j];
     // DWI = ti * XIJ, DWJ = tj * XIJ (kernel gradient, zero at r <= 1e-12)
@@ -280,7 +338,12 @@ __global__ void __launch_bounds__(128) k_force_pass(int n, DevParams P, Grid G, 
       dbs += pmi * proj_bi + pmj * proj_bj;
       dbd += -mj * proj_db * grad_i;
     }
-  });
+  };
+  {
+    const int cnt = L.cnt[i];
+    const int* __restrict__ row = L.idx + (size_t)(i >> 5) * L.cap * 32 + (i & 31);
+    for (int k = 0; k < cnt; k++) pair(row[k * 32]);
+  }
 
   // ---- CullenDehnenAlphaDiagnostics.post_loop (src/equations.py:357-429)
   const double termnorm = omegai * irhoi;
@@ -389,20 +452,24 @@ __global__ void __launch_bounds__(128) k_force_pass(int n, DevParams P, Grid G, 
   a.apsi[i] = apsi;
   a.divBsymm[i] = rhoi * dbs;
   a.divBdiff[i] = dbd;
-  (void)sc;
+  const unsigned mask = __activemask();
+  const unsigned sp = __reduce_add_sync(mask, npair), sc_ = __reduce_add_sync(mask, ncand);
+  if ((int)(threadIdx.x & 31) == __ffs(mask) - 1) {
+    atomicAdd(&sc->n_pairs, (unsigned long long)sp);
+    atomicAdd(&sc->n_candidates, (unsigned long long)sc_);
+  }
 }
 
 // ------------------------------------------------------------- dispatch
 template <int K, int DIM>
 static void density_launch(Ctx* c, MhdState* s, int n, int pass, const double* h_in, double* h_out, cudaStream_t st) {
-  k_density_pass<K, DIM><<<(n + 127) / 128, 128, 0, st>>>(n, pass, c->P, c->grid, c->cell_start, s->x, s->y, s->z,
-                                                          s->m, h_in, h_out, s->h0, s->rho_sum, s->omega,
-                                                          s->converged, c->d_sc);
+  k_density_pass<K, DIM><<<(n + 127) / 128, 128, 0, st>>>(n, pass, c->P, c->lists(), s->x, s->y, s->z, s->m, h_in,
+                                                          h_out, s->h0, s->rho_sum, s->omega, s->converged, c->d_sc);
 }
 
 template <int K, int DIM>
 static void force_launch(Ctx* c, const ForceArgs& a, int n, cudaStream_t st) {
-  k_force_pass<K, DIM><<<(n + 127) / 128, 128, 0, st>>>(n, c->P, c->grid, c->cell_start, a, c->d_sc);
+  k_force_pass<K, DIM><<<(n + 127) / 128, 128, 0, st>>>(n, c->P, c->lists(), a, c->d_sc);
 }
 
 #define MHD_DISPATCH(FN, ...)                                                   \
@@ -421,12 +488,14 @@ static void force_launch(Ctx* c, const ForceArgs& a, int n, cudaStream_t st) {
 
 void launch_density_pass(Ctx* c, MhdState* s, int n, int pass, const double* h_in, double* h_out, cudaStream_t st) {
   if (n <= 0) return;
+  TimedScope ts(c, MHD_TIMING_DENSITY, st);
   MHD_DISPATCH(density_launch, c, s, n, pass, h_in, h_out, st);
   c->launches++;
 }
 
 void launch_force_prologue(Ctx* c, MhdState* s, int n, cudaStream_t st) {
   if (n <= 0) return;
+  TimedScope ts(c, MHD_TIMING_PROLOGUE, st);
   if (c->P.dim == 3)
     k_force_prologue<3><<<(n + 255) / 256, 256, 0, st>>>(n, c->P, *s, c->inv_h, c->inv_rho, c->vwave, c->psich);
   else
@@ -455,6 +524,7 @@ void launch_force_pass(Ctx* c, MhdState* s, int n, cudaStream_t st) {
                    s->dvdx_yz, s->dvdx_zx, s->dvdx_zy, s->dvdx_zz};
   for (int k = 0; k < 24; k++) a.cd[k] = cd[k];
   for (int k = 0; k < 9; k++) a.dvdx[k] = dv[k];
+  TimedScope ts(c, MHD_TIMING_FORCE, st);
   MHD_DISPATCH(force_launch, c, a, n, st);
   c->launches++;
 }

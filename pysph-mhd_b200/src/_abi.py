@@ -80,8 +80,10 @@ EXPORTS = (
     "mhd_sorted_field_name", "mhd_ctx_create", "mhd_ctx_destroy", "mhd_ctx_set_params", "mhd_last_error",
     "mhd_launch_count", "mhd_cells_build", "mhd_density_iterate", "mhd_force_pass", "mhd_rhs", "mhd_timestep",
     "mhd_clock_set", "mhd_clock_get", "mhd_step_initialize", "mhd_step_stage1", "mhd_step_stage2",
-    "mhd_corrector_predictor", "mhd_step",
+    "mhd_corrector_predictor", "mhd_step", "mhd_timing_enable", "mhd_timing_read", "mhd_probe_fma_peak",
+    "mhd_pair_counts",
 )
+TIMING_KINDS = ("cells", "density", "prologue", "force", "dt", "integrate")
 
 
 def load(path: str = LIB_PATH):
@@ -122,6 +124,10 @@ def load(path: str = LIB_PATH):
     lib.mhd_step_stage2.argtypes = [vp, sp, i64, dbl, vp]
     lib.mhd_corrector_predictor.argtypes = [vp, sp, i64, i32, dbl, dbl, vp]
     lib.mhd_step.argtypes = [vp, sp, sp, i64, dbl, st, vp]
+    lib.mhd_timing_enable.argtypes = [vp, i32]
+    lib.mhd_timing_read.argtypes = [vp, ctypes.POINTER(dbl), ctypes.POINTER(i64)]
+    lib.mhd_probe_fma_peak.argtypes = [i32, ctypes.POINTER(dbl), vp]
+    lib.mhd_pair_counts.argtypes = [vp, ctypes.POINTER(i64), ctypes.POINTER(i64), vp]
     _lib = lib
     return lib
 
