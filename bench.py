@@ -44,11 +44,12 @@ for _p in (ROOT, PKG):
 METRIC = "particle-steps/s on 1 B200, FP32/batched vs plain FP64 at stated L2 error"
 UNIT = "particle-steps/s"
 
-# Algorithmic bytes per particle of the fused force pass (FP64): reads 25
-# doubles (x y z h m rho omega p epred u v w Bx By Bz alpha1 au' av' aw'
-# 1/h 1/rho v_wave psi*c_h psi cs), writes 16 (au av aw ae ah div div_psi
-# dt_cfl dt_adapt dB/dt x3 dpsi/dt divBsymm divBdiff alphaloc).
-FORCE_BYTES_PER_PARTICLE = {"fp64": (25 + 16) * 8}
+# Algorithmic bytes per particle of the fused force pass: reads the FP64
+# {x, y, z, h} record, six 4-vectors of the pair precision and six FP64
+# epilogue inputs (rho omega cs psi p epred), writes 16 FP64 outputs (au av aw
+# ae ah div div_psi dt_cfl dt_adapt dB/dt x3 dpsi/dt divBsymm divBdiff
+# alphaloc); each neighbour record counted once (ideal reuse).
+FORCE_BYTES_PER_PARTICLE = {"fp64": 32 + 6 * 32 + 6 * 8 + 16 * 8, "fp32": 32 + 6 * 16 + 6 * 8 + 16 * 8}
 # FP64 operations per neighbour pair of the force pass and per distance
 # test (add, sub, mul, div, sqrt count 1; fma counts 2), counted from
 # csrc/mhd_pairs.cu.
@@ -135,7 +136,7 @@ def measured_peaks():
     return 6650.0, "of fallback"
 
 
-def profiled_traffic(n):
+def profiled_traffic(n, precision):
     """DRAM bytes per force-pass launch from the committed ncu summary, scaled
     to n particles (traffic grows in proportion to the particles processed)."""
     path = os.path.join(ROOT, "profiles", "force_pass_traffic.json")
@@ -143,7 +144,8 @@ def profiled_traffic(n):
         return None
     with open(path) as f:
         d = json.load(f)
-    return float(d["dram_bytes_per_particle"]) * n
+    per = d.get(precision, {}).get("dram_bytes_per_particle")
+    return None if per is None else float(per) * n
 
 
 def cpu_cores():
@@ -196,7 +198,8 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
-def run_b200(args, rank, world):
+def _timed(args, prec, dev, barrier, dist, world):
+    """W untimed + K timed fused steps of the blast in one precision form."""
     import ctypes
 
     import torch
@@ -205,33 +208,14 @@ def run_b200(args, rank, world):
     from src.engine import Engine, params_from_dict
     from src.particle_array import ParticleArray
 
-    dist = world > 1
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    if dist:
-        import datetime
-
-        import torch.distributed as tdist
-
-        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
-
-    def barrier():
-        if dist:
-            import torch.distributed as tdist
-
-            tdist.barrier()
-
-    ic, prm = blast_case(args.n, args.precision)
+    ic, prm = blast_case(args.n, prec)
     n = args.n ** 3
     lib = _abi.load()
     eng = Engine(params_from_dict(prm), ParticleArray("fluid", ic, device=dev))
     eng.warmup()
-    dt0 = eng.initial_dt()
-    eng.begin(dt0)
+    eng.begin(eng.initial_dt())
     eng.advance(args.warmup, finish=False)
     torch.cuda.synchronize()
-
     st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
     ms_k = (ctypes.c_double * 6)()
     cnt_k = (ctypes.c_int64 * 6)()
@@ -241,8 +225,7 @@ def run_b200(args, rank, world):
     lib.mhd_pair_counts(eng.ctx, ctypes.byref(pairs), ctypes.byref(cands), st)
     passes0 = len(eng.density_passes)
     launches0 = eng.launches()
-    clocks = ClockSampler(local)
-
+    clocks = ClockSampler(dev.index or 0)
     barrier()
     torch.cuda.synchronize()
     clocks.start()
@@ -266,26 +249,82 @@ def run_b200(args, rank, world):
     lib.mhd_timing_read(eng.ctx, ms_k, cnt_k)
     lib.mhd_pair_counts(eng.ctx, ctypes.byref(pairs), ctypes.byref(cands), st)
     lib.mhd_timing_enable(eng.ctx, 0)
-    kern = {k: {"ms_total": ms_k[i], "launches": int(cnt_k[i])} for i, k in enumerate(_abi.TIMING_KINDS)}
     passes = eng.density_passes[passes0:]
+    eng.close()
+    kern = {k: {"ms_total": ms_k[i], "launches": int(cnt_k[i])} for i, k in enumerate(_abi.TIMING_KINDS)}
+    return {"value": world * n * args.steps / (ms_max * 1e-3), "ms_per_step": ms_max / args.steps,
+            "kernels": kern, "launches": launches, "clocks": clocks.summary(), "pairs": pairs.value,
+            "candidates": cands.value, "passes": passes}
 
-    value = world * n * args.steps / (ms_max * 1e-3)
+
+def _accuracy(args, dev, steps):
+    """rel L2 of the FP32 form against the FP64 path after `steps` steps."""
+    from src.engine import Engine, params_from_dict
+    from src.particle_array import ParticleArray
+
+    out = {}
+    for prec in ("fp64", "fp32"):
+        ic, prm = blast_case(args.n, prec)
+        eng = Engine(params_from_dict(prm), ParticleArray("fluid", ic, device=dev))
+        eng.warmup()
+        eng.begin(eng.initial_dt())
+        eng.advance(steps)
+        out[prec] = eng.pa.pull("rho", "u", "v", "w", "Bx", "By", "Bz", "e", "gid", order="gid")
+        eng.close()
+    a, b = out["fp32"], out["fp64"]
+
+    def rel(keys):
+        num = sum(float(np.sum((a[k] - b[k]) ** 2)) for k in keys)
+        den = sum(float(np.sum(b[k] ** 2)) for k in keys)
+        return math.sqrt(num / den)
+
+    return {"steps": steps, "rel_l2_rho": rel(["rho"]), "rel_l2_v": rel(["u", "v", "w"]),
+            "rel_l2_B": rel(["Bx", "By", "Bz"]), "rel_l2_e": rel(["e"]), "target": 1e-4}
+
+
+def run_b200(args, rank, world):
+    import ctypes
+
+    import torch
+
+    from src import _abi
+
+    dist = world > 1
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if dist:
+        import datetime
+
+        import torch.distributed as tdist
+
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+
+    def barrier():
+        if dist:
+            import torch.distributed as tdist
+
+            tdist.barrier()
+
+    n = args.n ** 3
+    head = _timed(args, args.precision, dev, barrier, dist, world)
+    other = "fp64" if args.precision == "fp32" else None
+    base = _timed(args, other, dev, barrier, dist, world) if (other and not args.no_fp64) else None
+    acc = _accuracy(args, dev, args.accuracy_steps) if (rank == 0 and not dist and args.accuracy_steps > 0) else None
+
+    lib = _abi.load()
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    peak = ctypes.c_double()
+    lib.mhd_probe_fma_peak(1 if args.precision == "fp32" else 0, ctypes.byref(peak), st)
+    kern = head["kernels"]
     force_ms = kern["force"]["ms_total"] / max(kern["force"]["launches"], 1)
-    bytes_per_launch = FORCE_BYTES_PER_PARTICLE.get(args.precision, 328) * n
+    bytes_per_launch = FORCE_BYTES_PER_PARTICLE[args.precision] * n
     hbm_peak, peak_src = measured_peaks()
     achieved_gbs = bytes_per_launch / (force_ms * 1e-3) / 1e9
-    nb_mean = pairs.value / (n * args.steps)
-    cand_mean = cands.value / (n * args.steps)
-    flops = (FORCE_FLOPS_PER_PAIR * pairs.value + FORCE_FLOPS_PER_CANDIDATE * cands.value) / args.steps
-    fp64_peak = ctypes.c_double()
-    lib.mhd_probe_fma_peak(0, ctypes.byref(fp64_peak), st)
+    flops = (FORCE_FLOPS_PER_PAIR * head["pairs"] + FORCE_FLOPS_PER_CANDIDATE * head["candidates"]) / args.steps
     achieved_tf = flops / (force_ms * 1e-3) / 1e12
-    eng.close()
 
-    # ---- end-to-end through the public API: host state -> device, PEC steps
-    # with the host-side dt each step (src/solver.py loop), output pulls every
-    # pfreq = 20 steps and at the end.
-    e2e = run_e2e(args, dev) if rank == 0 or dist else None
+    e2e = run_e2e(args, dev)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -295,26 +334,35 @@ def run_b200(args, rank, world):
                          f"{ns} particles, {args.cpu_steps} PEC steps after the warm-up, {el:.1f} s"}
 
     if rank == 0:
+        passes = head["passes"]
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32 pair sums / f64 iteration",
+            "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32 pair arithmetic, f64 h-iteration/epilogue/dt",
             "data": "synthetic",
             "config": {"workload": f"3-D MHD blast {args.n}^3 = {n} particles, cubic kernel hfact 1.2, "
-                                   f"alpha [0.1, 1], periodic unit cube", "precision": args.precision,
+                                   f"alpha [0.1, 1], periodic unit cube", "form": args.precision,
                        "parallelism": "replicas" if world > 1 else "single", "l2_flush": "inputs (~0.6 GB) > L2",
                        "density_passes_mean": sum(passes) / max(len(passes), 1),
-                       "neighbours_mean": nb_mean, "candidates_mean": cand_mean},
+                       "neighbours_mean": head["pairs"] / (n * args.steps),
+                       "list_entries_mean": head["candidates"] / (n * args.steps)},
+            "fp64_path": None if base is None else {"value": base["value"], "ms_per_step": base["ms_per_step"],
+                                                    "kernels_ms_per_step": {k: v["ms_total"] / args.steps for k, v
+                                                                            in base["kernels"].items()}},
+            "speedup_vs_fp64": None if base is None else head["value"] / base["value"],
+            "accuracy_vs_fp64": acc,
             "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
-                         "frac": achieved_gbs / hbm_peak, "traffic": profiled_traffic(n), "kernel": "k_force_pass",
-                         "peak_source": peak_src, "bytes_per_launch": bytes_per_launch,
+                         "frac": achieved_gbs / hbm_peak, "traffic": profiled_traffic(n, args.precision),
+                         "kernel": "k_force_pass", "peak_source": peak_src, "bytes_per_launch": bytes_per_launch,
                          "launch_ms": force_ms},
-            "roofline_compute": {"bound": "fp64_simt", "achieved": achieved_tf, "peak": fp64_peak.value / 1e12,
-                                 "unit": "TFLOP/s", "frac": achieved_tf * 1e12 / fp64_peak.value,
+            "roofline_compute": {"bound": "fp32_simt" if args.precision == "fp32" else "fp64_simt",
+                                 "achieved": achieved_tf, "peak": peak.value / 1e12, "unit": "TFLOP/s",
+                                 "frac": achieved_tf * 1e12 / peak.value,
                                  "peak_source": "measured FMA probe on this GPU", "flops_per_launch": flops},
             "kernels_ms_per_step": {k: v["ms_total"] / args.steps for k, v in kern.items()},
-            "gpu_launches": launches,
-            "clocks": clocks.summary(),
+            "gpu_launches": head["launches"],
+            "clocks": head["clocks"],
             "e2e": e2e,
             "cpu_baseline": cpu,
         }
@@ -378,7 +426,10 @@ def main():
     ap.add_argument("--n", type=int, default=128, help="lattice side of the blast (n^3 particles)")
     ap.add_argument("--ref-n", type=int, default=64, help="lattice side of the CPU sample")
     ap.add_argument("--cpu-steps", type=int, default=2)
-    ap.add_argument("--precision", default="fp64", choices=("fp64", "fp32"))
+    ap.add_argument("--precision", default="fp32", choices=("fp64", "fp32"),
+                    help="form timed as the headline value (the FP64 path is timed beside it)")
+    ap.add_argument("--accuracy-steps", type=int, default=100)
+    ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

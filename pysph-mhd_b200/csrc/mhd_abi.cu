@@ -106,6 +106,7 @@ int fill_params(Ctx* c, const MhdParams* p) {
   P.alpha_max = p->alpha_max;
   P.tf = p->tf;
   P.norm = kernel_norm(p->kernel, p->dim);
+  P.fp32 = p->precision == MHD_PRECISION_FP32 ? 1 : 0;
   return MHD_OK;
 }
 
@@ -487,9 +488,13 @@ int mhd_ctx_create(const MhdParams* params, int64_t n_max, void** out) {
             dev_alloc(c, &c->hist, (int64_t)256 * sb) == MHD_OK &&
             dev_alloc(c, &c->scan_sums, scan_sums_needed(N)) == MHD_OK && dev_alloc(c, &c->h_alt, N) == MHD_OK &&
             dev_alloc(c, &c->au_prev, N) == MHD_OK && dev_alloc(c, &c->av_prev, N) == MHD_OK &&
-            dev_alloc(c, &c->aw_prev, N) == MHD_OK && dev_alloc(c, &c->vwave, N) == MHD_OK &&
-            dev_alloc(c, &c->inv_rho, N) == MHD_OK && dev_alloc(c, &c->inv_h, N) == MHD_OK &&
-            dev_alloc(c, &c->psich, N) == MHD_OK && dev_alloc(c, &c->d_sc, 1) == MHD_OK;
+            dev_alloc(c, &c->aw_prev, N) == MHD_OK && dev_alloc(c, &c->d_sc, 1) == MHD_OK;
+  for (int k = 0; k < 7 && ok; k++) {
+    double* p = nullptr;
+    ok = dev_alloc(c, &p, 4 * ((N + 31) / 32 * 32)) == MHD_OK;
+    if (k == 0) c->rec_pos = p;
+    else c->rec[k - 1] = p;
+  }
   c->n_pad = (N + 31) / 32 * 32;
   {
     const double rr = radius_scale_of(params->kernel) * params->hfact * (1.0 + c->list_margin);
@@ -530,11 +535,8 @@ int mhd_ctx_destroy(void* ctx) {
   cudaFree(c->au_prev);
   cudaFree(c->av_prev);
   cudaFree(c->aw_prev);
-  cudaFree(c->vwave);
-  cudaFree(c->inv_rho);
-  cudaFree(c->inv_h);
-  cudaFree(c->psich);
-  cudaFree(c->f32_work);
+  cudaFree(c->rec_pos);
+  for (void* p : c->rec) cudaFree(p);
   cudaFree(c->nbr_idx);
   cudaFree(c->nbr_cnt);
   cudaFree(c->nbr_hlim);

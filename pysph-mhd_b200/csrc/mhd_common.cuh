@@ -50,6 +50,7 @@ struct DevParams {
   int min_iter;
   int max_iter;
   int periodic[3];
+  int fp32;  // pair arithmetic in FP32 (MHD_PRECISION_FP32)
   double L[3];
   double half[3];
   double lo[3];
@@ -85,53 +86,54 @@ struct DevScalars {
 // w(q) and dw/dq, unnormalised; forms and branch conditions follow PySPH's
 // pysph.base.kernels (restated): cubic spline (Monaghan), quintic spline
 // (Morris), Wendland C2/C4/C6, Gaussian, super-Gaussian.
-template <int K>
-__device__ __forceinline__ void w_dw(double q, int dim, double& w, double& dw) {
+template <int K, class T>
+__device__ __forceinline__ void w_dw(T q, int dim, T& w, T& dw) {
+  constexpr T c0 = 0, c1 = 1, c2 = 2, c3 = 3;
   if constexpr (K == MHD_KERNEL_CUBIC) {
-    if (q > 2.0) {
-      w = 0.0; dw = 0.0;
-    } else if (q > 1.0) {
-      const double t = 2.0 - q;
-      w = 0.25 * t * t * t; dw = -0.75 * t * t;
+    if (q > c2) {
+      w = c0; dw = c0;
+    } else if (q > c1) {
+      const T t = c2 - q;
+      w = (T)0.25 * t * t * t; dw = (T)-0.75 * t * t;
     } else {
-      w = 1.0 - 1.5 * q * q * (1.0 - 0.5 * q); dw = -3.0 * q * (1.0 - 0.75 * q);
+      w = c1 - (T)1.5 * q * q * (c1 - (T)0.5 * q); dw = (T)-3.0 * q * (c1 - (T)0.75 * q);
     }
   } else if constexpr (K == MHD_KERNEL_QUINTIC) {
-    if (q > 3.0) { w = 0.0; dw = 0.0; return; }
-    const double t3 = 3.0 - q, t2 = 2.0 - q, t1 = 1.0 - q;
-    const double t3s = t3 * t3, t2s = t2 * t2, t1s = t1 * t1;
+    if (q > c3) { w = c0; dw = c0; return; }
+    const T t3 = c3 - q, t2 = c2 - q, t1 = c1 - q;
+    const T t3s = t3 * t3, t2s = t2 * t2, t1s = t1 * t1;
     w = t3s * t3s * t3;
-    dw = -5.0 * t3s * t3s;
-    if (q <= 2.0) {
-      w -= 6.0 * t2s * t2s * t2;
-      dw += 30.0 * t2s * t2s;
-      if (q <= 1.0) {
-        w += 15.0 * t1s * t1s * t1;
-        dw -= 75.0 * t1s * t1s;
+    dw = (T)-5.0 * t3s * t3s;
+    if (q <= c2) {
+      w -= (T)6.0 * t2s * t2s * t2;
+      dw += (T)30.0 * t2s * t2s;
+      if (q <= c1) {
+        w += (T)15.0 * t1s * t1s * t1;
+        dw -= (T)75.0 * t1s * t1s;
       }
     }
   } else if constexpr (K == MHD_KERNEL_WENDLAND_C2) {
-    if (q >= 2.0) { w = 0.0; dw = 0.0; return; }
-    const double s = 1.0 - 0.5 * q, s3 = s * s * s;
-    w = s3 * s * (2.0 * q + 1.0); dw = -5.0 * q * s3;
+    if (q >= c2) { w = c0; dw = c0; return; }
+    const T s = c1 - (T)0.5 * q, s3 = s * s * s;
+    w = s3 * s * (c2 * q + c1); dw = (T)-5.0 * q * s3;
   } else if constexpr (K == MHD_KERNEL_WENDLAND_C4) {
-    if (q >= 2.0) { w = 0.0; dw = 0.0; return; }
-    const double s = 1.0 - 0.5 * q, s2 = s * s, s5 = s2 * s2 * s;
-    w = s5 * s * (35.0 / 12.0 * q * q + 3.0 * q + 1.0);
-    dw = -14.0 / 3.0 * q * (1.0 + 2.5 * q) * s5;
+    if (q >= c2) { w = c0; dw = c0; return; }
+    const T s = c1 - (T)0.5 * q, s2 = s * s, s5 = s2 * s2 * s;
+    w = s5 * s * ((T)(35.0 / 12.0) * q * q + c3 * q + c1);
+    dw = (T)(-14.0 / 3.0) * q * (c1 + (T)2.5 * q) * s5;
   } else if constexpr (K == MHD_KERNEL_WENDLAND_C6) {
-    if (q >= 2.0) { w = 0.0; dw = 0.0; return; }
-    const double s = 1.0 - 0.5 * q, s2 = s * s, s4 = s2 * s2, s7 = s4 * s2 * s;
-    w = s7 * s * (4.0 * q * q * q + 6.25 * q * q + 4.0 * q + 1.0);
-    dw = -5.5 * q * (1.0 + 3.5 * q + 4.0 * q * q) * s7;
+    if (q >= c2) { w = c0; dw = c0; return; }
+    const T s = c1 - (T)0.5 * q, s2 = s * s, s4 = s2 * s2, s7 = s4 * s2 * s;
+    w = s7 * s * ((T)4.0 * q * q * q + (T)6.25 * q * q + (T)4.0 * q + c1);
+    dw = (T)-5.5 * q * (c1 + (T)3.5 * q + (T)4.0 * q * q) * s7;
   } else if constexpr (K == MHD_KERNEL_GAUSSIAN) {
-    if (q >= 3.0) { w = 0.0; dw = 0.0; return; }
-    const double e = exp(-q * q);
-    w = e; dw = -2.0 * q * e;
+    if (q >= c3) { w = c0; dw = c0; return; }
+    const T e = exp(-q * q);
+    w = e; dw = -c2 * q * e;
   } else {
-    if (q >= 3.0) { w = 0.0; dw = 0.0; return; }
-    const double e = exp(-q * q), d2 = 0.5 * dim;
-    w = e * (d2 + 1.0 - q * q); dw = -2.0 * q * e * (d2 + 2.0 - q * q);
+    if (q >= c3) { w = c0; dw = c0; return; }
+    const T e = exp(-q * q), d2 = (T)0.5 * (T)dim;
+    w = e * (d2 + c1 - q * q); dw = -c2 * q * e * (d2 + c2 - q * q);
   }
 }
 

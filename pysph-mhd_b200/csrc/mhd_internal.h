@@ -55,11 +55,10 @@ struct Ctx {
   double* au_prev = nullptr;
   double* av_prev = nullptr;
   double* aw_prev = nullptr;
-  double* vwave = nullptr;
-  double* inv_rho = nullptr;
-  double* inv_h = nullptr;
-  double* psich = nullptr;
-  float* f32_work = nullptr;  // packed single-precision neighbour records
+  // packed per-particle records of the force pass: FP64 {x, y, z, h} and six
+  // 4-vectors in the pair precision (sized for FP64)
+  void* rec_pos = nullptr;
+  void* rec[6] = {};
 
   double* spare[kGatherMax] = {};  // replan buffers, allocated on first use
   double grid_margin = 1.0;        // cells are R * h_max * grid_margin * (1 + list_margin) wide
