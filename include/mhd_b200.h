@@ -188,6 +188,20 @@ int mhd_rhs(void* ctx, const MhdState* src, MhdState* dst, int64_t n, MhdRhsStat
    dt_host is non-null. */
 int mhd_timestep(void* ctx, const MhdState* s, int64_t n, double t, double* dt_host, void* stream);
 
+/* Allocation-free timestep reduction.  No counterpart in the reference: it
+   serves callers that cannot call cudaMalloc (code being captured into a
+   CUDA graph, embedders whose allocator policy forbids library-owned device
+   memory, real-time loops).  It needs no context: dt_adapt (device, n
+   values) in, *dt_out (device) = min_i dt_adapt_i clipped so t + dt <= tf, or
+   NaN if some dt_adapt is non-positive or non-finite.  Scratch is a
+   file-scope __device__ array (32 KiB) kept on every GPU that loads the
+   library; n above MHD_NOALLOC_MAX_N is rejected with MHD_ERR_INVALID.  The
+   first call on a device looks up the array's device address and clears it
+   (make it before any stream capture); calls that overlap on the GPU race on
+   the shared array. */
+#define MHD_NOALLOC_MAX_N 67108864
+int mhd_timestep_noalloc(const double* dt_adapt, int64_t n, double t, double tf, double* dt_out, void* stream);
+
 /* Device clock of the fused loop: t = start of the current step, dt = its
    size.  mhd_corrector_predictor with device dt advances it. */
 int mhd_clock_set(void* ctx, double t, double dt, void* stream);

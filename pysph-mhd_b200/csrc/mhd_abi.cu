@@ -35,6 +35,12 @@ double kernel_norm(int kernel, int dim) {
 using namespace mhd;
 
 namespace {
+thread_local std::string g_err;
+}  // namespace
+
+void mhd::set_library_error(const std::string& msg) { g_err = msg; }
+
+namespace {
 
 const char* const kFieldNames[] = {
 #define MHD_NAME_(n) #n,
@@ -42,8 +48,6 @@ const char* const kFieldNames[] = {
 #undef MHD_NAME_
     "itype"};
 constexpr int kFieldCount = sizeof(kFieldNames) / sizeof(kFieldNames[0]);
-
-thread_local std::string g_err;
 
 #define CK(call)                                                                   \
   do {                                                                             \

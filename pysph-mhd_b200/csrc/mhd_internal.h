@@ -109,6 +109,9 @@ struct TimedScope {
   }
 };
 
+// Message returned by mhd_last_error(NULL) (entry points without a context).
+void set_library_error(const std::string& msg);
+
 int max_sort_blocks(int64_t n_max);
 int64_t scan_sums_needed(int64_t n_max);
 void launch_reduce_hbox(Ctx* c, const MhdState* s, int n, cudaStream_t st);
