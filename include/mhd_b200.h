@@ -167,6 +167,13 @@ int mhd_pair_counts(void* ctx, int64_t* pairs, int64_t* candidates, void* stream
    alias.  The grid is kept in the context for the passes that follow. */
 int mhd_cells_build(void* ctx, const MhdState* src, MhdState* dst, int64_t n, void* stream);
 
+/* Neighbour count of every particle of `s` (device int32[n]) under the
+   exact FP64 rule of the neighbour search -- r2 < (R h_i)^2 or
+   r2 < (R h_j)^2, minimum image, self included -- with the current h; the
+   check that the compacted lists hold PySPH's neighbour sets
+   (src/application.py:63-78).  Needs a preceding mhd_cells_build. */
+int mhd_neighbour_counts(void* ctx, MhdState* s, int64_t n, int32_t* counts, void* stream);
+
 /* ---- equation groups (src/scheme.py:71-80) ----
    G1, DensityIteration with its iterated Group (src/equations.py:14-94,
    src/scheme.py:71); neighbours follow the current h in every pass. */

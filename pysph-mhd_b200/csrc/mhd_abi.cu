@@ -206,9 +206,10 @@ int plan_grid(Ctx* c, const MhdState* s, int n, cudaStream_t st) {
       ext = (hi - lo) * (1.0 + 1e-12) + 1e-300;
     }
     if (!isfinite(lo) || !isfinite(ext)) FAIL(MHD_ERR_NONFINITE, "non-finite particle position");
-    double ncd = floor(ext / cutoff);
-    int nc = ncd < 1.0 ? 1 : (ncd > 65536.0 ? 65536 : (int)ncd);
-    if (P.periodic[a] && nc < 3) nc = 1;
+    // packed cell coordinates hold 11/11/10 bits in 3-D, 16/16 in 2-D
+    const double axis_max = P.dim == 3 ? (a == 2 ? 1023.0 : 2047.0) : 65535.0;
+    double ncd = floor(ext * c->stencil / cutoff);
+    int nc = ncd < 1.0 ? 1 : (ncd > axis_max ? (int)axis_max : (int)ncd);
     g.nc[a] = nc;
     g.lo[a] = lo;
     extent[a] = ext;
@@ -220,16 +221,20 @@ int plan_grid(Ctx* c, const MhdState* s, int n, cudaStream_t st) {
     for (int b = 1; b < 3; b++)
       if (g.nc[b] > g.nc[a]) a = b;
     g.nc[a] = std::max(1, (int)(g.nc[a] * 0.8));
-    if (P.periodic[a] && g.nc[a] < 3) g.nc[a] = 1;
   }
+  // The stencil of +-stencil cells covers the cut-off on every axis with at
+  // least 2*stencil+1 cells; smaller axes are scanned whole.
   double hplan = INFINITY;
+  g.sw = c->stencil;
   for (int a = 0; a < 3; a++) {
     g.cs[a] = extent[a] / g.nc[a];
+    g.csf[a] = (float)g.cs[a];
     g.inv_cs[a] = a < P.dim ? 1.0 / g.cs[a] : 0.0;
-    const bool limits = a < P.dim && ((P.periodic[a] && g.nc[a] >= 3) || (!P.periodic[a] && g.nc[a] >= 2));
-    if (limits) hplan = std::min(hplan, g.cs[a] / P.R * (1.0 - 1e-9));
+    const bool limits = a < P.dim && g.nc[a] >= 2 * g.sw + 1;
+    if (limits) hplan = std::min(hplan, g.sw * g.cs[a] / (P.R * (1.0 + c->list_margin)) * (1.0 - 1e-9));
   }
   g.h_plan = hplan;
+  c->list_cut = cutoff;
   g.ncells = g.nc[0] * g.nc[1] * g.nc[2];
   if ((int64_t)g.ncells + 1 > c->cell_cap) {
     if (c->cell_start) cudaFree(c->cell_start);
@@ -276,6 +281,7 @@ int sort_into(Ctx* c, const MhdState* src, MhdState* dst, int n, cudaStream_t st
     a.nf = 3;
     launch_gather(c, a, n, st);
   }
+  launch_pack_positions(c, dst, n, st);
   launch_build_lists(c, dst, n, st);
   c->lists_checked = false;
   CK(cudaGetLastError());
@@ -316,6 +322,7 @@ int resort_in_place(Ctx* c, MhdState* s, int n, cudaStream_t st) {
       CK(cudaMemcpyAsync(home[f], c->spare[f], sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
     CK(cudaMemcpyAsync(s->itype, itmp, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, st));
   }
+  launch_pack_positions(c, s, n, st);
   launch_build_lists(c, s, n, st);
   c->lists_checked = false;
   CK(cudaGetLastError());
@@ -504,6 +511,7 @@ int mhd_ctx_create(const MhdParams* params, int64_t n_max, void** out) {
     const double rr = radius_scale_of(params->kernel) * params->hfact * (1.0 + c->list_margin);
     const double vol = params->dim == 3 ? 4.0 / 3.0 * M_PI * rr * rr * rr : M_PI * rr * rr;
     const int cap = ((int)(1.5 * vol) + 16 + 7) & ~7;
+    ok = ok && dev_alloc(c, &c->posf, c->n_pad) == MHD_OK && dev_alloc(c, &c->cellc, c->n_pad) == MHD_OK;
     ok = ok && dev_alloc(c, &c->nbr_cnt, c->n_pad) == MHD_OK && dev_alloc(c, &c->nbr_hlim, c->n_pad) == MHD_OK &&
          ensure_list_storage(c, cap) == MHD_OK;
   }
@@ -541,6 +549,8 @@ int mhd_ctx_destroy(void* ctx) {
   cudaFree(c->aw_prev);
   cudaFree(c->rec_pos);
   for (void* p : c->rec) cudaFree(p);
+  cudaFree(c->posf);
+  cudaFree(c->cellc);
   cudaFree(c->nbr_idx);
   cudaFree(c->nbr_cnt);
   cudaFree(c->nbr_hlim);
@@ -607,6 +617,20 @@ int mhd_pair_counts(void* ctx, int64_t* pairs, int64_t* candidates, void* stream
   if (pairs) *pairs = (int64_t)c->h_sc->n_pairs;
   if (candidates) *candidates = (int64_t)c->h_sc->n_candidates;
   CK(cudaMemsetAsync(&c->d_sc->n_pairs, 0, 2 * sizeof(unsigned long long), st));
+  return MHD_OK;
+}
+
+int mhd_neighbour_counts(void* ctx, MhdState* s, int64_t n, int32_t* counts, void* stream) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return MHD_ERR_INVALID;
+  if (n < 0 || n > c->n_max) FAIL(MHD_ERR_INVALID, "n exceeds the context's n_max");
+  if (!counts || !check_state(c, s, false)) FAIL(MHD_ERR_INVALID, "counts or state is null");
+  if (!c->have_grid) FAIL(MHD_ERR_INVALID, "mhd_cells_build must precede mhd_neighbour_counts");
+  const cudaStream_t st = S(stream);
+  int rc = ensure_lists(c, s, (int)n, st, nullptr);
+  if (rc != MHD_OK) return rc;
+  launch_neighbour_counts(c, s, (int)n, counts, st);
+  CK(cudaGetLastError());
   return MHD_OK;
 }
 

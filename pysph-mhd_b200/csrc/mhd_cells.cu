@@ -215,6 +215,36 @@ __global__ void __launch_bounds__(256) k_cell_starts(int n, int ncells, const ui
   for (int c = kprev + 1; c <= kcur; c++) cell_start[c] = s;
 }
 
+// ------------------------------------------------------- packed positions
+// FP32 position relative to the particle's cell origin (|error| <= 2^-24
+// cell widths) plus h, and the cell coordinates packed into one int: the
+// FP32 geometry of a pair is (pos_i - pos_j) + (cell_i - cell_j) * cell width.
+template <int DIM>
+__global__ void __launch_bounds__(256) k_pack_positions(int n, Grid g, const double* __restrict__ x,
+                                                        const double* __restrict__ y, const double* __restrict__ z,
+                                                        const double* __restrict__ h, float4* __restrict__ posf,
+                                                        int* __restrict__ cellc) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int cx = cell_coord(g, 0, x[i]);
+  const int cy = cell_coord(g, 1, y[i]);
+  const int cz = DIM == 3 ? cell_coord(g, 2, z[i]) : 0;
+  const float rx = (float)(x[i] - (g.lo[0] + cx * g.cs[0]));
+  const float ry = (float)(y[i] - (g.lo[1] + cy * g.cs[1]));
+  const float rz = DIM == 3 ? (float)(z[i] - (g.lo[2] + cz * g.cs[2])) : 0.f;
+  posf[i] = make_float4(rx, ry, rz, (float)h[i]);
+  cellc[i] = pack_cell<DIM>(cx, cy, cz);
+}
+
+void launch_pack_positions(Ctx* c, const MhdState* s, int n, cudaStream_t st) {
+  if (n <= 0) return;
+  if (c->P.dim == 3)
+    k_pack_positions<3><<<(n + 255) / 256, 256, 0, st>>>(n, c->grid, s->x, s->y, s->z, s->h, c->posf, c->cellc);
+  else
+    k_pack_positions<2><<<(n + 255) / 256, 256, 0, st>>>(n, c->grid, s->x, s->y, s->z, s->h, c->posf, c->cellc);
+  c->launches++;
+}
+
 // ------------------------------------------------------------------ gather
 __global__ void __launch_bounds__(256) k_gather(int n, const int32_t* __restrict__ perm, GatherSet gs) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;

@@ -28,6 +28,8 @@ struct Grid {
   double inv_cs[3];
   double cs[3];
   double h_plan;  // every h must stay <= h_plan for the grid to be valid
+  float csf[3];   // cell widths in FP32 (packed-position geometry)
+  int sw;         // stencil half-width in cells: widths >= cut-off / sw
 };
 
 // Compacted neighbour lists: entry k of particle i lives at
@@ -270,6 +272,131 @@ __device__ __forceinline__ void for_each_candidate(const Grid& G, const DevParam
       const RowRanges r = row_ranges(G, cell_start, zc * ny + yc, cx, P.periodic[0]);
       for (int j = r.b0; j < r.e0; j++) f(j);
       for (int j = r.b1; j < r.e1; j++) f(j);
+    }
+  }
+}
+
+// Cell coordinates in one int: 11/11/10 bits in 3-D, 16/16 in 2-D.
+template <int DIM>
+__device__ __forceinline__ int pack_cell(int cx, int cy, int cz) {
+  if constexpr (DIM == 3) return cx | (cy << 11) | (cz << 22);
+  else return cx | (cy << 16);
+}
+template <int DIM>
+__device__ __forceinline__ void unpack_cell(int c, int& cx, int& cy, int& cz) {
+  if constexpr (DIM == 3) {
+    cx = c & 2047;
+    cy = (c >> 11) & 2047;
+    cz = (c >> 22) & 1023;
+  } else {
+    cx = c & 65535;
+    cy = (c >> 16) & 65535;
+    cz = 0;
+  }
+}
+
+// Cell offset ci - cj along an axis, wrapped to the nearest periodic image.
+__device__ __forceinline__ int cell_delta(int d, int nc, int periodic) {
+  if (periodic && nc >= 3) {
+    if (d > nc / 2) d -= nc;
+    else if (d < -(nc / 2)) d += nc;
+  }
+  return d;
+}
+
+// FP32 minimum-image displacement x_i - x_j from packed positions: the cell
+// offset carries the large part exactly, the in-cell offsets the rest.  On a
+// periodic axis with at least 2*sw+1 cells a neighbour is at most sw cells
+// away and the wrapped cell offset selects its image; an axis with fewer
+// cells (scanned whole) can hold pairs nc/2 cells apart, whose image the
+// offset does not decide, so it takes the FP32 minimum image.
+template <int DIM>
+__device__ __forceinline__ void rel_dx(const Grid& G, const DevParams& P, const float4& pi, int ci, const float4& pj,
+                                       int cj, float& dx, float& dy, float& dz) {
+  int xi, yi, zi, xj, yj, zj;
+  unpack_cell<DIM>(ci, xi, yi, zi);
+  unpack_cell<DIM>(cj, xj, yj, zj);
+  dx = (pi.x - pj.x) + (float)cell_delta(xi - xj, G.nc[0], P.periodic[0]) * G.csf[0];
+  dy = (pi.y - pj.y) + (float)cell_delta(yi - yj, G.nc[1], P.periodic[1]) * G.csf[1];
+  dz = DIM == 3 ? (pi.z - pj.z) + (float)cell_delta(zi - zj, G.nc[2], P.periodic[2]) * G.csf[2] : 0.f;
+  const int whole = 2 * G.sw + 1;
+  if (P.periodic[0] && G.nc[0] < whole) {
+    const float L = (float)P.L[0], hL = 0.5f * L;
+    dx = dx > hL ? dx - L : (dx < -hL ? dx + L : dx);
+  }
+  if (P.periodic[1] && G.nc[1] < whole) {
+    const float L = (float)P.L[1], hL = 0.5f * L;
+    dy = dy > hL ? dy - L : (dy < -hL ? dy + L : dy);
+  }
+  if (DIM == 3 && P.periodic[2] && G.nc[2] < whole) {
+    const float L = (float)P.L[2], hL = 0.5f * L;
+    dz = dz > hL ? dz - L : (dz < -hL ? dz + L : dz);
+  }
+}
+
+// Visits every j in the cells within `cut` of (xi, yi, zi), per particle:
+// rows (y, z) whose cells lie farther than `cut` are skipped and each row's
+// x-range is trimmed to [x - cut, x + cut] (one or two contiguous ranges of
+// the cell-sorted order).  Requires cell widths >= cut / G.sw.
+template <int DIM, class F>
+__device__ __forceinline__ void for_each_candidate_trimmed(const Grid& G, const DevParams& P,
+                                                           const int* __restrict__ cell_start, double xi, double yi,
+                                                           double zi, double cut, F&& f) {
+  const int sw = G.sw;
+  const int nx = G.nc[0], ny = G.nc[1], nz = G.nc[2];
+  const int cy = cell_coord(G, 1, yi);
+  const int cz = DIM == 3 ? cell_coord(G, 2, zi) : 0;
+  // x-range of cells (unwrapped), trimmed to the cut-off
+  int xl, xh;
+  if (nx < 2 * sw + 1) {
+    xl = 0;
+    xh = nx - 1;
+  } else {
+    xl = (int)floor((xi - cut - G.lo[0]) * G.inv_cs[0]);
+    xh = (int)floor((xi + cut - G.lo[0]) * G.inv_cs[0]);
+    if (!P.periodic[0]) {
+      xl = xl < 0 ? 0 : xl;
+      xh = xh >= nx ? nx - 1 : xh;
+    }
+  }
+  const double cut2 = cut * cut;
+  const int zsw = (DIM == 3 && nz > 1) ? (nz < 2 * sw + 1 ? -1 : sw) : 0;
+  const int ysw = ny > 1 ? (ny < 2 * sw + 1 ? -1 : sw) : 0;
+  const int zlo = zsw < 0 ? 0 : cz - zsw, zhi = zsw < 0 ? nz - 1 : cz + zsw;
+  const int ylo = ysw < 0 ? 0 : cy - ysw, yhi = ysw < 0 ? ny - 1 : cy + ysw;
+  for (int zc0 = zlo; zc0 <= zhi; zc0++) {
+    int zc = zc0;
+    double dzm = 0.0;
+    if (DIM == 3 && zsw > 0) {
+      const double c_lo = G.lo[2] + zc0 * G.cs[2], c_hi = c_lo + G.cs[2];
+      dzm = zi < c_lo ? c_lo - zi : (zi > c_hi ? zi - c_hi : 0.0);
+      if (dzm * dzm >= cut2) continue;
+      if (zc < 0 || zc >= nz) {
+        if (!P.periodic[2]) continue;
+        zc = zc < 0 ? zc + nz : zc - nz;
+      }
+    }
+    for (int yc0 = ylo; yc0 <= yhi; yc0++) {
+      int yc = yc0;
+      if (ysw > 0) {
+        const double c_lo = G.lo[1] + yc0 * G.cs[1], c_hi = c_lo + G.cs[1];
+        const double dym = yi < c_lo ? c_lo - yi : (yi > c_hi ? yi - c_hi : 0.0);
+        if (dym * dym + dzm * dzm >= cut2) continue;
+        if (yc < 0 || yc >= ny) {
+          if (!P.periodic[1]) continue;
+          yc = yc < 0 ? yc + ny : yc - ny;
+        }
+      }
+      const int base = (zc * ny + yc) * nx;
+      if (xl < 0) {
+        for (int j = cell_start[base + xl + nx]; j < cell_start[base + nx]; j++) f(j);
+        for (int j = cell_start[base]; j < cell_start[base + xh + 1]; j++) f(j);
+      } else if (xh >= nx) {
+        for (int j = cell_start[base + xl]; j < cell_start[base + nx]; j++) f(j);
+        for (int j = cell_start[base]; j < cell_start[base + xh - nx + 1]; j++) f(j);
+      } else {
+        for (int j = cell_start[base + xl]; j < cell_start[base + xh + 1]; j++) f(j);
+      }
     }
   }
 }

@@ -62,9 +62,10 @@ struct Acc<float> {
   __device__ __forceinline__ double get() const { return (double)s - (double)c; }
 };
 
-__device__ __forceinline__ float fast_rcp(float x) { return __frcp_rn(x); }
+// FP32: the MUFU approximations (about 2 ulp); FP64: IEEE division and sqrt.
+__device__ __forceinline__ float fast_rcp(float x) { return __fdividef(1.0f, x); }
 __device__ __forceinline__ double fast_rcp(double x) { return 1.0 / x; }
-__device__ __forceinline__ float fast_sqrt(float x) { return __fsqrt_rn(x); }
+__device__ __forceinline__ float fast_sqrt(float x) { return x > 0.f ? x * rsqrtf(x) : 0.f; }
 __device__ __forceinline__ double fast_sqrt(double x) { return sqrt(x); }
 
 // ------------------------------------------------------------ records
@@ -72,6 +73,9 @@ template <class T>
 struct ForceRecords {
   const V4<double>* pos;  // {x, y, z, h}
   const V4<T>* r[6];
+  const float4* posf;     // packed FP32 positions (geometry of the FP32 form)
+  const int* cellc;
+  Grid G;
 };
 
 template <class T>
@@ -91,10 +95,12 @@ __global__ void __launch_bounds__(256) k_force_prologue(int n, DevParams P, MhdS
                                                         const double* __restrict__ awp, V4<double>* __restrict__ pos,
                                                         V4<T>* __restrict__ r0, V4<T>* __restrict__ r1,
                                                         V4<T>* __restrict__ r2, V4<T>* __restrict__ r3,
-                                                        V4<T>* __restrict__ r4, V4<T>* __restrict__ r5) {
+                                                        V4<T>* __restrict__ r4, V4<T>* __restrict__ r5,
+                                                        float4* __restrict__ posf) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double h = s.h[i];
+  reinterpret_cast<float*>(posf + i)[3] = (float)h;  // h after the density iteration
   const double rho = s.m[i] / pow_dim<DIM>(h / P.hfact);
   const double p = P.gamma1 * rho * s.epred[i];
   const double cs = sqrt(P.gamma * p / rho);
@@ -153,18 +159,41 @@ __global__ void __launch_bounds__(128) k_force_pass(int n, DevParams P, NbrList 
 
   const int cnt = L.cnt[i];
   const int* __restrict__ row = L.idx + (size_t)(i >> 5) * L.cap * 32 + (i & 31);
+  float4 pif = make_float4(0.f, 0.f, 0.f, 0.f);
+  int cif = 0;
+  if constexpr (sizeof(T) == 4) {
+    pif = R.posf[i];
+    cif = R.cellc[i];
+  }
+  const float Rf = (float)P.R;
   for (int k = 0; k < cnt; k++) {
     const int j = row[k * 32];
     ncand++;
-    const V4<double> pj = ld4(R.pos + j);
-    const double dxd = min_image(xi - pj.x, P.L[0], P.half[0], P.periodic[0]);
-    const double dyd = min_image(yi - pj.y, P.L[1], P.half[1], P.periodic[1]);
-    const double dzd = DIM == 3 ? min_image(zi - pj.z, P.L[2], P.half[2], P.periodic[2]) : 0.0;
-    const double r2d = r2_exact(dxd, dyd, dzd);
-    if (!(r2d < rhi2 || r2d < rh2_exact(P.R, pj.w))) continue;
+    T dx, dy, dz, r, inv_r0;
+    if constexpr (sizeof(T) == 4) {
+      // FP32 geometry from the packed positions; FP32 neighbour test
+      const float4 pj = __ldg(R.posf + j);
+      rel_dx<DIM>(R.G, P, pif, cif, pj, __ldg(R.cellc + j), dx, dy, dz);
+      const float r2 = dx * dx + dy * dy + dz * dz;
+      const float rh = Rf * fmaxf(pif.w, pj.w);
+      if (!(r2 < rh * rh)) continue;
+      inv_r0 = r2 > 0.f ? rsqrtf(r2) : 0.f;
+      r = r2 * inv_r0;
+    } else {
+      // FP64 geometry and the exact neighbour test of the oracle
+      const V4<double> pj = ld4(R.pos + j);
+      const double dxd = min_image(xi - pj.x, P.L[0], P.half[0], P.periodic[0]);
+      const double dyd = min_image(yi - pj.y, P.L[1], P.half[1], P.periodic[1]);
+      const double dzd = DIM == 3 ? min_image(zi - pj.z, P.L[2], P.half[2], P.periodic[2]) : 0.0;
+      const double r2d = r2_exact(dxd, dyd, dzd);
+      if (!(r2d < rhi2 || r2d < rh2_exact(P.R, pj.w))) continue;
+      dx = dxd;
+      dy = dyd;
+      dz = dzd;
+      r = sqrt(r2d);
+      inv_r0 = 0;
+    }
     npair++;
-    const T dx = (T)dxd, dy = (T)dyd, dz = (T)dzd;
-    const T r = fast_sqrt((T)r2d);
     const V4<T> j0 = ld4(R.r[0] + j), j1 = ld4(R.r[1] + j), j2 = ld4(R.r[2] + j), j3 = ld4(R.r[3] + j);
     const V4<T> j4 = ld4(R.r[4] + j), j5 = ld4(R.r[5] + j);
     const T mj = j0.x, rhoj = j0.y, irhoj = j0.z, omegaj = j0.w;
@@ -172,7 +201,7 @@ __global__ void __launch_bounds__(128) k_force_pass(int n, DevParams P, NbrList 
     // DWI = ti * XIJ, DWJ = tj * XIJ (zero at r <= 1e-12)
     T ti = 0, tj = 0, inv_r = 0;
     if (r > (T)kPairDistanceEpsilon) {
-      inv_r = fast_rcp(r);
+      inv_r = sizeof(T) == 4 ? inv_r0 : fast_rcp(r);
       T w, dw;
       w_dw<K>(r * h1i, DIM, w, dw);
       ti = faci * dw * h1i * inv_r;
@@ -395,6 +424,9 @@ static ForceRecords<T> records(Ctx* c) {
   ForceRecords<T> R;
   R.pos = reinterpret_cast<const V4<double>*>(c->rec_pos);
   for (int k = 0; k < 6; k++) R.r[k] = reinterpret_cast<const V4<T>*>(c->rec[k]);
+  R.posf = c->posf;
+  R.cellc = c->cellc;
+  R.G = c->grid;
   return R;
 }
 
@@ -405,10 +437,10 @@ static void prologue_launch(Ctx* c, MhdState* s, int n, cudaStream_t st) {
   V4<double>* pos = reinterpret_cast<V4<double>*>(c->rec_pos);
   if (c->P.dim == 3)
     k_force_prologue<3, T><<<(n + 255) / 256, 256, 0, st>>>(n, c->P, *s, c->au_prev, c->av_prev, c->aw_prev, pos,
-                                                            r[0], r[1], r[2], r[3], r[4], r[5]);
+                                                            r[0], r[1], r[2], r[3], r[4], r[5], c->posf);
   else
     k_force_prologue<2, T><<<(n + 255) / 256, 256, 0, st>>>(n, c->P, *s, c->au_prev, c->av_prev, c->aw_prev, pos,
-                                                            r[0], r[1], r[2], r[3], r[4], r[5]);
+                                                            r[0], r[1], r[2], r[3], r[4], r[5], c->posf);
 }
 
 void launch_force_prologue(Ctx* c, MhdState* s, int n, cudaStream_t st) {

@@ -63,6 +63,13 @@ struct Ctx {
   double* spare[kGatherMax] = {};  // replan buffers, allocated on first use
   double grid_margin = 1.0;        // cells are R * h_max * grid_margin * (1 + list_margin) wide
 
+  // packed FP32 positions relative to the cell origin, and packed cell
+  // coordinates, of the sorted particles (written after every sort)
+  float4* posf = nullptr;
+  int* cellc = nullptr;
+  int stencil = 2;       // cells are >= list cut-off / stencil wide
+  double list_cut = 0;   // R * h_max * (1 + list_margin) of the current grid
+
   // compacted neighbour lists (NbrList layout), built with every grid
   double list_margin = 0.05;
   int list_cap = 0;
@@ -119,6 +126,8 @@ void launch_sort_cells(Ctx* c, const MhdState* s, int n, cudaStream_t st);
 void launch_gather(Ctx* c, const GatherSet& gs, int n, cudaStream_t st);
 
 void launch_build_lists(Ctx* c, const MhdState* s, int n, cudaStream_t st);
+void launch_pack_positions(Ctx* c, const MhdState* s, int n, cudaStream_t st);
+void launch_neighbour_counts(Ctx* c, const MhdState* s, int n, int* out, cudaStream_t st);
 // density pass `pass` (0-based) reading h_in, writing h_out
 void launch_density_pass(Ctx* c, MhdState* s, int n, int pass, const double* h_in, double* h_out, cudaStream_t st);
 void launch_force_prologue(Ctx* c, MhdState* s, int n, cudaStream_t st);

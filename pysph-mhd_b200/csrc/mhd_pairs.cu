@@ -49,7 +49,8 @@ __global__ void __launch_bounds__(128) k_density_pass(int n, int pass, DevParams
                                                       const double* __restrict__ h_in, double* __restrict__ h_out,
                                                       const double* __restrict__ h0, double* __restrict__ rho_sum,
                                                       double* __restrict__ omega, double* __restrict__ converged,
-                                                      DevScalars* sc) {
+                                                      Grid G, const float4* __restrict__ posf,
+                                                      const int* __restrict__ cellc, DevScalars* sc) {
   // Stop when the iterated group already stopped after pass `pass` (1-based
   // count), or when the neighbour lists no longer cover the current h.
   if (sc->relist) return;
@@ -76,18 +77,43 @@ __global__ void __launch_bounds__(128) k_density_pass(int n, int pass, DevParams
   SumT<T> rs, ds;
   const int cnt = L.cnt[i];
   const int* __restrict__ row = L.idx + (size_t)(i >> 5) * L.cap * 32 + (i & 31);
+  // FP32 form: geometry from the packed positions; FP64: exact geometry.
+  float4 pif = make_float4(0.f, 0.f, 0.f, 0.f);
+  int cif = 0;
+  float rhi2f = 0.f;
+  if constexpr (sizeof(T) == 4) {
+    pif = posf[i];
+    cif = cellc[i];
+    const float rh = (float)P.R * (float)hi;
+    rhi2f = rh * rh;
+  }
   for (int k = 0; k < cnt; k++) {
     const int j = row[k * 32];
-    const double dx = min_image(xi - x[j], P.L[0], P.half[0], P.periodic[0]);
-    const double dy = min_image(yi - y[j], P.L[1], P.half[1], P.periodic[1]);
-    const double dz = DIM == 3 ? min_image(zi - z[j], P.L[2], P.half[2], P.periodic[2]) : 0.0;
-    const double r2 = r2_exact(dx, dy, dz);
-    // For compact kernels a pair admitted only by R*h_j has W(h_i) = 0 and
-    // dW/dh(h_i) = 0, so the h_i test alone gives the same sums.
-    bool nb = r2 < rhi2;
-    if (!compact && !nb) nb = r2 < rh2_exact(P.R, h_in[j]);
+    T r;
+    bool nb;
+    if constexpr (sizeof(T) == 4) {
+      float dx, dy, dz;
+      rel_dx<DIM>(G, P, pif, cif, __ldg(posf + j), __ldg(cellc + j), dx, dy, dz);
+      const float r2 = dx * dx + dy * dy + dz * dz;
+      nb = r2 < rhi2f;
+      if (!compact && !nb) {
+        const float rh = (float)P.R * (float)h_in[j];
+        nb = r2 < rh * rh;
+      }
+      r = r2 > 0.f ? r2 * rsqrtf(r2) : 0.f;
+    } else {
+      const double dx = min_image(xi - x[j], P.L[0], P.half[0], P.periodic[0]);
+      const double dy = min_image(yi - y[j], P.L[1], P.half[1], P.periodic[1]);
+      const double dz = DIM == 3 ? min_image(zi - z[j], P.L[2], P.half[2], P.periodic[2]) : 0.0;
+      const double r2 = r2_exact(dx, dy, dz);
+      // For compact kernels a pair admitted only by R*h_j has W(h_i) = 0 and
+      // dW/dh(h_i) = 0, so the h_i test alone gives the same sums.
+      nb = r2 < rhi2;
+      if (!compact && !nb) nb = r2 < rh2_exact(P.R, h_in[j]);
+      r = nb ? sqrt(r2) : 0.0;
+    }
     if (nb) {
-      const T q = sqrt((T)r2) * h1;
+      const T q = r * h1;
       T w, dw;
       w_dw<K>(q, DIM, w, dw);
       const T mj = (T)m[j];
@@ -130,49 +156,92 @@ __global__ void __launch_bounds__(128) k_density_pass(int n, int pass, DevParams
 // candidate, only the append is predicated) and appends every j within the
 // margin-enlarged symmetric radius.  Counts beyond `cap` are recorded, not
 // stored, and flag a rebuild with a larger capacity.
+// The test runs in FP32 on the packed positions with a relative slack of
+// 4e-6 on r^2 (FP32 geometry errors are ~1e-7), and a list is declared valid
+// only up to h_i * (1 + margin) * (1 - 1e-4): every pair the exact FP64
+// criterion admits while each h stays within its limit is in the list.
 template <int DIM>
 __global__ void __launch_bounds__(128) k_build_lists(int n, DevParams P, Grid G, const int* __restrict__ cell_start,
                                                      const double* __restrict__ x, const double* __restrict__ y,
                                                      const double* __restrict__ z, const double* __restrict__ h,
-                                                     double grow, int cap, int* __restrict__ idx,
+                                                     const float4* __restrict__ posf, const int* __restrict__ cellc,
+                                                     double cut, float grow, int cap, int* __restrict__ idx,
                                                      int* __restrict__ cnt_out, double* __restrict__ hlim,
                                                      DevScalars* sc) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const double xi = x[i], yi = y[i], zi = DIM == 3 ? z[i] : 0.0;
-  const double hg = h[i] * grow;
-  const double rhi = P.R * hg, rhi2 = rhi * rhi;
+  const float4 pi = posf[i];
+  const int ci = cellc[i];
+  const float Rg = (float)P.R * grow;
+  const float rhi = Rg * pi.w, rhi2 = rhi * rhi;
+  const float slack = 1.0f + 4e-6f;
   int* __restrict__ row = idx + (size_t)(i >> 5) * cap * 32 + (i & 31);
   int cnt = 0;
-  for_each_candidate<DIM>(G, P, cell_start, xi, yi, zi, [&](int j) {
-    const double dx = min_image(xi - x[j], P.L[0], P.half[0], P.periodic[0]);
-    const double dy = min_image(yi - y[j], P.L[1], P.half[1], P.periodic[1]);
-    const double dz = DIM == 3 ? min_image(zi - z[j], P.L[2], P.half[2], P.periodic[2]) : 0.0;
-    const double r2 = dx * dx + dy * dy + dz * dz;
-    const double rhj = P.R * h[j] * grow;
-    if (r2 < rhi2 || r2 < rhj * rhj) {
+  for_each_candidate_trimmed<DIM>(G, P, cell_start, x[i], y[i], DIM == 3 ? z[i] : 0.0, cut, [&](int j) {
+    const float4 pj = __ldg(posf + j);
+    float dx, dy, dz;
+    rel_dx<DIM>(G, P, pi, ci, pj, __ldg(cellc + j), dx, dy, dz);
+    const float r2 = dx * dx + dy * dy + dz * dz;
+    const float rhj = Rg * pj.w;
+    if (r2 < fmaxf(rhi2, rhj * rhj) * slack) {
       if (cnt < cap) row[cnt * 32] = j;
       cnt++;
     }
   });
   cnt_out[i] = cnt < cap ? cnt : cap;
-  hlim[i] = hg;
+  hlim[i] = h[i] * (double)grow * (1.0 - 1e-4);
   if (cnt > cap) {
     atomicMax(&sc->list_max, cnt);
     atomicExch(&sc->relist, 1);
   }
 }
 
+// Neighbours of each particle under the exact FP64 rule of the oracle
+// (r2 < (R h_i)^2 or r2 < (R h_j)^2, self included), counted over its list.
+template <int DIM>
+__global__ void __launch_bounds__(128) k_neighbour_counts(int n, DevParams P, NbrList L, const double* __restrict__ x,
+                                                          const double* __restrict__ y, const double* __restrict__ z,
+                                                          const double* __restrict__ h, int* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double xi = x[i], yi = y[i], zi = DIM == 3 ? z[i] : 0.0;
+  const double rhi2 = rh2_exact(P.R, h[i]);
+  const int cnt = L.cnt[i];
+  const int* __restrict__ row = L.idx + (size_t)(i >> 5) * L.cap * 32 + (i & 31);
+  int nb = 0;
+  for (int k = 0; k < cnt; k++) {
+    const int j = row[k * 32];
+    const double dx = min_image(xi - x[j], P.L[0], P.half[0], P.periodic[0]);
+    const double dy = min_image(yi - y[j], P.L[1], P.half[1], P.periodic[1]);
+    const double dz = DIM == 3 ? min_image(zi - z[j], P.L[2], P.half[2], P.periodic[2]) : 0.0;
+    const double r2 = r2_exact(dx, dy, dz);
+    nb += (r2 < rhi2 || r2 < rh2_exact(P.R, h[j])) ? 1 : 0;
+  }
+  out[i] = nb;
+}
+
+void launch_neighbour_counts(Ctx* c, const MhdState* s, int n, int* out, cudaStream_t st) {
+  if (n <= 0) return;
+  if (c->P.dim == 3)
+    k_neighbour_counts<3><<<(n + 127) / 128, 128, 0, st>>>(n, c->P, c->lists(), s->x, s->y, s->z, s->h, out);
+  else
+    k_neighbour_counts<2><<<(n + 127) / 128, 128, 0, st>>>(n, c->P, c->lists(), s->x, s->y, s->z, s->h, out);
+  c->launches++;
+}
+
 void launch_build_lists(Ctx* c, const MhdState* s, int n, cudaStream_t st) {
   if (n <= 0) return;
   TimedScope ts(c, MHD_TIMING_CELLS, st);
-  const double grow = 1.0 + c->list_margin;
+  const float grow = (float)(1.0 + c->list_margin);
+  const double cut = c->list_cut * (1.0 + 1e-6);
   if (c->P.dim == 3)
-    k_build_lists<3><<<(n + 127) / 128, 128, 0, st>>>(n, c->P, c->grid, c->cell_start, s->x, s->y, s->z, s->h, grow,
-                                                     c->list_cap, c->nbr_idx, c->nbr_cnt, c->nbr_hlim, c->d_sc);
+    k_build_lists<3><<<(n + 127) / 128, 128, 0, st>>>(n, c->P, c->grid, c->cell_start, s->x, s->y, s->z, s->h,
+                                                     c->posf, c->cellc, cut, grow, c->list_cap, c->nbr_idx,
+                                                     c->nbr_cnt, c->nbr_hlim, c->d_sc);
   else
-    k_build_lists<2><<<(n + 127) / 128, 128, 0, st>>>(n, c->P, c->grid, c->cell_start, s->x, s->y, s->z, s->h, grow,
-                                                     c->list_cap, c->nbr_idx, c->nbr_cnt, c->nbr_hlim, c->d_sc);
+    k_build_lists<2><<<(n + 127) / 128, 128, 0, st>>>(n, c->P, c->grid, c->cell_start, s->x, s->y, s->z, s->h,
+                                                     c->posf, c->cellc, cut, grow, c->list_cap, c->nbr_idx,
+                                                     c->nbr_cnt, c->nbr_hlim, c->d_sc);
   c->launches++;
 }
 
@@ -182,11 +251,12 @@ static void density_launch(Ctx* c, MhdState* s, int n, int pass, const double* h
   if (c->P.fp32) {
     k_density_pass<K, DIM, float><<<(n + 127) / 128, 128, 0, st>>>(n, pass, c->P, c->lists(), s->x, s->y, s->z, s->m,
                                                                    h_in, h_out, s->h0, s->rho_sum, s->omega,
-                                                                   s->converged, c->d_sc);
+                                                                   s->converged, c->grid, c->posf, c->cellc, c->d_sc);
     return;
   }
-  k_density_pass<K, DIM, double><<<(n + 127) / 128, 128, 0, st>>>(n, pass, c->P, c->lists(), s->x, s->y, s->z, s->m, h_in,
-                                                          h_out, s->h0, s->rho_sum, s->omega, s->converged, c->d_sc);
+  k_density_pass<K, DIM, double><<<(n + 127) / 128, 128, 0, st>>>(n, pass, c->P, c->lists(), s->x, s->y, s->z, s->m,
+                                                                  h_in, h_out, s->h0, s->rho_sum, s->omega,
+                                                                  s->converged, c->grid, c->posf, c->cellc, c->d_sc);
 }
 
 #define MHD_DISPATCH(FN, ...)                                                   \

@@ -81,7 +81,7 @@ EXPORTS = (
     "mhd_launch_count", "mhd_cells_build", "mhd_density_iterate", "mhd_force_pass", "mhd_rhs", "mhd_timestep",
     "mhd_clock_set", "mhd_clock_get", "mhd_step_initialize", "mhd_step_stage1", "mhd_step_stage2",
     "mhd_corrector_predictor", "mhd_step", "mhd_timing_enable", "mhd_timing_read", "mhd_probe_fma_peak",
-    "mhd_pair_counts", "mhd_timestep_noalloc",
+    "mhd_pair_counts", "mhd_timestep_noalloc", "mhd_neighbour_counts",
 )
 NOALLOC_MAX_N = 67108864
 TIMING_KINDS = ("cells", "density", "prologue", "force", "dt", "integrate")
@@ -130,6 +130,7 @@ def load(path: str = LIB_PATH):
     lib.mhd_probe_fma_peak.argtypes = [i32, ctypes.POINTER(dbl), vp]
     lib.mhd_pair_counts.argtypes = [vp, ctypes.POINTER(i64), ctypes.POINTER(i64), vp]
     lib.mhd_timestep_noalloc.argtypes = [vp, i64, dbl, dbl, vp, vp]
+    lib.mhd_neighbour_counts.argtypes = [vp, sp, i64, vp, vp]
     _lib = lib
     return lib
 

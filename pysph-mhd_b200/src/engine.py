@@ -101,6 +101,20 @@ class Engine:
                                           self.stream))
         return dt.value
 
+    def cells_build(self):
+        """Neighbour sort + lists (PySPH's NNPS update) without evaluating."""
+        src, dst = self.pa.state(), self.pa.state(spare=True)
+        self._check(self.lib.mhd_cells_build(self.ctx, ctypes.byref(src), ctypes.byref(dst), self.pa.n, self.stream))
+        self.pa.swap()
+
+    def neighbour_counts(self):
+        """Per-particle neighbour counts under the exact rule (current order)."""
+        out = torch.empty(self.pa.n, dtype=torch.int32, device=self.pa.device)
+        s = self.pa.state()
+        self._check(self.lib.mhd_neighbour_counts(self.ctx, ctypes.byref(s), self.pa.n, ctypes.c_void_p(out.data_ptr()),
+                                                  self.stream))
+        return out
+
     # --------------------------------------------------------- fused loop
     def begin(self, dt0: float, t0: float = 0.0):
         """Initialize + stage1 of the first step (after the warm-up)."""
