@@ -334,6 +334,78 @@ __device__ __forceinline__ void rel_dx(const Grid& G, const DevParams& P, const 
   }
 }
 
+// Calls f(cx, cy, cz, jb, je) for every cell within `cut` of (xi, yi, zi):
+// (cx, cy, cz) are unwrapped cell coordinates (their offset from the
+// particle's own cell selects the periodic image), [jb, je) the cell's range
+// in the sorted order.  Rows farther than `cut` are skipped and each row is
+// trimmed to [x - cut, x + cut].  Axes with fewer than 2*sw+1 cells are
+// scanned whole with their own coordinates (no image selection).
+template <int DIM, class F>
+__device__ __forceinline__ void for_each_cell_trimmed(const Grid& G, const DevParams& P,
+                                                      const int* __restrict__ cell_start, double xi, double yi,
+                                                      double zi, double cut, F&& f) {
+  const int sw = G.sw, whole = 2 * sw + 1;
+  const int nx = G.nc[0], ny = G.nc[1], nz = G.nc[2];
+  const int cy = cell_coord(G, 1, yi);
+  const int cz = DIM == 3 ? cell_coord(G, 2, zi) : 0;
+  int xl, xh;
+  if (nx < whole) {
+    xl = 0;
+    xh = nx - 1;
+  } else {
+    xl = (int)floor((xi - cut - G.lo[0]) * G.inv_cs[0]);
+    xh = (int)floor((xi + cut - G.lo[0]) * G.inv_cs[0]);
+    if (!P.periodic[0]) {
+      xl = xl < 0 ? 0 : xl;
+      xh = xh >= nx ? nx - 1 : xh;
+    }
+  }
+  const double cut2 = cut * cut;
+  const bool zs = DIM == 3 && nz >= whole, ys = ny >= whole;
+  const int zlo = DIM == 3 ? (zs ? cz - sw : 0) : 0, zhi = DIM == 3 ? (zs ? cz + sw : nz - 1) : 0;
+  const int ylo = ys ? cy - sw : 0, yhi = ys ? cy + sw : ny - 1;
+  for (int zu = zlo; zu <= zhi; zu++) {
+    int zc = zu;
+    double dzm = 0.0;
+    if (zs) {
+      const double c_lo = G.lo[2] + zu * G.cs[2], c_hi = c_lo + G.cs[2];
+      dzm = zi < c_lo ? c_lo - zi : (zi > c_hi ? zi - c_hi : 0.0);
+      if (dzm * dzm >= cut2) continue;
+      if (zc < 0 || zc >= nz) {
+        if (!P.periodic[2]) continue;
+        zc = zc < 0 ? zc + nz : zc - nz;
+      }
+    }
+    for (int yu = ylo; yu <= yhi; yu++) {
+      int yc = yu;
+      if (ys) {
+        const double c_lo = G.lo[1] + yu * G.cs[1], c_hi = c_lo + G.cs[1];
+        const double dym = yi < c_lo ? c_lo - yi : (yi > c_hi ? yi - c_hi : 0.0);
+        if (dym * dym + dzm * dzm >= cut2) continue;
+        if (yc < 0 || yc >= ny) {
+          if (!P.periodic[1]) continue;
+          yc = yc < 0 ? yc + ny : yc - ny;
+        }
+      }
+      const int base = (zc * ny + yc) * nx;
+      int xw = xl < 0 ? xl + nx : xl;
+      int jb = cell_start[base + xw];
+      for (int xu = xl; xu <= xh; xu++) {
+        const int next = xw + 1;
+        const int je = cell_start[base + next];
+        f(xu, yu, zu, jb, je);
+        if (next == nx) {
+          xw = 0;
+          jb = cell_start[base];
+        } else {
+          xw = next;
+          jb = je;
+        }
+      }
+    }
+  }
+}
+
 // Visits every j in the cells within `cut` of (xi, yi, zi), per particle:
 // rows (y, z) whose cells lie farther than `cut` are skipped and each row's
 // x-range is trimmed to [x - cut, x + cut] (one or two contiguous ranges of

@@ -171,21 +171,36 @@ __global__ void __launch_bounds__(128) k_build_lists(int n, DevParams P, Grid G,
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const float4 pi = posf[i];
-  const int ci = cellc[i];
   const float Rg = (float)P.R * grow;
   const float rhi = Rg * pi.w, rhi2 = rhi * rhi;
   const float slack = 1.0f + 4e-6f;
   int* __restrict__ row = idx + (size_t)(i >> 5) * cap * 32 + (i & 31);
   int cnt = 0;
-  for_each_candidate_trimmed<DIM>(G, P, cell_start, x[i], y[i], DIM == 3 ? z[i] : 0.0, cut, [&](int j) {
-    const float4 pj = __ldg(posf + j);
-    float dx, dy, dz;
-    rel_dx<DIM>(G, P, pi, ci, pj, __ldg(cellc + j), dx, dy, dz);
-    const float r2 = dx * dx + dy * dy + dz * dz;
-    const float rhj = Rg * pj.w;
-    if (r2 < fmaxf(rhi2, rhj * rhj) * slack) {
-      if (cnt < cap) row[cnt * 32] = j;
-      cnt++;
+  int cxi, cyi, czi;
+  unpack_cell<DIM>(cellc[i], cxi, cyi, czi);
+  // Per cell (unwrapped coordinates ox, oy, oz) the in-cell position of i
+  // shifted by the cell offset; a candidate then costs one float4 load.
+  const int whole = 2 * G.sw + 1;
+  const bool mx = P.periodic[0] && G.nc[0] < whole, my = P.periodic[1] && G.nc[1] < whole,
+             mz = DIM == 3 && P.periodic[2] && G.nc[2] < whole;
+  const float Lx = (float)P.L[0], Ly = (float)P.L[1], Lz = (float)P.L[2];
+  for_each_cell_trimmed<DIM>(G, P, cell_start, x[i], y[i], DIM == 3 ? z[i] : 0.0, cut,
+                             [&](int cxu, int cyu, int czu, int jb, int je) {
+    const float sx = pi.x + (float)(cxi - cxu) * G.csf[0];
+    const float sy = pi.y + (float)(cyi - cyu) * G.csf[1];
+    const float sz = DIM == 3 ? pi.z + (float)(czi - czu) * G.csf[2] : 0.f;
+    for (int j = jb; j < je; j++) {
+      const float4 pj = __ldg(posf + j);
+      float dx = sx - pj.x, dy = sy - pj.y, dz = DIM == 3 ? sz - pj.z : 0.f;
+      if (mx) dx = dx > 0.5f * Lx ? dx - Lx : (dx < -0.5f * Lx ? dx + Lx : dx);
+      if (my) dy = dy > 0.5f * Ly ? dy - Ly : (dy < -0.5f * Ly ? dy + Ly : dy);
+      if (mz) dz = dz > 0.5f * Lz ? dz - Lz : (dz < -0.5f * Lz ? dz + Lz : dz);
+      const float r2 = dx * dx + dy * dy + dz * dz;
+      const float rhj = Rg * pj.w;
+      if (r2 < fmaxf(rhi2, rhj * rhj) * slack) {
+        if (cnt < cap) row[cnt * 32] = j;
+        cnt++;
+      }
     }
   });
   cnt_out[i] = cnt < cap ? cnt : cap;
