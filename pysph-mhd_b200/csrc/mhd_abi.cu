@@ -529,6 +529,8 @@ int mhd_ctx_create(const MhdParams* params, int64_t n_max, void** out) {
     return MHD_ERR_CUDA;
   }
   if (const char* m = getenv("MHD_GRID_MARGIN")) c->grid_margin = std::max(1.0, atof(m));
+  if (const char* m = getenv("MHD_FORCE_SHAPE")) c->force_shape = std::max(0, std::min(3, atoi(m)));
+  if (const char* m = getenv("MHD_STENCIL")) c->stencil = std::max(1, std::min(3, atoi(m)));
   *out = c;
   return MHD_OK;
 }

@@ -127,9 +127,14 @@ __global__ void __launch_bounds__(256) k_force_prologue(int n, DevParams P, MhdS
   r5[i] = V4<T>{(T)brx, (T)bry, (T)brz, (T)((brx * brx + bry * bry + brz * brz) * P.inv_mu0)};
 }
 
-template <int K, int DIM, class T>
-__global__ void __launch_bounds__(128) k_force_pass(int n, DevParams P, NbrList L, ForceRecords<T> R, ForceOut<T> o,
-                                                    DevScalars* sc) {
+// Launch shapes (threads per block, minimum resident blocks per SM): the
+// second number caps the registers and so sets the occupancy.
+constexpr int kForceShapes[][2] = {{128, 2}, {128, 3}, {128, 4}, {256, 2}};
+constexpr int kForceShapeCount = 4;
+
+template <int K, int DIM, class T, int SHAPE>
+__global__ void __launch_bounds__(kForceShapes[SHAPE][0], kForceShapes[SHAPE][1])
+    k_force_pass(int n, DevParams P, NbrList L, ForceRecords<T> R, ForceOut<T> o, DevScalars* sc) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const V4<double> pi = R.pos[i];
@@ -455,7 +460,17 @@ void launch_force_prologue(Ctx* c, MhdState* s, int n, cudaStream_t st) {
 
 template <int K, int DIM, class T>
 static void force_launch_t(Ctx* c, const ForceOut<T>& o, int n, cudaStream_t st) {
-  k_force_pass<K, DIM, T><<<(n + 127) / 128, 128, 0, st>>>(n, c->P, c->lists(), records<T>(c), o, c->d_sc);
+  // default shapes measured on the 128^3 blast: FP64 uncapped (208-220
+  // registers, no spills), FP32 capped at 128 registers (16 warps per SM)
+  const int s = c->force_shape >= 0 ? c->force_shape : (sizeof(T) == 4 ? 2 : 0);
+  const int bs = kForceShapes[s][0];
+  const int grid = (n + bs - 1) / bs;
+  switch (s) {
+    case 1: k_force_pass<K, DIM, T, 1><<<grid, bs, 0, st>>>(n, c->P, c->lists(), records<T>(c), o, c->d_sc); break;
+    case 2: k_force_pass<K, DIM, T, 2><<<grid, bs, 0, st>>>(n, c->P, c->lists(), records<T>(c), o, c->d_sc); break;
+    case 3: k_force_pass<K, DIM, T, 3><<<grid, bs, 0, st>>>(n, c->P, c->lists(), records<T>(c), o, c->d_sc); break;
+    default: k_force_pass<K, DIM, T, 0><<<grid, bs, 0, st>>>(n, c->P, c->lists(), records<T>(c), o, c->d_sc);
+  }
 }
 
 template <int K, int DIM>

@@ -68,6 +68,7 @@ struct Ctx {
   float4* posf = nullptr;
   int* cellc = nullptr;
   int stencil = 2;       // cells are >= list cut-off / stencil wide
+  int force_shape = -1;  // launch-shape variant of the force pass (kForceShapes); -1 = per-precision default
   double list_cut = 0;   // R * h_max * (1 + list_margin) of the current grid
 
   // compacted neighbour lists (NbrList layout), built with every grid

@@ -1,0 +1,83 @@
+"""MHDSolver: the reference's time loop (src/solver.py:22-77) on the B200 path.
+
+The loop is the reference's: skip the start-up RHS when the application has
+already warmed it, ``dt = _get_timestep()``, step while ``tf - t`` exceeds the
+tolerance and ``count < max_steps``, dump every ``pfreq`` steps.  The step and
+the timestep reduction run on the device (``src.engine.Engine``); the dump is
+an ``.npz`` of ``OUTPUT_PROPERTIES`` ordered by ``gid``.
+"""
+
+from __future__ import annotations
+
+import logging
+import os
+
+import numpy as np
+
+from .particles import OUTPUT_PROPERTIES
+
+logger = logging.getLogger(__name__)
+
+EPSILON = 2.220446049250313e-16
+
+
+class MHDSolver:
+    def __init__(self, dim=3, integrator=None, kernel="cubic", dt=1.0, tf=1.0, adaptive_timestep=True, pfreq=1,
+                 max_steps=None, output_directory=None, fname="mhd", **kw):
+        self.dim = dim
+        self.integrator = integrator
+        self.kernel = kernel
+        self.dt = dt
+        self.tf = tf
+        self.adaptive_timestep = adaptive_timestep
+        self.pfreq = pfreq
+        self.max_steps = max_steps if max_steps is not None else (1 << 62)
+        self.output_directory = output_directory
+        self.fname = fname
+        self.t = 0.0
+        self.count = 0
+        self.initial_acceleration_is_current = False
+        self.pre_step_callbacks = []
+        self.post_step_callbacks = []
+        self.particles = None
+
+    def _get_timestep(self):
+        if self.adaptive_timestep:
+            return self.integrator.compute_time_step(self.dt, t=self.t)
+        dt = self.dt
+        if self.t + dt > self.tf:
+            dt = self.tf - self.t
+        return dt
+
+    def dump_output(self):
+        if self.output_directory is None or self.particles is None:
+            return None
+        os.makedirs(self.output_directory, exist_ok=True)
+        pa = self.particles[0]
+        arrays = pa.pull(*OUTPUT_PROPERTIES, order="gid")
+        path = os.path.join(self.output_directory, f"{self.fname}_{self.count:06d}.npz")
+        np.savez(path, t=self.t, dt=self.dt, count=self.count, **arrays)
+        return path
+
+    def solve(self, show_progress=False):
+        self._epsilon = EPSILON * self.tf
+        self.dump_output()
+        if self.initial_acceleration_is_current:
+            self.initial_acceleration_is_current = False
+        else:
+            self.integrator.initial_acceleration(self.t, self.dt)
+        self.dt = self._get_timestep()
+        while (self.tf - self.t) > self._epsilon and self.count < self.max_steps:
+            for cb in self.pre_step_callbacks:
+                cb(self)
+            logger.debug("Iteration=%d, time=%f, timestep=%f", self.count, self.t, self.dt)
+            self.integrator.step(self.t, self.dt)
+            for cb in self.post_step_callbacks:
+                cb(self)
+            self.t += self.dt
+            self.count += 1
+            self._epsilon = EPSILON * self.tf * self.count
+            self.dt = self._get_timestep()
+            if self.count % self.pfreq == 0:
+                self.dump_output()
+        self.dump_output()

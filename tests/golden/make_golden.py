@@ -256,7 +256,27 @@ def case_blast3d(ref, out, n=8):
     _run(app, domain, 3, 3, out)
 
 
+def case_lattice(ref, out):
+    """Points of the reference's close_packed_lattice (src/cases/lattice.py) for
+    the bounds its case generators use."""
+    import src.cases.lattice as lattice
+
+    setups = [
+        ((-0.5, 0.5, -0.5, 0.5, -4 * math.sqrt(6.0) / 16, 4 * math.sqrt(6.0) / 16), 1.0 / 16),  # orstang nx=16
+        ((-0.5, 0.5, -0.5, 0.5, -0.5, 0.5), 1.0 / 12),  # mhdblast nx=12
+        ((-1.5, 1.5, -0.75, 0.75, -0.75, 0.75), 3.0 / 24),  # alfven nx=24
+        ((-0.5, 0.0, -0.65, 0.65, -0.61, 0.61), 0.0625),  # mhdshock left, nx=8
+    ]
+    for k, (b, s) in enumerate(setups):
+        x, y, z = lattice.close_packed_lattice(b, s)
+        out[f"set{k}/bounds"] = np.array(b)
+        out[f"set{k}/spacing"] = np.array(s)
+        out[f"set{k}/x"], out[f"set{k}/y"], out[f"set{k}/z"] = x, y, z
+    out["n_sets"] = np.array(len(setups))
+
+
 CASES = {
+    "lattice": case_lattice,
     "ot2d": case_ot2d,
     "shock2d": case_shock2d,
     "blast3d": case_blast3d,

@@ -1,0 +1,89 @@
+"""Host-side layer on CPU: configs, lattice, cases, scheme compilation.
+
+No GPU work: the case generators produce numpy arrays, the scheme's group
+list is checked against the reference structure, and the TOML schema
+accepts the reference's files and the benchmark configs.
+"""
+
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from golden_io import GOLDEN
+
+PKG = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "pysph-mhd_b200")
+REFERENCE_CONFIGS = "/root/reference/configs"
+
+
+def test_close_packed_lattice_matches_reference_function():
+    from src.cases.lattice import close_packed_lattice
+
+    d = np.load(os.path.join(GOLDEN, "lattice.npz"))
+    for k in range(int(d["n_sets"])):
+        x, y, z = close_packed_lattice(tuple(d[f"set{k}/bounds"]), float(d[f"set{k}/spacing"]))
+        np.testing.assert_array_equal(x, d[f"set{k}/x"])
+        np.testing.assert_array_equal(y, d[f"set{k}/y"])
+        np.testing.assert_array_equal(z, d[f"set{k}/z"])
+
+
+def test_benchmark_configs_load_and_build_cases():
+    from src.run import CASES
+    from src.config import load_config
+
+    types = {n: a.config_type for n, a in CASES.items()}
+    sizes = {}
+    for path in sorted(glob.glob(os.path.join(PKG, "configs", "*.toml"))):
+        cfg = load_config(path, types)
+        app = CASES[cfg.case.name](cfg)
+        arrays = app.create_mhd_particles()
+        sizes[cfg.case.name] = len(arrays["x"])
+        assert np.all(np.isfinite(arrays["e"])) and np.all(arrays["h"] > 0)
+    assert sizes["orstang2d"] == 128 * 128
+    assert sizes["mhdblast3d"] == 128 ** 3
+    assert sizes["alfven2d"] == 64 * 128
+    assert 294_000 < sizes["mhdshock2d"] < 296_000  # 4096 x 128 left + 8:1 right
+
+
+@pytest.mark.skipif(not os.path.isdir(REFERENCE_CONFIGS), reason="reference checkout not present")
+def test_reference_toml_files_load_unchanged():
+    from src.config import SimulationConfig, load_config
+
+    for path in sorted(glob.glob(os.path.join(REFERENCE_CONFIGS, "*.toml"))):
+        if "jet" in os.path.basename(path):
+            continue  # the jet case has its own schema (out of scope)
+        name = os.path.basename(path)[:-5]
+        cfg = load_config(path, {name: SimulationConfig})
+        assert cfg.numerics.dim is None and cfg.execution.precision is None
+
+
+def test_scheme_groups_compile_to_kernel_parameters():
+    from src.config import load_config
+    from src.run import CASES
+    from src.scheme import MHDScheme, compile_groups
+
+    types = {n: a.config_type for n, a in CASES.items()}
+    cfg = load_config(os.path.join(PKG, "configs", "mhdblast3d.toml"), types)
+    scheme = MHDScheme(cfg)
+    groups = scheme.get_equations()
+    assert [type(e).__name__ for g in groups for e in g.equations][:3] == [
+        "DensityIteration", "SmoothingLengthRateFromDensityRelation", "DensityFromSmoothingLength"]
+    p = compile_groups(groups)
+    assert p["hfact"] == 1.2 and p["dim"] == 3 and p["iterate"] and p["min_iter"] == 2 and p["max_iter"] == 250
+    assert p["gamma"] == cfg.physics.gamma and abs(p["timestep_factor"] - 1.0) < 1e-15
+    with pytest.raises(NotImplementedError):
+        compile_groups(groups[:5] + groups[6:])
+
+
+def test_config_rejects_unknown_keys_and_bad_types(tmp_path):
+    from src.config import SimulationConfig, load_config
+
+    good = open(os.path.join(PKG, "configs", "orstang2d.toml")).read()
+    bad1 = good.replace("nx = 128", "nx = 128\nbogus = 1")
+    bad2 = good.replace("gamma = 1.6666666666666667", "gamma = 2")
+    for k, text in enumerate((bad1, bad2)):
+        p = tmp_path / f"c{k}.toml"
+        p.write_text(text)
+        with pytest.raises(ValueError):
+            load_config(p, {"orstang2d": SimulationConfig})

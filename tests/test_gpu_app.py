@@ -1,0 +1,56 @@
+"""The reference-facing path end to end: TOML -> case -> MHDApplication.run().
+
+``src.run.main`` mirrors ``python -m src.run <config>`` (src/run.py:32-39):
+the application warms up, takes the initial dt and runs MHDSolver.solve with
+the literal PEC step; the result must match the oracle driven the same way.
+"""
+
+import os
+
+import numpy as np
+import pytest
+
+pytest.importorskip("torch")
+
+import oracle  # noqa: E402
+from compare import assert_close, scales  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+PKG = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "pysph-mhd_b200")
+
+
+def _small_config(tmp_path, name, nx, steps, extra=""):
+    text = open(os.path.join(PKG, "configs", f"{name}.toml")).read()
+    text = text.replace("max_steps = 100", f"max_steps = {steps}").replace("max_steps = 50", f"max_steps = {steps}")
+    import re
+
+    text = re.sub(r"nx = \d+", f"nx = {nx}", text)
+    text = text.replace('directory = "outputs/', f'directory = "{tmp_path}/')
+    p = tmp_path / f"{name}.toml"
+    p.write_text(text + extra)
+    return str(p)
+
+
+def test_run_blast3d_config_matches_oracle(tmp_path):
+    from src.run import main
+
+    path = _small_config(tmp_path, "mhdblast3d", 12, 3)
+    text = open(path).read().replace('precision = "fp32"', 'precision = "fp64"')
+    open(path, "w").write(text)
+    app, pa = main([path])
+    got = pa.pull("x", "u", "v", "rho", "e", "Bx", "By", "alpha1", "h", order="gid")
+    assert app.solver.count == 3
+
+    ic = app.create_mhd_particles()
+    ic["gid"] = np.arange(len(ic["x"]), dtype=float)
+    prm = app.scheme.kernel_params(app.create_domain(), app.tf)
+    s = oracle.State(ic)
+    o = oracle.Oracle(prm, exact_order=False)
+    o.warmup(s)
+    o.run(s, 3, tf=app.tf)
+    ref = {k: s[k] for k in got if k != "gid"}
+    assert_close(got, ref, list(ref), 1e-8, scales(ic, s["cs"]), None, "src.run mhdblast3d")
+    # output dumps: initial, final
+    dumps = sorted(os.listdir(os.path.join(tmp_path, "mhdblast3d")))
+    assert dumps[0].endswith("000000.npz") and dumps[-1].endswith("000003.npz")
