@@ -244,7 +244,19 @@ int plan_grid(Ctx* c, const MhdState* s, int n, cudaStream_t st) {
     if (dev_alloc(c, &c->cell_start, want) != MHD_OK) return MHD_ERR_CUDA;
     c->cell_cap = want;
   }
+  g.cell_base = 0;
+  g.cut = cutoff;
+  for (int a = 0; a < 3; a++) {
+    g.periodic[a] = P.periodic[a];
+    g.L[a] = P.L[a];
+    g.half[a] = P.half[a];
+  }
   c->grid = g;
+  c->key_cells = g.ncells;
+  // The stream was synchronised above, so the previous upload of the staging
+  // copy has completed.
+  c->h_grids[0] = g;
+  CK(cudaMemcpyAsync(c->d_grids, c->h_grids, sizeof(Grid), cudaMemcpyHostToDevice, st));
   c->have_grid = true;
   return MHD_OK;
 }
@@ -516,6 +528,9 @@ int mhd_ctx_create(const MhdParams* params, int64_t n_max, void** out) {
          ensure_list_storage(c, cap) == MHD_OK;
   }
   if (ok && cudaMallocHost((void**)&c->h_sc, sizeof(DevScalars)) != cudaSuccess) ok = false;
+  ok = ok && dev_alloc(c, &c->d_grids, 1) == MHD_OK;
+  if (ok && cudaMallocHost((void**)&c->h_grids, sizeof(Grid)) != cudaSuccess) ok = false;
+  if (ok) c->grid_slots = 1;
   if (!ok) {
     g_err = c->err.empty() ? "workspace allocation failed" : c->err;
     mhd_ctx_destroy(c);
@@ -563,6 +578,9 @@ int mhd_ctx_destroy(void* ctx) {
   }
   cudaFree(c->d_sc);
   if (c->h_sc) cudaFreeHost(c->h_sc);
+  cudaFree(c->d_grids);
+  if (c->h_grids) cudaFreeHost(c->h_grids);
+  cudaFree(c->inst);
   delete c;
   return MHD_OK;
 }

@@ -56,15 +56,17 @@ __global__ void __launch_bounds__(256) k_reduce_hbox(int n, const double* __rest
 
 // --------------------------------------------------------------- cell keys
 template <int DIM>
-__global__ void __launch_bounds__(256) k_cell_keys(int n, Grid g, const double* __restrict__ x,
+__global__ void __launch_bounds__(256) k_cell_keys(int n, const Grid* __restrict__ grids,
+                                                   const int* __restrict__ inst, const double* __restrict__ x,
                                                    const double* __restrict__ y, const double* __restrict__ z,
                                                    uint32_t* __restrict__ keys, int32_t* __restrict__ vals) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  const Grid& g = grid_of(grids, inst, i);
   const int cx = cell_coord(g, 0, x[i]);
   const int cy = cell_coord(g, 1, y[i]);
   const int cz = DIM == 3 ? cell_coord(g, 2, z[i]) : 0;
-  keys[i] = (uint32_t)((cz * g.nc[1] + cy) * g.nc[0] + cx);
+  keys[i] = (uint32_t)(g.cell_base + (cz * g.nc[1] + cy) * g.nc[0] + cx);
   vals[i] = i;
 }
 
@@ -220,12 +222,14 @@ __global__ void __launch_bounds__(256) k_cell_starts(int n, int ncells, const ui
 // cell widths) plus h, and the cell coordinates packed into one int: the
 // FP32 geometry of a pair is (pos_i - pos_j) + (cell_i - cell_j) * cell width.
 template <int DIM>
-__global__ void __launch_bounds__(256) k_pack_positions(int n, Grid g, const double* __restrict__ x,
+__global__ void __launch_bounds__(256) k_pack_positions(int n, const Grid* __restrict__ grids,
+                                                        const int* __restrict__ inst, const double* __restrict__ x,
                                                         const double* __restrict__ y, const double* __restrict__ z,
                                                         const double* __restrict__ h, float4* __restrict__ posf,
                                                         int* __restrict__ cellc) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  const Grid& g = grid_of(grids, inst, i);
   const int cx = cell_coord(g, 0, x[i]);
   const int cy = cell_coord(g, 1, y[i]);
   const int cz = DIM == 3 ? cell_coord(g, 2, z[i]) : 0;
@@ -239,9 +243,11 @@ __global__ void __launch_bounds__(256) k_pack_positions(int n, Grid g, const dou
 void launch_pack_positions(Ctx* c, const MhdState* s, int n, cudaStream_t st) {
   if (n <= 0) return;
   if (c->P.dim == 3)
-    k_pack_positions<3><<<(n + 255) / 256, 256, 0, st>>>(n, c->grid, s->x, s->y, s->z, s->h, c->posf, c->cellc);
+    k_pack_positions<3><<<(n + 255) / 256, 256, 0, st>>>(n, c->d_grids, c->inst, s->x, s->y, s->z, s->h, c->posf,
+                                                         c->cellc);
   else
-    k_pack_positions<2><<<(n + 255) / 256, 256, 0, st>>>(n, c->grid, s->x, s->y, s->z, s->h, c->posf, c->cellc);
+    k_pack_positions<2><<<(n + 255) / 256, 256, 0, st>>>(n, c->d_grids, c->inst, s->x, s->y, s->z, s->h, c->posf,
+                                                         c->cellc);
   c->launches++;
 }
 
@@ -288,20 +294,20 @@ void launch_reduce_hbox(Ctx* c, const MhdState* s, int n, cudaStream_t st) {
   c->launches++;
 }
 
-// Sort the particles by cell of `c->grid`; leaves perm (sorted slot ->
-// source index) in c->perm and the cell table in c->cell_start.
+// Sort the particles by cell of their instance's grid (keys are
+// cell_base + linear cell); leaves perm (sorted slot -> source index) in
+// c->perm and the cell table (c->key_cells + 1 entries) in c->cell_start.
 void launch_sort_cells(Ctx* c, const MhdState* s, int n, cudaStream_t st) {
-  const Grid& g = c->grid;
   const int nb = ceil_div(n, 256);
   if (n > 0) {
     if (c->P.dim == 3)
-      k_cell_keys<3><<<nb, 256, 0, st>>>(n, g, s->x, s->y, s->z, c->keys[0], c->vals[0]);
+      k_cell_keys<3><<<nb, 256, 0, st>>>(n, c->d_grids, c->inst, s->x, s->y, s->z, c->keys[0], c->vals[0]);
     else
-      k_cell_keys<2><<<nb, 256, 0, st>>>(n, g, s->x, s->y, s->z, c->keys[0], c->vals[0]);
+      k_cell_keys<2><<<nb, 256, 0, st>>>(n, c->d_grids, c->inst, s->x, s->y, s->z, c->keys[0], c->vals[0]);
     c->launches++;
   }
   int bits = 1;
-  while ((1LL << bits) < (int64_t)g.ncells) bits++;
+  while ((1LL << bits) < (int64_t)c->key_cells) bits++;
   const int passes = (bits + 7) / 8;
   const int sb = max_sort_blocks(n);
   int cur = 0;
@@ -316,7 +322,7 @@ void launch_sort_cells(Ctx* c, const MhdState* s, int n, cudaStream_t st) {
   }
   c->sorted_keys = c->keys[cur];
   c->perm = c->vals[cur];
-  k_cell_starts<<<ceil_div(n + 1, 256), 256, 0, st>>>(n, g.ncells, c->sorted_keys, c->cell_start);
+  k_cell_starts<<<ceil_div(n + 1, 256), 256, 0, st>>>(n, c->key_cells, c->sorted_keys, c->cell_start);
   c->launches++;
 }
 

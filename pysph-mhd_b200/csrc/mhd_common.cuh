@@ -1,4 +1,4 @@
-// mhd_common.cuh -- device-side parameters, SPH kernels and neighbour-test
+// mhd_common.cuh -- device-side parameters, SPH kernels and neighbour-grid
 // helpers shared by the sm_100a kernels of the SPMHD particle update.
 #pragma once
 
@@ -10,33 +10,44 @@
 
 namespace mhd {
 
-constexpr double kDensityTolerance = 1.0e-4;          // src/equations.py:6
-constexpr double kCourantFactor = 0.3;                // src/equations.py:7
-constexpr double kForceFactor = 0.25;                 // src/equations.py:8
-constexpr double kPairDistanceEpsilon = 1.0e-12;      // src/equations.py:9
+constexpr double kDensityTolerance = 1.0e-4;            // src/equations.py:6
+constexpr double kCourantFactor = 0.3;                  // src/equations.py:7
+constexpr double kForceFactor = 0.25;                   // src/equations.py:8
+constexpr double kPairDistanceEpsilon = 1.0e-12;        // src/equations.py:9
 constexpr double kInteractionDistanceEpsilon = 1.0e-8;  // src/equations.py:10
 constexpr double kFloatTiny = 2.2250738585072014e-308;  // src/equations.py:11
 constexpr double kMachineEps = 2.220446049250313e-16;   // src/equations.py:67
-constexpr double kBigNumber = 1.0e29;                 // src/equations.py:574
+constexpr double kBigNumber = 1.0e29;                   // src/equations.py:574
 
-// Uniform cell grid over the box; cells along x are contiguous in the sorted
-// particle order, so a row of neighbouring cells is one index range.
+// One instance's uniform cell grid and periodic box (a batch holds one per
+// instance, indexed by the particle's instance; a single simulation is
+// instance 0).  Cells along x are contiguous in the sorted particle order.
 struct Grid {
   int nc[3];
   int ncells;
+  int cell_base;  // first global cell key of the instance
+  int sw;         // stencil half-width in cells: widths >= cut-off / sw
+  int periodic[3];
   double lo[3];
   double inv_cs[3];
   double cs[3];
+  double L[3];  // the instance's periodic box (lo .. lo + L on periodic axes)
+  double half[3];
   double h_plan;  // every h must stay <= h_plan for the grid to be valid
+  double cut;     // list cut-off R * h_max * (1 + margin)
   float csf[3];   // cell widths in FP32 (packed-position geometry)
-  int sw;         // stencil half-width in cells: widths >= cut-off / sw
 };
+
+__device__ __forceinline__ const Grid& grid_of(const Grid* __restrict__ grids, const int* __restrict__ inst, int i) {
+  return grids[inst ? inst[i] : 0];
+}
 
 // Compacted neighbour lists: entry k of particle i lives at
 // idx[((i / 32) * cap + k) * 32 + i % 32], so the 32 lanes of a warp read
 // entry k of their particles from one 128-byte line.  A list holds every j
 // with r_ij < R * max(h_i, h_j) * (1 + margin) for the h it was built with;
-// hlim[i] = h_i * (1 + margin) is the largest h_i it stays valid for.
+// hlim[i] (slightly below h_i * (1 + margin)) is the largest h_i it stays
+// valid for.
 struct NbrList {
   const int* idx;
   const int* cnt;
@@ -44,7 +55,7 @@ struct NbrList {
   int cap;
 };
 
-// Everything a kernel needs, passed by value.
+// Everything a kernel needs besides the grids, passed by value.
 struct DevParams {
   int dim;
   int kernel;
@@ -65,23 +76,23 @@ struct DevParams {
 
 // Device-resident scalars of one context (status, reductions, step clock).
 struct DevScalars {
-  double dt;         // step size in use (stage2 of the current step)
-  double dt_next;    // next step size (min dt_adapt, clipped to tf)
-  double t;          // time at the start of the current step
-  double t_next;     // time at the start of the next step
+  double dt;       // step size in use (stage2 of the current step)
+  double dt_next;  // next step size (min dt_adapt, clipped to tf)
+  double t;        // time at the start of the current step
+  double t_next;   // time at the start of the next step
   unsigned long long dt_min_bits;  // atomicMin target (positive doubles order as integers)
   unsigned long long h_max_bits;
-  unsigned long long lo_bits[3];   // bounding box (non-periodic axes), order-mapped
+  unsigned long long lo_bits[3];  // bounding box (non-periodic axes), order-mapped
   unsigned long long hi_bits[3];
-  int status;        // first device error, MHD_OK if none
-  int replan;        // an h outgrew the grid's h_plan during the density passes
-  int relist;        // an h outgrew its neighbour list, or a list overflowed
-  int list_max;      // longest neighbour list met by the last build
-  int passes_done;   // density passes executed in the current group evaluation
-  unsigned int ticket;  // last-block counter of the dt reduction
+  int status;       // first device error, MHD_OK if none
+  int relist;       // an h outgrew its neighbour list, or a list overflowed
+  int list_max;     // longest neighbour list met by the last build
+  int passes_done;  // density passes executed in the current group evaluation
+  unsigned int ticket;              // last-block counter of the dt reduction
+  int events;                       // batched steps that met a relist / overflow / pass cap
   unsigned long long n_pairs;       // force-pass neighbour pairs (accumulating)
   unsigned long long n_candidates;  // force-pass distance tests (accumulating)
-  int n_unconverged[256 + 8];  // per density pass
+  int n_unconverged[256 + 8];       // per density pass
 };
 
 // ------------------------------------------------------------ kernels (SPH)
@@ -139,11 +150,6 @@ __device__ __forceinline__ void w_dw(T q, int dim, T& w, T& dw) {
   }
 }
 
-template <int K>
-__host__ __device__ constexpr double radius_scale() {
-  return (K == MHD_KERNEL_QUINTIC || K == MHD_KERNEL_GAUSSIAN || K == MHD_KERNEL_SUPER_GAUSSIAN) ? 3.0 : 2.0;
-}
-
 inline double radius_scale_of(int k) {
   return (k == MHD_KERNEL_QUINTIC || k == MHD_KERNEL_GAUSSIAN || k == MHD_KERNEL_SUPER_GAUSSIAN) ? 3.0 : 2.0;
 }
@@ -154,12 +160,6 @@ template <int DIM>
 __device__ __forceinline__ double pow_dim(double a) {
   if constexpr (DIM == 2) return a * a;
   else return a * a * a;
-}
-
-// sigma_d / h^d
-template <int DIM>
-__device__ __forceinline__ double hfac(double norm, double h1) {
-  return norm * pow_dim<DIM>(h1);
 }
 
 // Minimum-image displacement along one periodic axis.
@@ -205,77 +205,6 @@ __device__ __forceinline__ int cell_coord(const Grid& g, int a, double x) {
   return c;
 }
 
-// Up to two index ranges covering the x-row of cells (cx-1..cx+1) at (cy, cz).
-struct RowRanges {
-  int b0, e0, b1, e1;
-};
-
-__device__ __forceinline__ RowRanges row_ranges(const Grid& g, const int* __restrict__ cell_start, int row, int cx,
-                                                int periodic_x) {
-  RowRanges r;
-  const int nx = g.nc[0];
-  const int base = row * nx;
-  r.b1 = 0;
-  r.e1 = 0;
-  if (nx < 3) {
-    r.b0 = cell_start[base];
-    r.e0 = cell_start[base + nx];
-    return r;
-  }
-  int lo = cx - 1, hi = cx + 1;
-  if (lo < 0) {
-    if (periodic_x) {
-      r.b1 = cell_start[base + nx - 1];
-      r.e1 = cell_start[base + nx];
-    }
-    lo = 0;
-  }
-  if (hi >= nx) {
-    if (periodic_x) {
-      r.b1 = cell_start[base];
-      r.e1 = cell_start[base + 1];
-    }
-    hi = nx - 1;
-  }
-  r.b0 = cell_start[base + lo];
-  r.e0 = cell_start[base + hi + 1];
-  return r;
-}
-
-}  // namespace mhd
-
-namespace mhd {
-
-// Visits every particle index j in the 3^DIM cells around (xi, yi, zi):
-// per (y, z) row one or two contiguous ranges of the cell-sorted order.
-template <int DIM, class F>
-__device__ __forceinline__ void for_each_candidate(const Grid& G, const DevParams& P, const int* __restrict__ cell_start,
-                                                   double xi, double yi, double zi, F&& f) {
-  const int cx = cell_coord(G, 0, xi);
-  const int cy = cell_coord(G, 1, yi);
-  const int cz = DIM == 3 ? cell_coord(G, 2, zi) : 0;
-  const int ny = G.nc[1], nz = G.nc[2];
-  const int zlo = (DIM == 3 && nz > 1) ? -1 : 0, zhi = (DIM == 3 && nz > 1) ? 1 : 0;
-  const int ylo = ny > 1 ? -1 : 0, yhi = ny > 1 ? 1 : 0;
-  for (int oz = zlo; oz <= zhi; oz++) {
-    int zc = cz + oz;
-    if (zc < 0 || zc >= nz) {
-      if (!P.periodic[2]) continue;
-      zc = zc < 0 ? zc + nz : zc - nz;
-    }
-    for (int oy = ylo; oy <= yhi; oy++) {
-      int yc = cy + oy;
-      if (yc < 0 || yc >= ny) {
-        if (!P.periodic[1]) continue;
-        yc = yc < 0 ? yc + ny : yc - ny;
-      }
-      const RowRanges r = row_ranges(G, cell_start, zc * ny + yc, cx, P.periodic[0]);
-      for (int j = r.b0; j < r.e0; j++) f(j);
-      for (int j = r.b1; j < r.e1; j++) f(j);
-    }
-  }
-}
-
 // Cell coordinates in one int: 11/11/10 bits in 3-D, 16/16 in 2-D.
 template <int DIM>
 __device__ __forceinline__ int pack_cell(int cx, int cy, int cz) {
@@ -311,25 +240,25 @@ __device__ __forceinline__ int cell_delta(int d, int nc, int periodic) {
 // cells (scanned whole) can hold pairs nc/2 cells apart, whose image the
 // offset does not decide, so it takes the FP32 minimum image.
 template <int DIM>
-__device__ __forceinline__ void rel_dx(const Grid& G, const DevParams& P, const float4& pi, int ci, const float4& pj,
-                                       int cj, float& dx, float& dy, float& dz) {
+__device__ __forceinline__ void rel_dx(const Grid& G, const float4& pi, int ci, const float4& pj, int cj, float& dx,
+                                       float& dy, float& dz) {
   int xi, yi, zi, xj, yj, zj;
   unpack_cell<DIM>(ci, xi, yi, zi);
   unpack_cell<DIM>(cj, xj, yj, zj);
-  dx = (pi.x - pj.x) + (float)cell_delta(xi - xj, G.nc[0], P.periodic[0]) * G.csf[0];
-  dy = (pi.y - pj.y) + (float)cell_delta(yi - yj, G.nc[1], P.periodic[1]) * G.csf[1];
-  dz = DIM == 3 ? (pi.z - pj.z) + (float)cell_delta(zi - zj, G.nc[2], P.periodic[2]) * G.csf[2] : 0.f;
+  dx = (pi.x - pj.x) + (float)cell_delta(xi - xj, G.nc[0], G.periodic[0]) * G.csf[0];
+  dy = (pi.y - pj.y) + (float)cell_delta(yi - yj, G.nc[1], G.periodic[1]) * G.csf[1];
+  dz = DIM == 3 ? (pi.z - pj.z) + (float)cell_delta(zi - zj, G.nc[2], G.periodic[2]) * G.csf[2] : 0.f;
   const int whole = 2 * G.sw + 1;
-  if (P.periodic[0] && G.nc[0] < whole) {
-    const float L = (float)P.L[0], hL = 0.5f * L;
+  if (G.periodic[0] && G.nc[0] < whole) {
+    const float L = (float)G.L[0], hL = 0.5f * L;
     dx = dx > hL ? dx - L : (dx < -hL ? dx + L : dx);
   }
-  if (P.periodic[1] && G.nc[1] < whole) {
-    const float L = (float)P.L[1], hL = 0.5f * L;
+  if (G.periodic[1] && G.nc[1] < whole) {
+    const float L = (float)G.L[1], hL = 0.5f * L;
     dy = dy > hL ? dy - L : (dy < -hL ? dy + L : dy);
   }
-  if (DIM == 3 && P.periodic[2] && G.nc[2] < whole) {
-    const float L = (float)P.L[2], hL = 0.5f * L;
+  if (DIM == 3 && G.periodic[2] && G.nc[2] < whole) {
+    const float L = (float)G.L[2], hL = 0.5f * L;
     dz = dz > hL ? dz - L : (dz < -hL ? dz + L : dz);
   }
 }
@@ -341,9 +270,8 @@ __device__ __forceinline__ void rel_dx(const Grid& G, const DevParams& P, const 
 // trimmed to [x - cut, x + cut].  Axes with fewer than 2*sw+1 cells are
 // scanned whole with their own coordinates (no image selection).
 template <int DIM, class F>
-__device__ __forceinline__ void for_each_cell_trimmed(const Grid& G, const DevParams& P,
-                                                      const int* __restrict__ cell_start, double xi, double yi,
-                                                      double zi, double cut, F&& f) {
+__device__ __forceinline__ void for_each_cell_trimmed(const Grid& G, const int* __restrict__ cell_start, double xi,
+                                                      double yi, double zi, double cut, F&& f) {
   const int sw = G.sw, whole = 2 * sw + 1;
   const int nx = G.nc[0], ny = G.nc[1], nz = G.nc[2];
   const int cy = cell_coord(G, 1, yi);
@@ -355,7 +283,7 @@ __device__ __forceinline__ void for_each_cell_trimmed(const Grid& G, const DevPa
   } else {
     xl = (int)floor((xi - cut - G.lo[0]) * G.inv_cs[0]);
     xh = (int)floor((xi + cut - G.lo[0]) * G.inv_cs[0]);
-    if (!P.periodic[0]) {
+    if (!G.periodic[0]) {
       xl = xl < 0 ? 0 : xl;
       xh = xh >= nx ? nx - 1 : xh;
     }
@@ -372,7 +300,7 @@ __device__ __forceinline__ void for_each_cell_trimmed(const Grid& G, const DevPa
       dzm = zi < c_lo ? c_lo - zi : (zi > c_hi ? zi - c_hi : 0.0);
       if (dzm * dzm >= cut2) continue;
       if (zc < 0 || zc >= nz) {
-        if (!P.periodic[2]) continue;
+        if (!G.periodic[2]) continue;
         zc = zc < 0 ? zc + nz : zc - nz;
       }
     }
@@ -383,11 +311,11 @@ __device__ __forceinline__ void for_each_cell_trimmed(const Grid& G, const DevPa
         const double dym = yi < c_lo ? c_lo - yi : (yi > c_hi ? yi - c_hi : 0.0);
         if (dym * dym + dzm * dzm >= cut2) continue;
         if (yc < 0 || yc >= ny) {
-          if (!P.periodic[1]) continue;
+          if (!G.periodic[1]) continue;
           yc = yc < 0 ? yc + ny : yc - ny;
         }
       }
-      const int base = (zc * ny + yc) * nx;
+      const int base = G.cell_base + (zc * ny + yc) * nx;
       int xw = xl < 0 ? xl + nx : xl;
       int jb = cell_start[base + xw];
       for (int xu = xl; xu <= xh; xu++) {
@@ -401,73 +329,6 @@ __device__ __forceinline__ void for_each_cell_trimmed(const Grid& G, const DevPa
           xw = next;
           jb = je;
         }
-      }
-    }
-  }
-}
-
-// Visits every j in the cells within `cut` of (xi, yi, zi), per particle:
-// rows (y, z) whose cells lie farther than `cut` are skipped and each row's
-// x-range is trimmed to [x - cut, x + cut] (one or two contiguous ranges of
-// the cell-sorted order).  Requires cell widths >= cut / G.sw.
-template <int DIM, class F>
-__device__ __forceinline__ void for_each_candidate_trimmed(const Grid& G, const DevParams& P,
-                                                           const int* __restrict__ cell_start, double xi, double yi,
-                                                           double zi, double cut, F&& f) {
-  const int sw = G.sw;
-  const int nx = G.nc[0], ny = G.nc[1], nz = G.nc[2];
-  const int cy = cell_coord(G, 1, yi);
-  const int cz = DIM == 3 ? cell_coord(G, 2, zi) : 0;
-  // x-range of cells (unwrapped), trimmed to the cut-off
-  int xl, xh;
-  if (nx < 2 * sw + 1) {
-    xl = 0;
-    xh = nx - 1;
-  } else {
-    xl = (int)floor((xi - cut - G.lo[0]) * G.inv_cs[0]);
-    xh = (int)floor((xi + cut - G.lo[0]) * G.inv_cs[0]);
-    if (!P.periodic[0]) {
-      xl = xl < 0 ? 0 : xl;
-      xh = xh >= nx ? nx - 1 : xh;
-    }
-  }
-  const double cut2 = cut * cut;
-  const int zsw = (DIM == 3 && nz > 1) ? (nz < 2 * sw + 1 ? -1 : sw) : 0;
-  const int ysw = ny > 1 ? (ny < 2 * sw + 1 ? -1 : sw) : 0;
-  const int zlo = zsw < 0 ? 0 : cz - zsw, zhi = zsw < 0 ? nz - 1 : cz + zsw;
-  const int ylo = ysw < 0 ? 0 : cy - ysw, yhi = ysw < 0 ? ny - 1 : cy + ysw;
-  for (int zc0 = zlo; zc0 <= zhi; zc0++) {
-    int zc = zc0;
-    double dzm = 0.0;
-    if (DIM == 3 && zsw > 0) {
-      const double c_lo = G.lo[2] + zc0 * G.cs[2], c_hi = c_lo + G.cs[2];
-      dzm = zi < c_lo ? c_lo - zi : (zi > c_hi ? zi - c_hi : 0.0);
-      if (dzm * dzm >= cut2) continue;
-      if (zc < 0 || zc >= nz) {
-        if (!P.periodic[2]) continue;
-        zc = zc < 0 ? zc + nz : zc - nz;
-      }
-    }
-    for (int yc0 = ylo; yc0 <= yhi; yc0++) {
-      int yc = yc0;
-      if (ysw > 0) {
-        const double c_lo = G.lo[1] + yc0 * G.cs[1], c_hi = c_lo + G.cs[1];
-        const double dym = yi < c_lo ? c_lo - yi : (yi > c_hi ? yi - c_hi : 0.0);
-        if (dym * dym + dzm * dzm >= cut2) continue;
-        if (yc < 0 || yc >= ny) {
-          if (!P.periodic[1]) continue;
-          yc = yc < 0 ? yc + ny : yc - ny;
-        }
-      }
-      const int base = (zc * ny + yc) * nx;
-      if (xl < 0) {
-        for (int j = cell_start[base + xl + nx]; j < cell_start[base + nx]; j++) f(j);
-        for (int j = cell_start[base]; j < cell_start[base + xh + 1]; j++) f(j);
-      } else if (xh >= nx) {
-        for (int j = cell_start[base + xl]; j < cell_start[base + nx]; j++) f(j);
-        for (int j = cell_start[base]; j < cell_start[base + xh - nx + 1]; j++) f(j);
-      } else {
-        for (int j = cell_start[base + xl]; j < cell_start[base + xh + 1]; j++) f(j);
       }
     }
   }

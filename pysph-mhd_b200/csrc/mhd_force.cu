@@ -75,7 +75,8 @@ struct ForceRecords {
   const V4<T>* r[6];
   const float4* posf;     // packed FP32 positions (geometry of the FP32 form)
   const int* cellc;
-  Grid G;
+  const Grid* grids;  // per-instance geometry
+  const int* inst;    // instance of each particle (null: one instance)
 };
 
 template <class T>
@@ -137,6 +138,7 @@ __global__ void __launch_bounds__(kForceShapes[SHAPE][0], kForceShapes[SHAPE][1]
     k_force_pass(int n, DevParams P, NbrList L, ForceRecords<T> R, ForceOut<T> o, DevScalars* sc) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  const Grid& G = grid_of(R.grids, R.inst, i);
   const V4<double> pi = R.pos[i];
   const V4<T> i0 = R.r[0][i], i1 = R.r[1][i], i2 = R.r[2][i], i3 = R.r[3][i], i4 = R.r[4][i], i5 = R.r[5][i];
   const double xi = pi.x, yi = pi.y, zi = DIM == 3 ? pi.z : 0.0, hi = pi.w;
@@ -178,7 +180,7 @@ __global__ void __launch_bounds__(kForceShapes[SHAPE][0], kForceShapes[SHAPE][1]
     if constexpr (sizeof(T) == 4) {
       // FP32 geometry from the packed positions; FP32 neighbour test
       const float4 pj = __ldg(R.posf + j);
-      rel_dx<DIM>(R.G, P, pif, cif, pj, __ldg(R.cellc + j), dx, dy, dz);
+      rel_dx<DIM>(G, pif, cif, pj, __ldg(R.cellc + j), dx, dy, dz);
       const float r2 = dx * dx + dy * dy + dz * dz;
       const float rh = Rf * fmaxf(pif.w, pj.w);
       if (!(r2 < rh * rh)) continue;
@@ -187,9 +189,9 @@ __global__ void __launch_bounds__(kForceShapes[SHAPE][0], kForceShapes[SHAPE][1]
     } else {
       // FP64 geometry and the exact neighbour test of the oracle
       const V4<double> pj = ld4(R.pos + j);
-      const double dxd = min_image(xi - pj.x, P.L[0], P.half[0], P.periodic[0]);
-      const double dyd = min_image(yi - pj.y, P.L[1], P.half[1], P.periodic[1]);
-      const double dzd = DIM == 3 ? min_image(zi - pj.z, P.L[2], P.half[2], P.periodic[2]) : 0.0;
+      const double dxd = min_image(xi - pj.x, G.L[0], G.half[0], G.periodic[0]);
+      const double dyd = min_image(yi - pj.y, G.L[1], G.half[1], G.periodic[1]);
+      const double dzd = DIM == 3 ? min_image(zi - pj.z, G.L[2], G.half[2], G.periodic[2]) : 0.0;
       const double r2d = r2_exact(dxd, dyd, dzd);
       if (!(r2d < rhi2 || r2d < rh2_exact(P.R, pj.w))) continue;
       dx = dxd;
@@ -431,7 +433,8 @@ static ForceRecords<T> records(Ctx* c) {
   for (int k = 0; k < 6; k++) R.r[k] = reinterpret_cast<const V4<T>*>(c->rec[k]);
   R.posf = c->posf;
   R.cellc = c->cellc;
-  R.G = c->grid;
+  R.grids = c->d_grids;
+  R.inst = c->inst;
   return R;
 }
 

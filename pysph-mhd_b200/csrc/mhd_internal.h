@@ -33,7 +33,13 @@ struct GatherSet {
 struct Ctx {
   MhdParams params;
   DevParams P;
-  Grid grid;
+  Grid grid;                // host copy of instance 0's grid
+  Grid* d_grids = nullptr;  // device grid table, one entry per instance
+  Grid* h_grids = nullptr;  // pinned staging copy of d_grids
+  int grid_slots = 0;       // entries allocated in d_grids / h_grids
+  int* inst = nullptr;      // instance of each particle; null = one instance
+  int n_inst = 1;
+  int key_cells = 0;        // cells over all instances (the sort key range)
   bool have_grid = false;
   int64_t n_max = 0;
   int device = 0;

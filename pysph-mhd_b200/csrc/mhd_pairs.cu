@@ -49,7 +49,8 @@ __global__ void __launch_bounds__(128) k_density_pass(int n, int pass, DevParams
                                                       const double* __restrict__ h_in, double* __restrict__ h_out,
                                                       const double* __restrict__ h0, double* __restrict__ rho_sum,
                                                       double* __restrict__ omega, double* __restrict__ converged,
-                                                      Grid G, const float4* __restrict__ posf,
+                                                      const Grid* __restrict__ grids, const int* __restrict__ inst,
+                                                      const float4* __restrict__ posf,
                                                       const int* __restrict__ cellc, DevScalars* sc) {
   // Stop when the iterated group already stopped after pass `pass` (1-based
   // count), or when the neighbour lists no longer cover the current h.
@@ -68,6 +69,7 @@ __global__ void __launch_bounds__(128) k_density_pass(int n, int pass, DevParams
     h_out[i] = hi;
     return;
   }
+  const Grid& G = grid_of(grids, inst, i);
   const double xi = x[i], yi = y[i], zi = DIM == 3 ? z[i] : 0.0;
   const T h1 = (T)(1.0 / hi);
   const T fac = (T)P.norm * (DIM == 2 ? h1 * h1 : h1 * h1 * h1);
@@ -93,7 +95,7 @@ __global__ void __launch_bounds__(128) k_density_pass(int n, int pass, DevParams
     bool nb;
     if constexpr (sizeof(T) == 4) {
       float dx, dy, dz;
-      rel_dx<DIM>(G, P, pif, cif, __ldg(posf + j), __ldg(cellc + j), dx, dy, dz);
+      rel_dx<DIM>(G, pif, cif, __ldg(posf + j), __ldg(cellc + j), dx, dy, dz);
       const float r2 = dx * dx + dy * dy + dz * dz;
       nb = r2 < rhi2f;
       if (!compact && !nb) {
@@ -102,9 +104,9 @@ __global__ void __launch_bounds__(128) k_density_pass(int n, int pass, DevParams
       }
       r = r2 > 0.f ? r2 * rsqrtf(r2) : 0.f;
     } else {
-      const double dx = min_image(xi - x[j], P.L[0], P.half[0], P.periodic[0]);
-      const double dy = min_image(yi - y[j], P.L[1], P.half[1], P.periodic[1]);
-      const double dz = DIM == 3 ? min_image(zi - z[j], P.L[2], P.half[2], P.periodic[2]) : 0.0;
+      const double dx = min_image(xi - x[j], G.L[0], G.half[0], G.periodic[0]);
+      const double dy = min_image(yi - y[j], G.L[1], G.half[1], G.periodic[1]);
+      const double dz = DIM == 3 ? min_image(zi - z[j], G.L[2], G.half[2], G.periodic[2]) : 0.0;
       const double r2 = r2_exact(dx, dy, dz);
       // For compact kernels a pair admitted only by R*h_j has W(h_i) = 0 and
       // dW/dh(h_i) = 0, so the h_i test alone gives the same sums.
@@ -161,15 +163,17 @@ __global__ void __launch_bounds__(128) k_density_pass(int n, int pass, DevParams
 // only up to h_i * (1 + margin) * (1 - 1e-4): every pair the exact FP64
 // criterion admits while each h stays within its limit is in the list.
 template <int DIM>
-__global__ void __launch_bounds__(128) k_build_lists(int n, DevParams P, Grid G, const int* __restrict__ cell_start,
+__global__ void __launch_bounds__(128) k_build_lists(int n, DevParams P, const Grid* __restrict__ grids,
+                                                     const int* __restrict__ inst, const int* __restrict__ cell_start,
                                                      const double* __restrict__ x, const double* __restrict__ y,
                                                      const double* __restrict__ z, const double* __restrict__ h,
                                                      const float4* __restrict__ posf, const int* __restrict__ cellc,
-                                                     double cut, float grow, int cap, int* __restrict__ idx,
+                                                     float grow, int cap, int* __restrict__ idx,
                                                      int* __restrict__ cnt_out, double* __restrict__ hlim,
                                                      DevScalars* sc) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  const Grid& G = grid_of(grids, inst, i);
   const float4 pi = posf[i];
   const float Rg = (float)P.R * grow;
   const float rhi = Rg * pi.w, rhi2 = rhi * rhi;
@@ -178,17 +182,18 @@ __global__ void __launch_bounds__(128) k_build_lists(int n, DevParams P, Grid G,
   int cnt = 0;
   int cxi, cyi, czi;
   unpack_cell<DIM>(cellc[i], cxi, cyi, czi);
-  // Per cell (unwrapped coordinates ox, oy, oz) the in-cell position of i
-  // shifted by the cell offset; a candidate then costs one float4 load.
+  // Per cell (unwrapped coordinates) the in-cell position of i shifted by
+  // the cell offset; a candidate then costs one float4 load.
   const int whole = 2 * G.sw + 1;
-  const bool mx = P.periodic[0] && G.nc[0] < whole, my = P.periodic[1] && G.nc[1] < whole,
-             mz = DIM == 3 && P.periodic[2] && G.nc[2] < whole;
-  const float Lx = (float)P.L[0], Ly = (float)P.L[1], Lz = (float)P.L[2];
-  for_each_cell_trimmed<DIM>(G, P, cell_start, x[i], y[i], DIM == 3 ? z[i] : 0.0, cut,
+  const bool mx = G.periodic[0] && G.nc[0] < whole, my = G.periodic[1] && G.nc[1] < whole,
+             mz = DIM == 3 && G.periodic[2] && G.nc[2] < whole;
+  const float Lx = (float)G.L[0], Ly = (float)G.L[1], Lz = (float)G.L[2];
+  const float csx = G.csf[0], csy = G.csf[1], csz = G.csf[2];
+  for_each_cell_trimmed<DIM>(G, cell_start, x[i], y[i], DIM == 3 ? z[i] : 0.0, G.cut * (1.0 + 1e-6),
                              [&](int cxu, int cyu, int czu, int jb, int je) {
-    const float sx = pi.x + (float)(cxi - cxu) * G.csf[0];
-    const float sy = pi.y + (float)(cyi - cyu) * G.csf[1];
-    const float sz = DIM == 3 ? pi.z + (float)(czi - czu) * G.csf[2] : 0.f;
+    const float sx = pi.x + (float)(cxi - cxu) * csx;
+    const float sy = pi.y + (float)(cyi - cyu) * csy;
+    const float sz = DIM == 3 ? pi.z + (float)(czi - czu) * csz : 0.f;
     for (int j = jb; j < je; j++) {
       const float4 pj = __ldg(posf + j);
       float dx = sx - pj.x, dy = sy - pj.y, dz = DIM == 3 ? sz - pj.z : 0.f;
@@ -214,11 +219,14 @@ __global__ void __launch_bounds__(128) k_build_lists(int n, DevParams P, Grid G,
 // Neighbours of each particle under the exact FP64 rule of the oracle
 // (r2 < (R h_i)^2 or r2 < (R h_j)^2, self included), counted over its list.
 template <int DIM>
-__global__ void __launch_bounds__(128) k_neighbour_counts(int n, DevParams P, NbrList L, const double* __restrict__ x,
-                                                          const double* __restrict__ y, const double* __restrict__ z,
-                                                          const double* __restrict__ h, int* __restrict__ out) {
+__global__ void __launch_bounds__(128) k_neighbour_counts(int n, DevParams P, const Grid* __restrict__ grids,
+                                                          const int* __restrict__ inst, NbrList L,
+                                                          const double* __restrict__ x, const double* __restrict__ y,
+                                                          const double* __restrict__ z, const double* __restrict__ h,
+                                                          int* __restrict__ out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  const Grid& G = grid_of(grids, inst, i);
   const double xi = x[i], yi = y[i], zi = DIM == 3 ? z[i] : 0.0;
   const double rhi2 = rh2_exact(P.R, h[i]);
   const int cnt = L.cnt[i];
@@ -226,9 +234,9 @@ __global__ void __launch_bounds__(128) k_neighbour_counts(int n, DevParams P, Nb
   int nb = 0;
   for (int k = 0; k < cnt; k++) {
     const int j = row[k * 32];
-    const double dx = min_image(xi - x[j], P.L[0], P.half[0], P.periodic[0]);
-    const double dy = min_image(yi - y[j], P.L[1], P.half[1], P.periodic[1]);
-    const double dz = DIM == 3 ? min_image(zi - z[j], P.L[2], P.half[2], P.periodic[2]) : 0.0;
+    const double dx = min_image(xi - x[j], G.L[0], G.half[0], G.periodic[0]);
+    const double dy = min_image(yi - y[j], G.L[1], G.half[1], G.periodic[1]);
+    const double dz = DIM == 3 ? min_image(zi - z[j], G.L[2], G.half[2], G.periodic[2]) : 0.0;
     const double r2 = r2_exact(dx, dy, dz);
     nb += (r2 < rhi2 || r2 < rh2_exact(P.R, h[j])) ? 1 : 0;
   }
@@ -238,9 +246,11 @@ __global__ void __launch_bounds__(128) k_neighbour_counts(int n, DevParams P, Nb
 void launch_neighbour_counts(Ctx* c, const MhdState* s, int n, int* out, cudaStream_t st) {
   if (n <= 0) return;
   if (c->P.dim == 3)
-    k_neighbour_counts<3><<<(n + 127) / 128, 128, 0, st>>>(n, c->P, c->lists(), s->x, s->y, s->z, s->h, out);
+    k_neighbour_counts<3><<<(n + 127) / 128, 128, 0, st>>>(n, c->P, c->d_grids, c->inst, c->lists(), s->x, s->y,
+                                                           s->z, s->h, out);
   else
-    k_neighbour_counts<2><<<(n + 127) / 128, 128, 0, st>>>(n, c->P, c->lists(), s->x, s->y, s->z, s->h, out);
+    k_neighbour_counts<2><<<(n + 127) / 128, 128, 0, st>>>(n, c->P, c->d_grids, c->inst, c->lists(), s->x, s->y,
+                                                           s->z, s->h, out);
   c->launches++;
 }
 
@@ -248,14 +258,13 @@ void launch_build_lists(Ctx* c, const MhdState* s, int n, cudaStream_t st) {
   if (n <= 0) return;
   TimedScope ts(c, MHD_TIMING_CELLS, st);
   const float grow = (float)(1.0 + c->list_margin);
-  const double cut = c->list_cut * (1.0 + 1e-6);
   if (c->P.dim == 3)
-    k_build_lists<3><<<(n + 127) / 128, 128, 0, st>>>(n, c->P, c->grid, c->cell_start, s->x, s->y, s->z, s->h,
-                                                     c->posf, c->cellc, cut, grow, c->list_cap, c->nbr_idx,
+    k_build_lists<3><<<(n + 127) / 128, 128, 0, st>>>(n, c->P, c->d_grids, c->inst, c->cell_start, s->x, s->y, s->z,
+                                                     s->h, c->posf, c->cellc, grow, c->list_cap, c->nbr_idx,
                                                      c->nbr_cnt, c->nbr_hlim, c->d_sc);
   else
-    k_build_lists<2><<<(n + 127) / 128, 128, 0, st>>>(n, c->P, c->grid, c->cell_start, s->x, s->y, s->z, s->h,
-                                                     c->posf, c->cellc, cut, grow, c->list_cap, c->nbr_idx,
+    k_build_lists<2><<<(n + 127) / 128, 128, 0, st>>>(n, c->P, c->d_grids, c->inst, c->cell_start, s->x, s->y, s->z,
+                                                     s->h, c->posf, c->cellc, grow, c->list_cap, c->nbr_idx,
                                                      c->nbr_cnt, c->nbr_hlim, c->d_sc);
   c->launches++;
 }
@@ -266,12 +275,12 @@ static void density_launch(Ctx* c, MhdState* s, int n, int pass, const double* h
   if (c->P.fp32) {
     k_density_pass<K, DIM, float><<<(n + 127) / 128, 128, 0, st>>>(n, pass, c->P, c->lists(), s->x, s->y, s->z, s->m,
                                                                    h_in, h_out, s->h0, s->rho_sum, s->omega,
-                                                                   s->converged, c->grid, c->posf, c->cellc, c->d_sc);
+                                                                   s->converged, c->d_grids, c->inst, c->posf, c->cellc, c->d_sc);
     return;
   }
   k_density_pass<K, DIM, double><<<(n + 127) / 128, 128, 0, st>>>(n, pass, c->P, c->lists(), s->x, s->y, s->z, s->m,
                                                                   h_in, h_out, s->h0, s->rho_sum, s->omega,
-                                                                  s->converged, c->grid, c->posf, c->cellc, c->d_sc);
+                                                                  s->converged, c->d_grids, c->inst, c->posf, c->cellc, c->d_sc);
 }
 
 #define MHD_DISPATCH(FN, ...)                                                   \
