@@ -34,6 +34,7 @@ extern "C" {
 #define MHD_ERR_NONFINITE (-4)      /* NaN/Inf met in the timestep reduction */
 #define MHD_ERR_CAPACITY (-5)       /* cell grid larger than the supported maximum */
 #define MHD_ERR_NO_DEVICE (-6)      /* no CUDA device, or not sm_100 */
+#define MHD_ERR_RELIST (-7)         /* a captured run met a list rebuild: its state is invalid, replay it uncaptured */
 
 /* Kernel ids: the reference's kernel map, src/scheme.py:48-56. */
 #define MHD_KERNEL_CUBIC 0
@@ -231,6 +232,57 @@ int mhd_corrector_predictor(void* ctx, MhdState* s, int64_t n, int32_t mode, dou
    RHS, stage2, wrap) on `src`; the result is in `dst` (particle order
    changes with the neighbour sort).  dt < 0 uses the device dt. */
 int mhd_step(void* ctx, MhdState* src, MhdState* dst, int64_t n, double dt, MhdRhsStats* stats, void* stream);
+
+/* ---- batched form and captured runs ----
+   No counterpart in the reference, which advances one case per Application
+   (src/application.py) with its solver loop (src/solver.py:35-76). */
+
+/* Declares the first start[n_inst] particles of the context as n_inst
+   independent instances stored one after another: instance k holds
+   [start[k], start[k+1]) (start[0] = 0, every instance non-empty).  The
+   instances share the parameters and the domain; each keeps its own grid,
+   clock and timestep, and its results equal a run of the instance alone
+   while its grid stays within capacity.  Plans every grid from `s`
+   (synchronising) and fixes its cell capacity at ceil(cells * cell_headroom)
+   per axis (1 <= cell_headroom <= 16); from then on grids are planned on the
+   device within those capacities (coarser cells when h shrinks further),
+   without host synchronisation.  n_inst = 1 puts a single simulation on the
+   device planner.  Resets every clock to t = dt = 0 and drops captured
+   runs. */
+int mhd_ctx_set_instances(void* ctx, const MhdState* s, int32_t n_inst, const int64_t* start, double cell_headroom,
+                          void* stream);
+int32_t mhd_instance_count(void* ctx);
+
+/* Clocks of all instances, t[n_inst] and dt[n_inst] in host memory
+   (synchronising).  mhd_clock_set / mhd_clock_get address instance 0. */
+int mhd_clock_set_all(void* ctx, const double* t, const double* dt, void* stream);
+int mhd_clock_get_all(void* ctx, double* t, double* dt, void* stream);
+
+/* `steps` fused PEC steps on the device clocks: per step the right-hand side
+   from the current state into the other buffer set, the per-instance
+   timestep (tf clip per instance), then the fused corrector-predictor
+   (mode 1 on the last step when `finish`, else 3).  The state starts in
+   `a`; the sorted fields ping-pong between `a` and `b` (mhd_cells_build's
+   src and dst), so after an odd number of steps it is in `b`.
+   capture = 0 runs step by step with the host-checked density iteration
+   and list rebuilds of mhd_rhs.  capture = 1 (after mhd_ctx_set_instances)
+   captures the steps once into a CUDA graph -- cached per buffers, step
+   count and context configuration -- and launches them as one graph: each
+   density iteration runs min(max_iter, 8) passes with the on-device stop
+   test, and nothing synchronises until the run ends.  A captured run whose
+   lists stopped covering an h (or overflowed), or whose density iteration
+   had not stopped after its captured passes, returns MHD_ERR_RELIST: its
+   state is invalid; restore the input state and clocks and replay the run
+   with capture = 0. */
+int mhd_advance(void* ctx, MhdState* a, MhdState* b, int64_t n, int32_t steps, int32_t finish, int32_t capture,
+                void* stream);
+
+/* Autotuner hook: cells >= list cut-off / stencil wide (stencil 1..3) and the
+   force pass's launch shape (0..3: 128x2, 128x3, 128x4, 256x2 threads x
+   minimum resident blocks; -1 = per-precision default).  Drops captured
+   runs; a batched context re-plans its capacities at the next
+   mhd_ctx_set_instances. */
+int mhd_ctx_tune(void* ctx, int32_t stencil, int32_t force_shape);
 
 #ifdef __cplusplus
 }

@@ -164,93 +164,66 @@ int build_gather(const MhdState* src, MhdState* dst, GatherSet& g) {
   return k;
 }
 
-// h_max and bounding box -> uniform grid with cells >= R * h_max * margin.
-int plan_grid(Ctx* c, const MhdState* s, int n, cudaStream_t st) {
-  DevScalars init;
-  CK(cudaMemcpyAsync(c->h_sc, c->d_sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, st));
-  CK(cudaStreamSynchronize(st));
-  init = *c->h_sc;
-  init.h_max_bits = 0ULL;
+void refresh_spec(Ctx* c) {
+  PlanSpec& S = c->spec;
+  const DevParams& P = c->P;
+  S.dim = P.dim;
+  S.stencil = c->stencil;
   for (int a = 0; a < 3; a++) {
-    init.lo_bits[a] = ~0ULL;
-    init.hi_bits[a] = 0ULL;
+    S.periodic[a] = P.periodic[a];
+    S.lo[a] = P.lo[a];
+    S.L[a] = P.L[a];
+    S.half[a] = P.half[a];
   }
-  *c->h_sc = init;
-  CK(cudaMemcpyAsync(c->d_sc, c->h_sc, sizeof(DevScalars), cudaMemcpyHostToDevice, st));
+  S.R = P.R;
+  S.grid_margin = c->grid_margin;
+  S.list_margin = c->list_margin;
+}
+
+int grow_cell_table(Ctx* c, int64_t cells) {
+  if (cells + 1 <= c->cell_cap) return MHD_OK;
+  if (c->cell_start) cudaFree(c->cell_start);
+  c->cell_start = nullptr;
+  c->cell_cap = 0;
+  const int64_t want = cells + 1 + (cells >> 2);
+  if (dev_alloc(c, &c->cell_start, want) != MHD_OK) return MHD_ERR_CUDA;
+  c->cell_cap = want;
+  c->generation++;
+  return MHD_OK;
+}
+
+// h_max and bounding box -> uniform grid with cells >= R * h_max * margin.
+// A single simulation plans on the host (the cell table grows as needed);
+// a batched context plans every instance on the device, within the cell
+// capacities fixed when its instances were set, with no synchronisation.
+int plan_grid(Ctx* c, const MhdState* s, int n, cudaStream_t st) {
+  refresh_spec(c);
+  if (c->batched) {
+    launch_reduce_hbox(c, s, n, st);
+    launch_plan_grids(c, st);
+    CK(cudaGetLastError());
+    c->have_grid = true;
+    return MHD_OK;
+  }
   launch_reduce_hbox(c, s, n, st);
   CK(cudaGetLastError());
-  CK(cudaMemcpyAsync(c->h_sc, c->d_sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(c->h_inst, c->d_inst, sizeof(InstScalars), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(&c->h_sc->status, &c->d_sc->status, sizeof(int), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
-  const DevScalars& h = *c->h_sc;
-  if (h.status != MHD_OK) FAIL(h.status, "non-finite or non-positive smoothing length");
-  const double hmax = n > 0 ? dbl_unorder(h.h_max_bits) : 1.0;
-  const DevParams& P = c->P;
-  const double cutoff = P.R * hmax * c->grid_margin * (1.0 + c->list_margin);
+  launch_reset_hbox(c, st);
+  if (c->h_sc->status != MHD_OK) FAIL(c->h_sc->status, "non-finite or non-positive smoothing length");
+  const InstScalars& q = *c->h_inst;
+  double lo[3], hi[3];
+  for (int a = 0; a < 3; a++) {
+    lo[a] = dbl_unorder(q.lo_bits[a]);
+    hi[a] = dbl_unorder(q.hi_bits[a]);
+  }
   Grid g;
-  memset(&g, 0, sizeof g);
-  double extent[3];
-  for (int a = 0; a < 3; a++) {
-    if (a >= P.dim) {
-      g.nc[a] = 1;
-      g.lo[a] = 0.0;
-      extent[a] = 1.0;
-      continue;
-    }
-    double lo, ext;
-    if (P.periodic[a]) {
-      lo = P.lo[a];
-      ext = P.L[a];
-    } else {
-      lo = n > 0 ? dbl_unorder(h.lo_bits[a]) : 0.0;
-      const double hi = n > 0 ? dbl_unorder(h.hi_bits[a]) : 1.0;
-      ext = (hi - lo) * (1.0 + 1e-12) + 1e-300;
-    }
-    if (!isfinite(lo) || !isfinite(ext)) FAIL(MHD_ERR_NONFINITE, "non-finite particle position");
-    // packed cell coordinates hold 11/11/10 bits in 3-D, 16/16 in 2-D
-    const double axis_max = P.dim == 3 ? (a == 2 ? 1023.0 : 2047.0) : 65535.0;
-    double ncd = floor(ext * c->stencil / cutoff);
-    int nc = ncd < 1.0 ? 1 : (ncd > axis_max ? (int)axis_max : (int)ncd);
-    g.nc[a] = nc;
-    g.lo[a] = lo;
-    extent[a] = ext;
-  }
-  // Keep the table within 2^24 cells; coarser cells stay valid.
-  const int64_t cap = (int64_t)1 << 24;
-  while ((int64_t)g.nc[0] * g.nc[1] * g.nc[2] > cap) {
-    int a = 0;
-    for (int b = 1; b < 3; b++)
-      if (g.nc[b] > g.nc[a]) a = b;
-    g.nc[a] = std::max(1, (int)(g.nc[a] * 0.8));
-  }
-  // The stencil of +-stencil cells covers the cut-off on every axis with at
-  // least 2*stencil+1 cells; smaller axes are scanned whole.
-  double hplan = INFINITY;
-  g.sw = c->stencil;
-  for (int a = 0; a < 3; a++) {
-    g.cs[a] = extent[a] / g.nc[a];
-    g.csf[a] = (float)g.cs[a];
-    g.inv_cs[a] = a < P.dim ? 1.0 / g.cs[a] : 0.0;
-    const bool limits = a < P.dim && g.nc[a] >= 2 * g.sw + 1;
-    if (limits) hplan = std::min(hplan, g.sw * g.cs[a] / (P.R * (1.0 + c->list_margin)) * (1.0 - 1e-9));
-  }
-  g.h_plan = hplan;
-  c->list_cut = cutoff;
-  g.ncells = g.nc[0] * g.nc[1] * g.nc[2];
-  if ((int64_t)g.ncells + 1 > c->cell_cap) {
-    if (c->cell_start) cudaFree(c->cell_start);
-    c->cell_start = nullptr;
-    c->cell_cap = 0;
-    const int64_t want = (int64_t)g.ncells + 1 + (g.ncells >> 2);
-    if (dev_alloc(c, &c->cell_start, want) != MHD_OK) return MHD_ERR_CUDA;
-    c->cell_cap = want;
-  }
+  if (plan_instance(c->spec, n, dbl_unorder(q.h_max_bits), lo, hi, nullptr, g) != MHD_OK)
+    FAIL(MHD_ERR_NONFINITE, "non-finite particle position");
   g.cell_base = 0;
-  g.cut = cutoff;
-  for (int a = 0; a < 3; a++) {
-    g.periodic[a] = P.periodic[a];
-    g.L[a] = P.L[a];
-    g.half[a] = P.half[a];
-  }
+  c->list_cut = g.cut;
+  if (grow_cell_table(c, g.ncells) != MHD_OK) return MHD_ERR_CUDA;
   c->grid = g;
   c->key_cells = g.ncells;
   // The stream was synchronised above, so the previous upload of the staging
@@ -258,6 +231,49 @@ int plan_grid(Ctx* c, const MhdState* s, int n, cudaStream_t st) {
   c->h_grids[0] = g;
   CK(cudaMemcpyAsync(c->d_grids, c->h_grids, sizeof(Grid), cudaMemcpyHostToDevice, st));
   c->have_grid = true;
+  return MHD_OK;
+}
+
+// (Re)allocate the per-instance tables for n_inst instances whose particles
+// start at start[0..n_inst] and reset their clocks and reductions.  The
+// instance index array is left to the caller.
+int alloc_instances(Ctx* c, int n_inst, const int64_t* start) {
+  if (n_inst > c->grid_slots) {
+    cudaFree(c->d_grids);
+    cudaFree(c->d_inst);
+    cudaFree(c->d_stage);
+    if (c->h_grids) cudaFreeHost(c->h_grids);
+    if (c->h_inst) cudaFreeHost(c->h_inst);
+    c->d_grids = nullptr;
+    c->d_inst = nullptr;
+    c->d_stage = nullptr;
+    c->h_grids = nullptr;
+    c->h_inst = nullptr;
+    c->grid_slots = 0;
+    if (dev_alloc(c, &c->d_grids, n_inst) != MHD_OK || dev_alloc(c, &c->d_inst, n_inst) != MHD_OK ||
+        dev_alloc(c, &c->d_stage, 2 * n_inst) != MHD_OK)
+      return MHD_ERR_CUDA;
+    if (cudaMallocHost((void**)&c->h_grids, sizeof(Grid) * n_inst) != cudaSuccess ||
+        cudaMallocHost((void**)&c->h_inst, sizeof(InstScalars) * n_inst) != cudaSuccess)
+      FAIL(MHD_ERR_CUDA, "pinned allocation failed");
+    c->grid_slots = n_inst;
+    c->generation++;
+  }
+  for (int k = 0; k < n_inst; k++) {
+    InstScalars& q = c->h_inst[k];
+    memset(&q, 0, sizeof q);
+    q.dt_min_bits = ~0ULL;
+    q.h_max_bits = 0ULL;
+    for (int a = 0; a < 3; a++) {
+      q.lo_bits[a] = ~0ULL;
+      q.hi_bits[a] = 0ULL;
+      q.nc_cap[a] = 1;
+    }
+    q.n = (int)(start[k + 1] - start[k]);
+  }
+  CK(cudaMemcpy(c->d_inst, c->h_inst, sizeof(InstScalars) * n_inst, cudaMemcpyHostToDevice));
+  c->n_inst = n_inst;
+  c->inst_start.assign(start, start + n_inst + 1);
   return MHD_OK;
 }
 
@@ -269,6 +285,7 @@ int ensure_list_storage(Ctx* c, int cap) {
   c->list_cap = 0;
   if (dev_alloc(c, &c->nbr_idx, c->n_pad * (int64_t)cap) != MHD_OK) return MHD_ERR_CUDA;
   c->list_cap = cap;
+  c->generation++;
   return MHD_OK;
 }
 
@@ -426,7 +443,7 @@ int density_iterate(Ctx* c, MhdState* s, int n, MhdRhsStats* stats, cudaStream_t
     stats->density_passes = c->h_sc->passes_done;
     stats->grid_rebuilds += rebuilds;
     stats->n_unconverged = unconv;
-    stats->n_cells = c->grid.ncells;
+    stats->n_cells = c->batched ? c->key_cells : c->grid.ncells;
   }
   return MHD_OK;
 }
@@ -452,6 +469,89 @@ int read_status(Ctx* c, cudaStream_t st) {
     FAIL(code, "device reported a non-finite value (timestep or smoothing length)");
   }
   return MHD_OK;
+}
+
+// Right-hand side with nothing that synchronises (batched contexts): device
+// planning, sort and lists, a fixed number of density passes with their
+// on-device stop test, the force pass.  Lists that stop covering an h, or a
+// group that has not stopped after the captured passes, raise relist or an
+// event that the caller reads after the run.
+int rhs_captured(Ctx* c, const MhdState* src, MhdState* dst, int n, cudaStream_t st) {
+  int rc = plan_grid(c, src, n, st);
+  if (rc != MHD_OK) return rc;
+  rc = sort_into(c, src, dst, n, st);
+  if (rc != MHD_OK) return rc;
+  CK(cudaMemsetAsync(&c->d_sc->n_unconverged[0], 0, sizeof(c->d_sc->n_unconverged), st));
+  CK(cudaMemsetAsync(&c->d_sc->passes_done, 0, sizeof(int), st));
+  double* buf[2] = {dst->h, c->h_alt};
+  const int passes = std::min(c->P.max_iter, c->graph_passes);
+  for (int k = 0; k < passes; k++) launch_density_pass(c, dst, n, k, buf[k & 1], buf[(k + 1) & 1], st);
+  launch_finish_density(c, dst, n, passes, st);
+  launch_force_prologue(c, dst, n, st);
+  launch_force_pass(c, dst, n, st);
+  CK(cudaGetLastError());
+  return MHD_OK;
+}
+
+// One fused step on the device clocks: the right-hand side from cur into
+// nxt, the per-instance timestep, the corrector-predictor on nxt.
+int step_fused(Ctx* c, const MhdState* cur, MhdState* nxt, int n, int mode, bool captured, cudaStream_t st) {
+  int rc;
+  if (captured) {
+    rc = rhs_captured(c, cur, nxt, n, st);
+  } else {
+    rc = plan_grid(c, cur, n, st);
+    if (rc == MHD_OK) rc = sort_into(c, cur, nxt, n, st);
+    if (rc == MHD_OK) rc = density_iterate(c, nxt, n, nullptr, st);
+    if (rc == MHD_OK) rc = force_pass(c, nxt, n, st);
+  }
+  if (rc != MHD_OK) return rc;
+  launch_dt_reduce(c, nxt, n, -1.0, st);
+  launch_corrector_predictor(c, nxt, n, mode, -1.0, -1.0, st);
+  CK(cudaGetLastError());
+  return MHD_OK;
+}
+
+// Capture `steps` fused steps (a -> b -> a ...) into an executable graph.
+int capture_run(Ctx* c, MhdState* a, MhdState* b, int n, int steps, int finish, Ctx::GraphEntry& e) {
+  if (!c->cap_stream) CK(cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking));
+  const cudaStream_t cs = c->cap_stream;
+  const bool timing = c->timing;
+  const int64_t l0 = c->launches;
+  c->timing = false;
+  CK(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+  int rc = MHD_OK;
+  for (int k = 0; k < steps && rc == MHD_OK; k++) {
+    const MhdState* cur = (k & 1) ? b : a;
+    MhdState* nxt = (k & 1) ? a : b;
+    const int mode = (finish && k == steps - 1) ? 1 : 3;
+    rc = step_fused(c, cur, nxt, n, mode, true, cs);
+  }
+  cudaGraph_t g = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(cs, &g);
+  c->timing = timing;
+  e.launches = c->launches - l0;
+  c->launches = l0;
+  if (rc != MHD_OK) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (ce != cudaSuccess) FAIL(MHD_ERR_CUDA, std::string("stream capture failed: ") + cudaGetErrorString(ce));
+  const cudaError_t ie = cudaGraphInstantiate(&e.exec, g, 0ULL);
+  cudaGraphDestroy(g);
+  if (ie != cudaSuccess) FAIL(MHD_ERR_CUDA, std::string("graph instantiation failed: ") + cudaGetErrorString(ie));
+  e.a = *a;
+  e.b = *b;
+  e.n = n;
+  e.steps = steps;
+  e.finish = finish;
+  e.generation = c->generation;
+  return MHD_OK;
+}
+
+void drop_graphs(Ctx* c) {
+  for (auto& e : c->graphs) cudaGraphExecDestroy(e.exec);
+  c->graphs.clear();
 }
 
 inline cudaStream_t S(void* stream) { return (cudaStream_t)stream; }
@@ -528,16 +628,14 @@ int mhd_ctx_create(const MhdParams* params, int64_t n_max, void** out) {
          ensure_list_storage(c, cap) == MHD_OK;
   }
   if (ok && cudaMallocHost((void**)&c->h_sc, sizeof(DevScalars)) != cudaSuccess) ok = false;
-  ok = ok && dev_alloc(c, &c->d_grids, 1) == MHD_OK;
-  if (ok && cudaMallocHost((void**)&c->h_grids, sizeof(Grid)) != cudaSuccess) ok = false;
-  if (ok) c->grid_slots = 1;
+  const int64_t one[2] = {0, N};
+  ok = ok && alloc_instances(c, 1, one) == MHD_OK;
   if (!ok) {
     g_err = c->err.empty() ? "workspace allocation failed" : c->err;
     mhd_ctx_destroy(c);
     return MHD_ERR_CUDA;
   }
   memset(c->h_sc, 0, sizeof(DevScalars));
-  c->h_sc->dt_min_bits = ~0ULL;
   if (cudaMemcpy(c->d_sc, c->h_sc, sizeof(DevScalars), cudaMemcpyHostToDevice) != cudaSuccess) {
     g_err = "workspace initialisation failed";
     mhd_ctx_destroy(c);
@@ -546,6 +644,7 @@ int mhd_ctx_create(const MhdParams* params, int64_t n_max, void** out) {
   if (const char* m = getenv("MHD_GRID_MARGIN")) c->grid_margin = std::max(1.0, atof(m));
   if (const char* m = getenv("MHD_FORCE_SHAPE")) c->force_shape = std::max(0, std::min(3, atoi(m)));
   if (const char* m = getenv("MHD_STENCIL")) c->stencil = std::max(1, std::min(3, atoi(m)));
+  if (const char* m = getenv("MHD_GRAPH_PASSES")) c->graph_passes = std::max(1, std::min(256, atoi(m)));
   *out = c;
   return MHD_OK;
 }
@@ -581,6 +680,11 @@ int mhd_ctx_destroy(void* ctx) {
   cudaFree(c->d_grids);
   if (c->h_grids) cudaFreeHost(c->h_grids);
   cudaFree(c->inst);
+  cudaFree(c->d_inst);
+  if (c->h_inst) cudaFreeHost(c->h_inst);
+  cudaFree(c->d_stage);
+  drop_graphs(c);
+  if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
   delete c;
   return MHD_OK;
 }
@@ -588,6 +692,7 @@ int mhd_ctx_destroy(void* ctx) {
 int mhd_ctx_set_params(void* ctx, const MhdParams* params) {
   Ctx* c = (Ctx*)ctx;
   if (!c) return MHD_ERR_INVALID;
+  c->generation++;
   return fill_params(c, params);
 }
 
@@ -703,10 +808,10 @@ int mhd_timestep(void* ctx, const MhdState* s, int64_t n, double t, double* dt_h
   launch_dt_reduce(c, s, (int)n, t, st);
   CK(cudaGetLastError());
   if (dt_host) {
-    CK(cudaMemcpyAsync(&c->h_sc->dt_next, &c->d_sc->dt_next, sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&c->h_inst->dt_next, &c->d_inst->dt_next, sizeof(double), cudaMemcpyDeviceToHost, st));
     int rc = read_status(c, st);
     if (rc != MHD_OK) return rc;
-    *dt_host = c->h_sc->dt_next;
+    *dt_host = c->h_inst->dt_next;
   }
   return MHD_OK;
 }
@@ -724,9 +829,10 @@ int mhd_clock_get(void* ctx, double* t, double* dt, void* stream) {
   if (!c) return MHD_ERR_INVALID;
   const cudaStream_t st = S(stream);
   CK(cudaMemcpyAsync(c->h_sc, c->d_sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(c->h_inst, c->d_inst, sizeof(InstScalars), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
-  if (t) *t = c->h_sc->t;
-  if (dt) *dt = c->h_sc->dt;
+  if (t) *t = c->h_inst->t;
+  if (dt) *dt = c->h_inst->dt;
   if (c->h_sc->status != MHD_OK) return read_status(c, st);
   return MHD_OK;
 }
@@ -791,6 +897,184 @@ int mhd_step(void* ctx, MhdState* src, MhdState* dst, int64_t n, double dt, MhdR
   rc = mhd_step_stage2(ctx, dst, n, dt, stream);
   if (rc != MHD_OK) return rc;
   (void)st;
+  return MHD_OK;
+}
+
+// ------------------------------------------------------------ batched form
+int mhd_ctx_set_instances(void* ctx, const MhdState* s, int32_t n_inst, const int64_t* start, double cell_headroom,
+                          void* stream) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return MHD_ERR_INVALID;
+  if (n_inst < 1 || !start) FAIL(MHD_ERR_INVALID, "n_inst must be >= 1 and start non-null");
+  if (start[0] != 0) FAIL(MHD_ERR_INVALID, "start[0] must be 0");
+  for (int k = 0; k < n_inst; k++)
+    if (start[k + 1] <= start[k]) FAIL(MHD_ERR_INVALID, "every instance needs at least one particle");
+  const int64_t n = start[n_inst];
+  if (n > c->n_max) FAIL(MHD_ERR_INVALID, "instances exceed the context's n_max");
+  if (!(cell_headroom >= 1.0 && cell_headroom <= 16.0)) FAIL(MHD_ERR_INVALID, "cell_headroom must be in [1, 16]");
+  if (!check_state(c, s, false)) return MHD_ERR_INVALID;
+  const cudaStream_t st = S(stream);
+  CK(cudaStreamSynchronize(st));
+  drop_graphs(c);
+  c->batched = false;
+  int rc = alloc_instances(c, n_inst, start);
+  if (rc != MHD_OK) return rc;
+  cudaFree(c->inst);
+  c->inst = nullptr;
+  if (n_inst > 1) {
+    if (dev_alloc(c, &c->inst, c->n_max) != MHD_OK) return MHD_ERR_CUDA;
+    std::vector<int> idx((size_t)n);
+    for (int k = 0; k < n_inst; k++)
+      for (int64_t i = start[k]; i < start[k + 1]; i++) idx[(size_t)i] = k;
+    CK(cudaMemcpy(c->inst, idx.data(), sizeof(int) * (size_t)n, cudaMemcpyHostToDevice));
+  }
+  // Plan every instance on the host once to fix its cell capacity.
+  refresh_spec(c);
+  launch_reduce_hbox(c, s, (int)n, st);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(c->h_inst, c->d_inst, sizeof(InstScalars) * n_inst, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(&c->h_sc->status, &c->d_sc->status, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (c->h_sc->status != MHD_OK) {
+    CK(cudaMemsetAsync(&c->d_sc->status, 0, sizeof(int), st));
+    FAIL(MHD_ERR_NONFINITE, "non-finite or non-positive smoothing length");
+  }
+  const double axis_max[3] = {c->P.dim == 3 ? 2047.0 : 65535.0, c->P.dim == 3 ? 2047.0 : 65535.0,
+                              c->P.dim == 3 ? 1023.0 : 1.0};
+  int64_t base = 0;
+  for (int k = 0; k < n_inst; k++) {
+    InstScalars& q = c->h_inst[k];
+    double lo[3], hi[3];
+    for (int a = 0; a < 3; a++) {
+      lo[a] = dbl_unorder(q.lo_bits[a]);
+      hi[a] = dbl_unorder(q.hi_bits[a]);
+    }
+    Grid g;
+    if (plan_instance(c->spec, q.n, dbl_unorder(q.h_max_bits), lo, hi, nullptr, g) != MHD_OK)
+      FAIL(MHD_ERR_NONFINITE, "non-finite particle position");
+    int64_t cells = 1;
+    for (int a = 0; a < 3; a++) {
+      const double want = a < c->P.dim ? ceil(g.nc[a] * cell_headroom) : 1.0;
+      q.nc_cap[a] = (int)std::min(axis_max[a], std::max(1.0, want));
+      cells *= q.nc_cap[a];
+    }
+    if (cells > ((int64_t)1 << 24)) {
+      cells = 1;
+      for (int a = 0; a < 3; a++) {
+        q.nc_cap[a] = g.nc[a];
+        cells *= g.nc[a];
+      }
+    }
+    q.cell_base = (int)base;
+    base += cells;
+    if (base > ((int64_t)1 << 30)) FAIL(MHD_ERR_CAPACITY, "instances need more than 2^30 cells");
+    q.h_max_bits = 0ULL;
+    for (int a = 0; a < 3; a++) {
+      q.lo_bits[a] = ~0ULL;
+      q.hi_bits[a] = 0ULL;
+    }
+    q.dt_min_bits = ~0ULL;
+    if (k == 0) {
+      g.cell_base = 0;
+      c->grid = g;
+    }
+  }
+  CK(cudaMemcpy(c->d_inst, c->h_inst, sizeof(InstScalars) * n_inst, cudaMemcpyHostToDevice));
+  if (grow_cell_table(c, base) != MHD_OK) return MHD_ERR_CUDA;
+  c->key_cells = (int)base;
+  c->batched = true;
+  c->generation++;
+  return MHD_OK;
+}
+
+int mhd_clock_set_all(void* ctx, const double* t, const double* dt, void* stream) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return MHD_ERR_INVALID;
+  if (!t || !dt) FAIL(MHD_ERR_INVALID, "t and dt must be non-null");
+  const cudaStream_t st = S(stream);
+  CK(cudaStreamSynchronize(st));
+  CK(cudaMemcpy(c->d_stage, t, sizeof(double) * c->n_inst, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->d_stage + c->n_inst, dt, sizeof(double) * c->n_inst, cudaMemcpyHostToDevice));
+  launch_clock_load(c, st);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(st));
+  return MHD_OK;
+}
+
+int mhd_clock_get_all(void* ctx, double* t, double* dt, void* stream) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return MHD_ERR_INVALID;
+  if (!t || !dt) FAIL(MHD_ERR_INVALID, "t and dt must be non-null");
+  const cudaStream_t st = S(stream);
+  launch_clock_store(c, st);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(st));
+  CK(cudaMemcpy(t, c->d_stage, sizeof(double) * c->n_inst, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(dt, c->d_stage + c->n_inst, sizeof(double) * c->n_inst, cudaMemcpyDeviceToHost));
+  return read_status(c, st);
+}
+
+int32_t mhd_instance_count(void* ctx) { return ctx ? ((Ctx*)ctx)->n_inst : 0; }
+
+int mhd_ctx_tune(void* ctx, int32_t stencil, int32_t force_shape) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return MHD_ERR_INVALID;
+  if (stencil < 1 || stencil > 3) FAIL(MHD_ERR_INVALID, "stencil must be 1, 2 or 3");
+  if (force_shape < -1 || force_shape > 3) FAIL(MHD_ERR_INVALID, "force_shape must be in -1..3");
+  c->stencil = stencil;
+  c->force_shape = force_shape;
+  drop_graphs(c);
+  c->generation++;
+  return MHD_OK;
+}
+
+int mhd_advance(void* ctx, MhdState* a, MhdState* b, int64_t n, int32_t steps, int32_t finish, int32_t capture,
+                void* stream) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return MHD_ERR_INVALID;
+  if (n < 1 || n > c->n_max) FAIL(MHD_ERR_INVALID, "n must be in [1, n_max]");
+  if (steps < 0) FAIL(MHD_ERR_INVALID, "steps must be >= 0");
+  if (!check_state(c, a, false) || !check_state(c, b, false)) return MHD_ERR_INVALID;
+  if (a->x == b->x) FAIL(MHD_ERR_INVALID, "a and b must not alias");
+  if (c->batched && n != c->inst_start.back()) FAIL(MHD_ERR_INVALID, "n differs from the instances' total");
+  if (capture && !c->batched) FAIL(MHD_ERR_INVALID, "captured runs need mhd_ctx_set_instances first");
+  if (steps == 0) return MHD_OK;
+  const cudaStream_t st = S(stream);
+  if (!capture) {
+    for (int k = 0; k < steps; k++) {
+      const MhdState* cur = (k & 1) ? b : a;
+      MhdState* nxt = (k & 1) ? a : b;
+      const int mode = (finish && k == steps - 1) ? 1 : 3;
+      int rc = step_fused(c, cur, nxt, (int)n, mode, false, st);
+      if (rc != MHD_OK) return rc;
+    }
+    return read_status(c, st);
+  }
+  Ctx::GraphEntry* hit = nullptr;
+  for (auto& e : c->graphs)
+    if (e.generation == c->generation && e.n == n && e.steps == steps && e.finish == finish &&
+        !memcmp(&e.a, a, sizeof(MhdState)) && !memcmp(&e.b, b, sizeof(MhdState)))
+      hit = &e;
+  if (!hit) {
+    if (c->graphs.size() >= 8) drop_graphs(c);
+    Ctx::GraphEntry e;
+    memset(&e, 0, sizeof e);
+    int rc = capture_run(c, a, b, (int)n, steps, finish, e);
+    if (rc != MHD_OK) return rc;
+    c->graphs.push_back(e);
+    hit = &c->graphs.back();
+  }
+  CK(cudaGraphLaunch(hit->exec, st));
+  c->launches += hit->launches;
+  CK(cudaMemcpyAsync(c->h_sc, c->d_sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  const int rc = read_status(c, st);
+  if (rc != MHD_OK) return rc;
+  if (c->h_sc->relist || c->h_sc->events) {
+    CK(cudaMemsetAsync(&c->d_sc->events, 0, sizeof(int), st));
+    FAIL(MHD_ERR_RELIST, "the captured run met a neighbour-list rebuild or an unfinished density iteration; "
+                         "restore its input state and replay it uncaptured");
+  }
   return MHD_OK;
 }
 

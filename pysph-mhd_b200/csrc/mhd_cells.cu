@@ -16,42 +16,109 @@
 namespace mhd {
 
 // ---------------------------------------------------------------- reductions
-// h_max over all particles and the bounding box of positions (for axes that
-// are not periodic).  Order-mapped integer atomics; sc->h_max_bits etc. must
-// be reset by the caller.
-__global__ void __launch_bounds__(256) k_reduce_hbox(int n, const double* __restrict__ x,
-                                                     const double* __restrict__ y, const double* __restrict__ z,
-                                                     const double* __restrict__ h, DevScalars* sc) {
-  double hm = 0.0;
-  double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+// Per-instance h_max and bounding box (order-mapped integer atomics into the
+// instance's InstScalars, which the consumer resets).  The particles of an
+// instance are contiguous, so each block takes one contiguous chunk and a
+// thread flushes a partial result only where the instance changes; a warp
+// whose lanes all hold the same instance combines them first.
+struct HBox {
+  double hm, lo[3], hi[3];
+  __device__ void reset() {
+    hm = 0.0;
+    for (int a = 0; a < 3; a++) {
+      lo[a] = INFINITY;
+      hi[a] = -INFINITY;
+    }
+  }
+  __device__ void flush(InstScalars* is, int k) const {
+    atomicMax(&is[k].h_max_bits, dbl_order(hm));
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      atomicMin(&is[k].lo_bits[a], dbl_order(lo[a]));
+      atomicMax(&is[k].hi_bits[a], dbl_order(hi[a]));
+    }
+  }
+};
+
+__global__ void __launch_bounds__(256) k_reduce_hbox(int n, int chunk, const int* __restrict__ inst,
+                                                     const double* __restrict__ x, const double* __restrict__ y,
+                                                     const double* __restrict__ z, const double* __restrict__ h,
+                                                     InstScalars* is, DevScalars* sc) {
   const double* pos[3] = {x, y, z};
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  const int b0 = blockIdx.x * chunk, b1 = min(n, b0 + chunk);
+  int key = -1;
+  HBox acc;
+  acc.reset();
+  bool bad = false;
+  for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
+    const int k = inst ? inst[i] : 0;
+    if (k != key) {
+      if (key >= 0) acc.flush(is, key);
+      acc.reset();
+      key = k;
+    }
     const double hv = h[i];
-    hm = hv > hm ? hv : hm;
-    if (!(hv > 0.0) || !isfinite(hv)) set_status(sc, MHD_ERR_NONFINITE);
+    acc.hm = hv > acc.hm ? hv : acc.hm;
+    bad |= !(hv > 0.0) || !isfinite(hv);
 #pragma unroll
     for (int a = 0; a < 3; a++) {
       const double v = pos[a][i];
-      lo[a] = fmin(lo[a], v);
-      hi[a] = fmax(hi[a], v);
+      acc.lo[a] = fmin(acc.lo[a], v);
+      acc.hi[a] = fmax(acc.hi[a], v);
     }
   }
-  for (int o = 16; o > 0; o >>= 1) {
-    hm = fmax(hm, __shfl_xor_sync(0xffffffffu, hm, o));
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) set_status(sc, MHD_ERR_NONFINITE);
+  const int wkey = __reduce_max_sync(0xffffffffu, key);
+  if (__all_sync(0xffffffffu, key < 0 || key == wkey)) {
+    for (int o = 16; o > 0; o >>= 1) {
+      acc.hm = fmax(acc.hm, __shfl_xor_sync(0xffffffffu, acc.hm, o));
 #pragma unroll
-    for (int a = 0; a < 3; a++) {
-      lo[a] = fmin(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], o));
-      hi[a] = fmax(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], o));
+      for (int a = 0; a < 3; a++) {
+        acc.lo[a] = fmin(acc.lo[a], __shfl_xor_sync(0xffffffffu, acc.lo[a], o));
+        acc.hi[a] = fmax(acc.hi[a], __shfl_xor_sync(0xffffffffu, acc.hi[a], o));
+      }
     }
+    if ((threadIdx.x & 31) == 0 && wkey >= 0) acc.flush(is, wkey);
+  } else if (key >= 0) {
+    acc.flush(is, key);
   }
-  if ((threadIdx.x & 31) == 0) {
-    atomicMax(&sc->h_max_bits, dbl_order(hm));
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-      atomicMin(&sc->lo_bits[a], dbl_order(lo[a]));
-      atomicMax(&sc->hi_bits[a], dbl_order(hi[a]));
-    }
+}
+
+__device__ __forceinline__ void reset_hbox(InstScalars& q) {
+  q.h_max_bits = 0ULL;
+  for (int a = 0; a < 3; a++) {
+    q.lo_bits[a] = ~0ULL;
+    q.hi_bits[a] = 0ULL;
   }
+}
+
+__global__ void k_reset_hbox(int n_inst, InstScalars* is) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n_inst) reset_hbox(is[k]);
+}
+
+// Device planner of a batched context: one thread per instance plans its
+// grid from the reductions above (same arithmetic as the host planner),
+// within the instance's cell capacity, and resets the reductions.
+__global__ void k_plan_grids(int n_inst, PlanSpec S, InstScalars* is, Grid* grids, DevScalars* sc) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n_inst) return;
+  InstScalars& q = is[k];
+  const double hmax = dbl_unorder(q.h_max_bits);
+  double lo[3], hi[3];
+  for (int a = 0; a < 3; a++) {
+    lo[a] = dbl_unorder(q.lo_bits[a]);
+    hi[a] = dbl_unorder(q.hi_bits[a]);
+  }
+  Grid g;
+  const int rc = plan_instance(S, q.n, hmax, lo, hi, q.nc_cap, g);
+  if (rc != MHD_OK) {
+    set_status(sc, rc);
+  } else {
+    g.cell_base = q.cell_base;
+    grids[k] = g;
+  }
+  reset_hbox(q);
 }
 
 // --------------------------------------------------------------- cell keys
@@ -290,7 +357,18 @@ int64_t scan_sums_needed(int64_t n_max) {
 
 void launch_reduce_hbox(Ctx* c, const MhdState* s, int n, cudaStream_t st) {
   const int blocks = n > 0 ? (ceil_div(n, 256) < 1184 ? ceil_div(n, 256) : 1184) : 1;
-  k_reduce_hbox<<<blocks, 256, 0, st>>>(n, s->x, s->y, s->z, s->h, c->d_sc);
+  const int chunk = n > 0 ? ceil_div(n, blocks) : 1;
+  k_reduce_hbox<<<blocks, 256, 0, st>>>(n, chunk, c->inst, s->x, s->y, s->z, s->h, c->d_inst, c->d_sc);
+  c->launches++;
+}
+
+void launch_reset_hbox(Ctx* c, cudaStream_t st) {
+  k_reset_hbox<<<ceil_div(c->n_inst, 128), 128, 0, st>>>(c->n_inst, c->d_inst);
+  c->launches++;
+}
+
+void launch_plan_grids(Ctx* c, cudaStream_t st) {
+  k_plan_grids<<<ceil_div(c->n_inst, 128), 128, 0, st>>>(c->n_inst, c->spec, c->d_inst, c->d_grids, c->d_sc);
   c->launches++;
 }
 

@@ -74,25 +74,34 @@ struct DevParams {
   double norm;  // kernel normalisation sigma_d
 };
 
-// Device-resident scalars of one context (status, reductions, step clock).
+// Device-resident scalars of one context (status, pass counters, events).
 struct DevScalars {
-  double dt;       // step size in use (stage2 of the current step)
-  double dt_next;  // next step size (min dt_adapt, clipped to tf)
-  double t;        // time at the start of the current step
-  double t_next;   // time at the start of the next step
-  unsigned long long dt_min_bits;  // atomicMin target (positive doubles order as integers)
-  unsigned long long h_max_bits;
-  unsigned long long lo_bits[3];  // bounding box (non-periodic axes), order-mapped
-  unsigned long long hi_bits[3];
   int status;       // first device error, MHD_OK if none
   int relist;       // an h outgrew its neighbour list, or a list overflowed
   int list_max;     // longest neighbour list met by the last build
   int passes_done;  // density passes executed in the current group evaluation
   unsigned int ticket;              // last-block counter of the dt reduction
-  int events;                       // batched steps that met a relist / overflow / pass cap
+  int events;                       // captured runs: bit 0 = density passes ran out before the group stopped
   unsigned long long n_pairs;       // force-pass neighbour pairs (accumulating)
   unsigned long long n_candidates;  // force-pass distance tests (accumulating)
   int n_unconverged[256 + 8];       // per density pass
+};
+
+// Device-resident scalars of one instance: its step clock and the
+// reductions its grid is planned from (a single simulation uses entry 0).
+struct InstScalars {
+  double dt;       // step size in use (stage2 of the current step)
+  double dt_next;  // next step size (min dt_adapt, clipped to tf)
+  double t;        // time at the start of the current step
+  double t_next;   // time at the start of the next step
+  unsigned long long dt_min_bits;  // atomicMin target (order-mapped); reset to ~0 after use
+  unsigned long long h_max_bits;   // order-mapped; reset to 0 after use
+  unsigned long long lo_bits[3];   // bounding box, order-mapped; reset to ~0 / 0 after use
+  unsigned long long hi_bits[3];
+  int nc_cap[3];   // per-axis cell capacity (batched contexts)
+  int cell_base;   // first global cell key of the instance
+  int n;           // particles of the instance
+  int pad;
 };
 
 // ------------------------------------------------------------ kernels (SPH)
@@ -193,6 +202,114 @@ __host__ __device__ inline double dbl_unorder(unsigned long long b) {
   double d;
   memcpy(&d, &v, sizeof d);
   return d;
+}
+
+// Products, quotients and sums rounded once each (no contraction), so the
+// device planner reproduces the host planner bit for bit.
+__host__ __device__ inline double mul_rn(double a, double b) {
+#ifdef __CUDA_ARCH__
+  return __dmul_rn(a, b);
+#else
+  return a * b;
+#endif
+}
+__host__ __device__ inline double div_rn(double a, double b) {
+#ifdef __CUDA_ARCH__
+  return __ddiv_rn(a, b);
+#else
+  return a / b;
+#endif
+}
+__host__ __device__ inline double add_rn(double a, double b) {
+#ifdef __CUDA_ARCH__
+  return __dadd_rn(a, b);
+#else
+  return a + b;
+#endif
+}
+
+// What the grid plans of a context's instances share.
+struct PlanSpec {
+  int dim;
+  int stencil;  // cells are >= cut-off / stencil wide
+  int periodic[3];
+  double lo[3];  // periodic box
+  double L[3];
+  double half[3];
+  double R;
+  double grid_margin;
+  double list_margin;
+};
+
+// Uniform grid of one instance from its h_max and bounding box [lo, hi]
+// (used on non-periodic axes): cells at least
+// R * h_max * grid_margin * (1 + list_margin) / stencil wide, at most
+// 2047/2047/1023 (3-D) or 65535 (2-D) per axis (the packed cell-coordinate
+// widths) and 2^24 in all, and at most nc_cap[a] per axis when nc_cap is
+// given.  Fills everything but cell_base.  Returns MHD_OK or
+// MHD_ERR_NONFINITE.
+__host__ __device__ inline int plan_instance(const PlanSpec& S, int n, double hmax, const double* lo_red,
+                                             const double* hi_red, const int* nc_cap, Grid& g) {
+  g = Grid{};
+  if (n <= 0) hmax = 1.0;
+  const double cutoff = mul_rn(mul_rn(mul_rn(S.R, hmax), S.grid_margin), add_rn(1.0, S.list_margin));
+  double extent[3];
+  for (int a = 0; a < 3; a++) {
+    g.periodic[a] = a < S.dim ? S.periodic[a] : 0;
+    g.L[a] = S.L[a];
+    g.half[a] = S.half[a];
+    if (a >= S.dim) {
+      g.nc[a] = 1;
+      g.lo[a] = 0.0;
+      extent[a] = 1.0;
+      continue;
+    }
+    double lo, ext;
+    if (S.periodic[a]) {
+      lo = S.lo[a];
+      ext = S.L[a];
+    } else {
+      lo = n > 0 ? lo_red[a] : 0.0;
+      const double hi = n > 0 ? hi_red[a] : 1.0;
+      ext = add_rn(mul_rn(add_rn(hi, -lo), 1.0 + 1e-12), 1e-300);
+    }
+    if (!isfinite(lo) || !isfinite(ext) || !isfinite(cutoff)) return MHD_ERR_NONFINITE;
+    const double axis_max = S.dim == 3 ? (a == 2 ? 1023.0 : 2047.0) : 65535.0;
+    const double ncd = floor(div_rn(mul_rn(ext, (double)S.stencil), cutoff));
+    g.nc[a] = ncd < 1.0 ? 1 : (ncd > axis_max ? (int)axis_max : (int)ncd);
+    g.lo[a] = lo;
+    extent[a] = ext;
+  }
+  // Keep the table within 2^24 cells; coarser cells stay valid.
+  const long long cap = 1LL << 24;
+  while ((long long)g.nc[0] * g.nc[1] * g.nc[2] > cap) {
+    int a = 0;
+    for (int b = 1; b < 3; b++)
+      if (g.nc[b] > g.nc[a]) a = b;
+    const int shrunk = (int)mul_rn((double)g.nc[a], 0.8);
+    g.nc[a] = shrunk > 1 ? shrunk : 1;
+  }
+  if (nc_cap)
+    for (int a = 0; a < 3; a++) g.nc[a] = g.nc[a] < nc_cap[a] ? g.nc[a] : (nc_cap[a] > 1 ? nc_cap[a] : 1);
+  // The stencil of +-stencil cells covers the cut-off on every axis with at
+  // least 2*stencil+1 cells; smaller axes are scanned whole.
+  double hplan = INFINITY;
+  g.sw = S.stencil;
+  for (int a = 0; a < 3; a++) {
+    g.cs[a] = div_rn(extent[a], (double)g.nc[a]);
+    g.csf[a] = (float)g.cs[a];
+    g.inv_cs[a] = a < S.dim ? div_rn(1.0, g.cs[a]) : 0.0;
+    const bool limits = a < S.dim && g.nc[a] >= 2 * g.sw + 1;
+    if (limits) {
+      const double hp = mul_rn(div_rn(mul_rn((double)g.sw, g.cs[a]), mul_rn(S.R, add_rn(1.0, S.list_margin))),
+                               1.0 - 1e-9);
+      hplan = hp < hplan ? hp : hplan;
+    }
+  }
+  g.h_plan = hplan;
+  g.cut = cutoff;
+  g.ncells = g.nc[0] * g.nc[1] * g.nc[2];
+  return MHD_OK;
 }
 
 __device__ __forceinline__ void set_status(DevScalars* sc, int code) { atomicCAS(&sc->status, MHD_OK, code); }

@@ -118,14 +118,18 @@ __global__ void __launch_bounds__(256) k_stage2(int n, MhdState s, DevParams P, 
 }
 
 // stage2(dt_cur) of this step, then initialize + stage1(dt_next) of the next.
-// mode bit 1: corrector; bit 2: predictor.  dev_dt: read both steps from sc.
+// mode bit 1: corrector; bit 2: predictor.  dev_dt: read both steps from the
+// clock of the particle's instance.
 __global__ void __launch_bounds__(256) k_corrector_predictor(int n, MhdState s, DevParams P, int mode, double dt_cur,
-                                                             double dt_next, int dev_dt, const DevScalars* sc) {
+                                                             double dt_next, int dev_dt,
+                                                             const int* __restrict__ inst,
+                                                             const InstScalars* __restrict__ is) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   if (dev_dt) {
-    dt_cur = sc->dt;
-    dt_next = sc->dt_next;
+    const InstScalars& q = is[inst ? inst[i] : 0];
+    dt_cur = q.dt;
+    dt_next = q.dt_next;
   }
   const bool fluid = s.itype[i] == 1;
   double u = s.u[i], v = s.v[i], w = s.w[i], e = s.e[i];
@@ -195,48 +199,86 @@ __global__ void __launch_bounds__(256) k_corrector_predictor(int n, MhdState s, 
   s.psipred[i] = psi + dt * apsi;
 }
 
-// min(dt_adapt) with the tf clip; the last block finishes the reduction.
-// t_host < 0: the step starts at the device clock's t + dt.
-__global__ void __launch_bounds__(256) k_dt_reduce(int n, const double* __restrict__ dt_adapt, double t_host,
-                                                   DevScalars* sc, unsigned int* ticket, double tf) {
+// Per-instance min(dt_adapt) with the tf clip; the last block finishes the
+// reduction of every instance.  Each block takes one contiguous chunk (the
+// particles of an instance are contiguous) and flushes per instance.
+// t_host < 0: each instance's step starts at its clock's t + dt.
+__global__ void __launch_bounds__(256) k_dt_reduce(int n, int chunk, const int* __restrict__ inst, int n_inst,
+                                                   const double* __restrict__ dt_adapt, double t_host,
+                                                   InstScalars* is, DevScalars* sc, double tf) {
+  const int b0 = blockIdx.x * chunk, b1 = min(n, b0 + chunk);
+  int key = -1;
   double m = INFINITY;
   bool bad = false;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
+    const int k = inst ? inst[i] : 0;
+    if (k != key) {
+      if (key >= 0) atomicMin(&is[key].dt_min_bits, dbl_order(m));
+      m = INFINITY;
+      key = k;
+    }
     const double v = dt_adapt[i];
     bad |= !(v > 0.0) || !isfinite(v);
     m = fmin(m, v);
   }
-  for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
   if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) set_status(sc, MHD_ERR_NONFINITE);
-  if ((threadIdx.x & 31) == 0) atomicMin(&sc->dt_min_bits, dbl_order(m));
+  const int wkey = __reduce_max_sync(0xffffffffu, key);
+  if (__all_sync(0xffffffffu, key < 0 || key == wkey)) {
+    for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && wkey >= 0) atomicMin(&is[wkey].dt_min_bits, dbl_order(m));
+  } else if (key >= 0) {
+    atomicMin(&is[key].dt_min_bits, dbl_order(m));
+  }
   __shared__ bool last;
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
-    last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    last = atomicAdd(&sc->ticket, 1u) == gridDim.x - 1;
   }
   __syncthreads();
-  if (last && threadIdx.x == 0) {
-    __threadfence();
-    const double dmin = dbl_unorder(atomicAdd(&sc->dt_min_bits, 0ULL));
-    const double t_next = t_host >= 0.0 ? t_host : sc->t + sc->dt;
+  if (!last) return;
+  __threadfence();
+  for (int k = threadIdx.x; k < n_inst; k += blockDim.x) {
+    InstScalars& q = is[k];
+    const double dmin = dbl_unorder(atomicAdd(&q.dt_min_bits, 0ULL));
+    const double t_next = t_host >= 0.0 ? t_host : q.t + q.dt;
     double dt = dmin;
     if (t_next + dt > tf) dt = tf - t_next;
-    sc->dt_next = dt;
-    sc->t_next = t_next;
-    sc->dt_min_bits = ~0ULL;
-    *ticket = 0u;
+    q.dt_next = dt;
+    q.t_next = t_next;
+    q.dt_min_bits = ~0ULL;
   }
+  if (threadIdx.x == 0) sc->ticket = 0u;
 }
 
-__global__ void k_clock_advance(DevScalars* sc) {
-  sc->t = sc->t_next;
-  sc->dt = sc->dt_next;
+__global__ void k_clock_advance(int n_inst, InstScalars* is) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n_inst) return;
+  is[k].t = is[k].t_next;
+  is[k].dt = is[k].dt_next;
 }
 
-__global__ void k_clock_set(DevScalars* sc, double t, double dt) {
-  sc->t = t;
-  sc->dt = dt;
+// Clock of every instance from / to stage[0:n_inst] (t) and
+// stage[n_inst:2*n_inst] (dt).  Setting a clock also sets the pending step
+// (t_next, dt_next) to it, so that a predictor with the device dt followed
+// by the clock advance starts the step [t, t + dt].
+__global__ void k_clock_load(int n_inst, const double* __restrict__ stage, InstScalars* is) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n_inst) return;
+  is[k].t = is[k].t_next = stage[k];
+  is[k].dt = is[k].dt_next = stage[n_inst + k];
+}
+
+__global__ void k_clock_store(int n_inst, const InstScalars* __restrict__ is, double* __restrict__ stage) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n_inst) return;
+  stage[k] = is[k].t;
+  stage[n_inst + k] = is[k].dt;
+}
+
+__global__ void k_clock_set(InstScalars* is, double t, double dt) {
+  is->t = is->t_next = t;
+  is->dt = is->dt_next = dt;
 }
 
 static int blocks_for(int n) { return n > 0 ? (n + 255) / 256 : 1; }
@@ -255,11 +297,12 @@ void launch_corrector_predictor(Ctx* c, MhdState* s, int n, int mode, double dt_
   const int dev = (mode & 1 ? dt_cur < 0.0 : false) || (mode & 2 ? dt_next < 0.0 : false);
   TimedScope ts(c, MHD_TIMING_INTEGRATE, st);
   if (n > 0) {
-    k_corrector_predictor<<<blocks_for(n), 256, 0, st>>>(n, *s, c->P, mode, dt_cur, dt_next, dev, c->d_sc);
+    k_corrector_predictor<<<blocks_for(n), 256, 0, st>>>(n, *s, c->P, mode, dt_cur, dt_next, dev, c->inst,
+                                                         c->d_inst);
     c->launches++;
   }
   if (dev && (mode & 2)) {
-    k_clock_advance<<<1, 1, 0, st>>>(c->d_sc);
+    k_clock_advance<<<(c->n_inst + 127) / 128, 128, 0, st>>>(c->n_inst, c->d_inst);
     c->launches++;
   }
 }
@@ -267,13 +310,24 @@ void launch_corrector_predictor(Ctx* c, MhdState* s, int n, int mode, double dt_
 void launch_dt_reduce(Ctx* c, const MhdState* s, int n, double t, cudaStream_t st) {
   int blocks = blocks_for(n);
   if (blocks > 1184) blocks = 1184;
+  const int chunk = n > 0 ? (n + blocks - 1) / blocks : 1;
   TimedScope ts(c, MHD_TIMING_DT, st);
-  k_dt_reduce<<<blocks, 256, 0, st>>>(n, s->dt_adapt, t, c->d_sc, &c->d_sc->ticket, c->P.tf);
+  k_dt_reduce<<<blocks, 256, 0, st>>>(n, chunk, c->inst, c->n_inst, s->dt_adapt, t, c->d_inst, c->d_sc, c->P.tf);
   c->launches++;
 }
 
 void launch_clock_set(Ctx* c, double t, double dt, cudaStream_t st) {
-  k_clock_set<<<1, 1, 0, st>>>(c->d_sc, t, dt);
+  k_clock_set<<<1, 1, 0, st>>>(c->d_inst, t, dt);
+  c->launches++;
+}
+
+void launch_clock_load(Ctx* c, cudaStream_t st) {
+  k_clock_load<<<(c->n_inst + 127) / 128, 128, 0, st>>>(c->n_inst, c->d_stage, c->d_inst);
+  c->launches++;
+}
+
+void launch_clock_store(Ctx* c, cudaStream_t st) {
+  k_clock_store<<<(c->n_inst + 127) / 128, 128, 0, st>>>(c->n_inst, c->d_inst, c->d_stage);
   c->launches++;
 }
 

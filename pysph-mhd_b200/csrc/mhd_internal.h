@@ -39,7 +39,25 @@ struct Ctx {
   int grid_slots = 0;       // entries allocated in d_grids / h_grids
   int* inst = nullptr;      // instance of each particle; null = one instance
   int n_inst = 1;
+  bool batched = false;     // instances set: grids planned on the device within fixed capacities
   int key_cells = 0;        // cells over all instances (the sort key range)
+  InstScalars* d_inst = nullptr;  // per-instance clock and reductions (n_inst entries)
+  InstScalars* h_inst = nullptr;  // pinned staging copy of d_inst
+  double* d_stage = nullptr;      // 2 * n_inst doubles for clock uploads / downloads
+  std::vector<int64_t> inst_start;  // first particle of each instance (n_inst + 1 entries)
+  PlanSpec spec;                  // what every instance's grid plan shares
+  int64_t generation = 0;         // bumped when a buffer captured by a graph is reallocated
+  int graph_passes = 8;           // density passes captured per right-hand side
+  cudaStream_t cap_stream = nullptr;
+  struct GraphEntry {
+    MhdState a, b;
+    int64_t n;
+    int steps, finish;
+    int64_t generation;
+    cudaGraphExec_t exec;
+    int64_t launches;  // kernels per replay
+  };
+  std::vector<GraphEntry> graphs;
   bool have_grid = false;
   int64_t n_max = 0;
   int device = 0;
@@ -132,17 +150,22 @@ void launch_reduce_hbox(Ctx* c, const MhdState* s, int n, cudaStream_t st);
 void launch_sort_cells(Ctx* c, const MhdState* s, int n, cudaStream_t st);
 void launch_gather(Ctx* c, const GatherSet& gs, int n, cudaStream_t st);
 
+void launch_reset_hbox(Ctx* c, cudaStream_t st);
+void launch_plan_grids(Ctx* c, cudaStream_t st);
 void launch_build_lists(Ctx* c, const MhdState* s, int n, cudaStream_t st);
 void launch_pack_positions(Ctx* c, const MhdState* s, int n, cudaStream_t st);
 void launch_neighbour_counts(Ctx* c, const MhdState* s, int n, int* out, cudaStream_t st);
 // density pass `pass` (0-based) reading h_in, writing h_out
 void launch_density_pass(Ctx* c, MhdState* s, int n, int pass, const double* h_in, double* h_out, cudaStream_t st);
+void launch_finish_density(Ctx* c, MhdState* s, int n, int passes, cudaStream_t st);
 void launch_force_prologue(Ctx* c, MhdState* s, int n, cudaStream_t st);
 void launch_force_pass(Ctx* c, MhdState* s, int n, cudaStream_t st);
 
 void launch_dt_reduce(Ctx* c, const MhdState* s, int n, double t, cudaStream_t st);
 void launch_stage(Ctx* c, MhdState* s, int n, int which, double dt, cudaStream_t st);
 void launch_clock_set(Ctx* c, double t, double dt, cudaStream_t st);
+void launch_clock_load(Ctx* c, cudaStream_t st);
+void launch_clock_store(Ctx* c, cudaStream_t st);
 int probe_fma_peak(int precision, double* flops, cudaStream_t st);
 void launch_corrector_predictor(Ctx* c, MhdState* s, int n, int mode, double dt_cur, double dt_next,
                                 cudaStream_t st);

@@ -304,4 +304,26 @@ void launch_density_pass(Ctx* c, MhdState* s, int n, int pass, const double* h_i
   c->launches++;
 }
 
+// End of a captured density iteration (a fixed number of passes, each with
+// the on-device stop test): the latest h is in h_alt after an odd number of
+// passes; a group that had not stopped when the passes ran out raises an
+// event (the run is replayed uncaptured).
+__global__ void __launch_bounds__(256) k_finish_density(int n, DevParams P, int passes, double* __restrict__ h,
+                                                        const double* __restrict__ h_alt, DevScalars* sc) {
+  const int done = sc->passes_done;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) {
+    const bool stopped = done >= P.max_iter || (!P.iterate && done > 0) ||
+                         (done >= P.min_iter && done > 0 && sc->n_unconverged[done - 1] == 0);
+    if (!stopped && done >= passes) atomicOr(&sc->events, 1);
+  }
+  if (i < n && (done & 1)) h[i] = h_alt[i];
+}
+
+void launch_finish_density(Ctx* c, MhdState* s, int n, int passes, cudaStream_t st) {
+  if (n <= 0) return;
+  k_finish_density<<<(n + 255) / 256, 256, 0, st>>>(n, c->P, passes, s->h, c->h_alt, c->d_sc);
+  c->launches++;
+}
+
 }  // namespace mhd

@@ -21,7 +21,9 @@ ERRORS = {
     -4: "MHD_ERR_NONFINITE",
     -5: "MHD_ERR_CAPACITY",
     -6: "MHD_ERR_NO_DEVICE",
+    -7: "MHD_ERR_RELIST",
 }
+MHD_ERR_RELIST = -7
 
 KERNELS = {"cubic": 0, "quintic": 1, "wendland_c2": 2, "wendland_c4": 3, "wendland_c6": 4, "gaussian": 5,
            "super_gaussian": 6}
@@ -81,7 +83,8 @@ EXPORTS = (
     "mhd_launch_count", "mhd_cells_build", "mhd_density_iterate", "mhd_force_pass", "mhd_rhs", "mhd_timestep",
     "mhd_clock_set", "mhd_clock_get", "mhd_step_initialize", "mhd_step_stage1", "mhd_step_stage2",
     "mhd_corrector_predictor", "mhd_step", "mhd_timing_enable", "mhd_timing_read", "mhd_probe_fma_peak",
-    "mhd_pair_counts", "mhd_timestep_noalloc", "mhd_neighbour_counts",
+    "mhd_pair_counts", "mhd_timestep_noalloc", "mhd_neighbour_counts", "mhd_ctx_set_instances",
+    "mhd_instance_count", "mhd_clock_set_all", "mhd_clock_get_all", "mhd_advance", "mhd_ctx_tune",
 )
 NOALLOC_MAX_N = 67108864
 TIMING_KINDS = ("cells", "density", "prologue", "force", "dt", "integrate")
@@ -131,6 +134,13 @@ def load(path: str = LIB_PATH):
     lib.mhd_pair_counts.argtypes = [vp, ctypes.POINTER(i64), ctypes.POINTER(i64), vp]
     lib.mhd_timestep_noalloc.argtypes = [vp, i64, dbl, dbl, vp, vp]
     lib.mhd_neighbour_counts.argtypes = [vp, sp, i64, vp, vp]
+    lib.mhd_ctx_set_instances.argtypes = [vp, sp, i32, ctypes.POINTER(i64), dbl, vp]
+    lib.mhd_instance_count.argtypes = [vp]
+    lib.mhd_instance_count.restype = i32
+    lib.mhd_clock_set_all.argtypes = [vp, ctypes.POINTER(dbl), ctypes.POINTER(dbl), vp]
+    lib.mhd_clock_get_all.argtypes = [vp, ctypes.POINTER(dbl), ctypes.POINTER(dbl), vp]
+    lib.mhd_advance.argtypes = [vp, sp, sp, i64, i32, i32, i32, vp]
+    lib.mhd_ctx_tune.argtypes = [vp, i32, i32]
     _lib = lib
     return lib
 

@@ -19,7 +19,7 @@ def _declared():
     names = []
     for h in HEADERS:
         text = open(h).read()
-        names += re.findall(r"^\s*(?:int|int64_t|const char\*|void)\s+\**(mhd_\w+)\s*\(", text, re.M)
+        names += re.findall(r"^\s*(?:int|int32_t|int64_t|const char\*|void)\s+\**(mhd_\w+)\s*\(", text, re.M)
     return sorted(set(names))
 
 

@@ -1,0 +1,180 @@
+"""Batched form: uneven instances in one context, captured runs, autotuner.
+
+Each instance keeps its own grid, clock and timestep, and the sort keeps an
+instance's particles in the order a standalone run gives them, so an
+instance advanced in the batch must equal the same case advanced alone, bit
+for bit, in FP64 and in FP32 (while no neighbour-list rebuild intervenes).
+The standalone runs are the drop-in path already checked against the oracle.
+"""
+
+import numpy as np
+import pytest
+
+pytest.importorskip("torch")
+
+import small_cases as sc_  # noqa: E402
+from compare import assert_close  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("x", "y", "u", "v", "rho", "h", "e", "Bx", "By", "psi", "alpha1", "p")
+
+
+def _instances(sizes=(12, 17, 22), scales=(1.0, 0.85, 1.15), seed=3):
+    ics, prm = [], None
+    for k, (n, s) in enumerate(zip(sizes, scales)):
+        ic, prm = sc_.orszag_tang_2d(n, "quintic", jitter=0.05, seed=seed + k)
+        ic["Bx"] = ic["Bx"] * s
+        ic["By"] = ic["By"] * s
+        ics.append(ic)
+    return ics, prm
+
+
+def _alone(ic, prm, precision, steps):
+    from src.engine import Engine, params_from_dict
+    from src.particle_array import ParticleArray
+
+    eng = Engine(params_from_dict(prm, precision), ParticleArray("fluid", dict(ic)))
+    eng.warmup()
+    eng.begin(eng.initial_dt())
+    eng.advance(steps)
+    out = eng.pa.pull(*FIELDS, "gid", order="gid")
+    t, dt = eng.clock()
+    eng.close()
+    return out, t
+
+
+def _batch(ics, prm, precision, steps, capture=True, **kw):
+    from src.batch import BatchEngine
+    from src.engine import params_from_dict
+
+    eng = BatchEngine(params_from_dict(prm, precision), [dict(ic) for ic in ics], **kw)
+    eng.warmup()
+    eng.begin(eng.initial_dt())
+    eng.advance(steps, capture=capture)
+    return eng
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_batch_equals_each_instance_alone(precision):
+    ics, prm = _instances()
+    steps = 4
+    eng = _batch(ics, prm, precision, steps)
+    t_all, _ = eng.clocks()
+    for k, ic in enumerate(ics):
+        ref, t_ref = _alone(ic, prm, precision, steps)
+        got = eng.pull_instance(k, *FIELDS, "gid")
+        np.testing.assert_array_equal(got["gid"], ref["gid"])
+        for f in FIELDS:
+            np.testing.assert_array_equal(got[f], ref[f], err_msg=f"instance {k} field {f} ({precision})")
+        assert t_all[k] == t_ref
+    assert eng.replays == 0
+    eng.close()
+
+
+def test_captured_equals_uncaptured():
+    ics, prm = _instances(sizes=(16, 9, 20), seed=11)
+    a = _batch(ics, prm, "fp64", 5, capture=True)
+    b = _batch(ics, prm, "fp64", 5, capture=False)
+    for k in range(len(ics)):
+        ga, gb = a.pull_instance(k, *FIELDS), b.pull_instance(k, *FIELDS)
+        for f in FIELDS:
+            np.testing.assert_array_equal(ga[f], gb[f], err_msg=f"instance {k} field {f}")
+    np.testing.assert_array_equal(a.clocks()[0], b.clocks()[0])
+    a.close()
+    b.close()
+
+
+def test_graph_is_reused_and_runs_continue():
+    ics, prm = _instances(sizes=(10, 14), seed=5)
+    a = _batch(ics, prm, "fp64", 2, capture=True)
+    a.advance(2, capture=True)  # same buffers and step count: the cached graph
+    b = _batch(ics, prm, "fp64", 2, capture=False)
+    b.advance(2, capture=False)
+    for k in range(len(ics)):
+        ga, gb = a.pull_instance(k, *FIELDS), b.pull_instance(k, *FIELDS)
+        for f in FIELDS:
+            np.testing.assert_array_equal(ga[f], gb[f], err_msg=f"instance {k} field {f}")
+    a.close()
+    b.close()
+
+
+def test_unfinished_captured_iteration_replays(monkeypatch):
+    # One captured density pass cannot satisfy min_iter = 2: every captured
+    # run raises the event and is replayed uncaptured from its snapshot.
+    monkeypatch.setenv("MHD_GRAPH_PASSES", "1")
+    ics, prm = _instances(sizes=(12, 15), seed=7)
+    a = _batch(ics, prm, "fp64", 3, capture=True)
+    assert a.replays == 1
+    monkeypatch.delenv("MHD_GRAPH_PASSES")
+    b = _batch(ics, prm, "fp64", 3, capture=False)
+    for k in range(len(ics)):
+        ga, gb = a.pull_instance(k, *FIELDS), b.pull_instance(k, *FIELDS)
+        for f in FIELDS:
+            np.testing.assert_array_equal(ga[f], gb[f], err_msg=f"instance {k} field {f}")
+    a.close()
+    b.close()
+
+
+def test_single_instance_on_the_device_planner():
+    ic, prm = sc_.orszag_tang_2d(24, "quintic", jitter=0.05, seed=2)
+    ref, t_ref = _alone(ic, prm, "fp64", 3)
+    eng = _batch([ic], prm, "fp64", 3)
+    got = eng.pull_instance(0, *FIELDS)
+    for f in FIELDS:
+        np.testing.assert_array_equal(got[f], ref[f], err_msg=f)
+    assert eng.clocks()[0][0] == t_ref
+    eng.close()
+
+
+def test_autotuner_picks_a_valid_configuration():
+    from src.batch import FORCE_SHAPES, STENCILS
+
+    ics, prm = _instances(sizes=(16, 24, 12), seed=9)
+    from src.batch import BatchEngine
+    from src.engine import params_from_dict
+
+    eng = BatchEngine(params_from_dict(prm, "fp32"), [dict(ic) for ic in ics])
+    eng.warmup()
+    eng.begin(eng.initial_dt())
+    best = eng.tune(steps=2, stencils=(1, 2), shapes=(0, 2))
+    assert best["stencil"] in STENCILS and best["force_shape"] in FORCE_SHAPES
+    assert len(best["trials"]) == 4 and all(r["ms_per_step"] > 0 for r in best["trials"])
+    eng.advance(3)
+    # the tuned grid orders the sums differently: equal to roundoff
+    for k, ic in enumerate(ics):
+        ref, _ = _alone(ic, prm, "fp32", 3)
+        got = eng.pull_instance(k, *FIELDS)
+        assert_close(got, ref, ["rho", "u", "v", "Bx", "By", "e", "h"], 1e-5, None, None, f"tuned instance {k}")
+    eng.close()
+
+
+def test_instance_declaration_is_validated():
+    import ctypes
+
+    from src import _abi
+    from src.batch import BatchEngine
+    from src.engine import params_from_dict
+
+    ics, prm = _instances(sizes=(8, 8))
+    eng = BatchEngine(params_from_dict(prm, "fp64"), ics)
+    s = eng.pa.state()
+    bad = (ctypes.c_int64 * 3)(0, 64, 64)  # empty second instance
+    assert eng.lib.mhd_ctx_set_instances(eng.ctx, ctypes.byref(s), 2, bad, 1.25, eng.stream) == -1
+    too_many = (ctypes.c_int64 * 3)(0, 64, 10 ** 9)
+    assert eng.lib.mhd_ctx_set_instances(eng.ctx, ctypes.byref(s), 2, too_many, 1.25, eng.stream) == -1
+    ok = (ctypes.c_int64 * 3)(0, 64, 128)
+    assert eng.lib.mhd_ctx_set_instances(eng.ctx, ctypes.byref(s), 2, ok, 0.5, eng.stream) == -1
+    assert eng.lib.mhd_instance_count(eng.ctx) == 2
+    eng.close()
+
+    # capture needs declared instances
+    from src.engine import Engine
+    from src.particle_array import ParticleArray
+
+    e2 = Engine(params_from_dict(prm, "fp64"), ParticleArray("fluid", dict(ics[0])))
+    a, b = e2.pa.state(), e2.pa.state(spare=True)
+    rc = e2.lib.mhd_advance(e2.ctx, ctypes.byref(a), ctypes.byref(b), e2.pa.n, 1, 1, 1, e2.stream)
+    assert rc == -1 and "set_instances" in e2.lib.mhd_last_error(e2.ctx).decode()
+    assert _abi.ERRORS[-7] == "MHD_ERR_RELIST"
+    e2.close()
