@@ -274,14 +274,32 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_add(uint32_t* __restrict_
 }
 
 // --------------------------------------------------------------- cell table
-// cell_start[c] = first sorted slot whose key >= c, for c in [0, ncells].
+// cell_start[c] = first sorted slot whose key >= c, for c in [0, ncells]:
+// one thread per cell, a lower-bound search in the sorted keys.  Two threads
+// of each block first bound the block's 256 cells, so the per-cell searches
+// cover only the slots of those cells.  Long runs of empty cells (capacity
+// tails of a batched context) cost no more than occupied ones.
+__device__ __forceinline__ int lower_bound_key(const uint32_t* __restrict__ k, int lo, int hi, uint32_t key) {
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (k[mid] < key) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
 __global__ void __launch_bounds__(256) k_cell_starts(int n, int ncells, const uint32_t* __restrict__ skeys,
                                                      int* __restrict__ cell_start) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s > n) return;
-  const int kcur = s < n ? (int)skeys[s] : ncells;
-  const int kprev = s > 0 ? (int)skeys[s - 1] : -1;
-  for (int c = kprev + 1; c <= kcur; c++) cell_start[c] = s;
+  __shared__ int range[2];
+  const int c0 = blockIdx.x * 256;
+  if (threadIdx.x < 2) {
+    const long long c = (long long)c0 + (threadIdx.x ? 256 : 0);
+    range[threadIdx.x] = c > ncells ? n : lower_bound_key(skeys, 0, n, (uint32_t)c);
+  }
+  __syncthreads();
+  const int c = c0 + threadIdx.x;
+  if (c > ncells) return;
+  cell_start[c] = lower_bound_key(skeys, range[0], range[1], (uint32_t)c);
 }
 
 // ------------------------------------------------------- packed positions
@@ -400,7 +418,8 @@ void launch_sort_cells(Ctx* c, const MhdState* s, int n, cudaStream_t st) {
   }
   c->sorted_keys = c->keys[cur];
   c->perm = c->vals[cur];
-  k_cell_starts<<<ceil_div(n + 1, 256), 256, 0, st>>>(n, c->key_cells, c->sorted_keys, c->cell_start);
+  k_cell_starts<<<ceil_div((int64_t)c->key_cells + 1, 256), 256, 0, st>>>(n, c->key_cells, c->sorted_keys,
+                                                                         c->cell_start);
   c->launches++;
 }
 

@@ -51,3 +51,23 @@ class OrszagTang2D(MHDApplication):
         mass = rho / count
         return dict(x=x, y=y, z=np.zeros(count),
                     **_fields(x, y, count, mass, rho, self.gamma, self.hfact, 2, -0.5, -0.5, b0scale))
+
+
+def orszag_tang_batch(config, n_inst=64, n_min=32, n_max=256, b0_range=(0.8, 1.2), seed=0):
+    """The batched workload: ``n_inst`` independent 2-D Orszag-Tang
+    instances (``OrszagTang2D`` with ``config``), instance k an N_k x N_k
+    square lattice with N_k uniform in [n_min, n_max] and B0 scaled by a
+    factor uniform in ``b0_range``, both drawn from ``seed``.  Returns the
+    instance arrays, the shared kernel parameters, the sizes and the scales."""
+    from dataclasses import replace
+
+    rng = np.random.default_rng(seed)
+    sizes = rng.integers(n_min, n_max + 1, n_inst)
+    scales = rng.uniform(b0_range[0], b0_range[1], n_inst)
+    instances, params = [], None
+    for n, s in zip(sizes, scales):
+        app = OrszagTang2D(replace(config, case=replace(config.case, nx=int(n))))
+        instances.append(app.create_mhd_particles(b0scale=float(s)))
+        if params is None:
+            params = app.scheme.kernel_params(app.create_domain(), app.tf)
+    return instances, params, sizes, scales
