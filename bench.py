@@ -10,9 +10,16 @@ Synthetic seeded inputs of that shape; no dataset is involved.
 
 One "step" is one predictor-evaluate-corrector step of the whole particle
 set (neighbour sort, iterated density, fused force pass, FP64 dt reduction,
-fused corrector-predictor), after the reference's 3-RHS warm-up.  Inputs
+fused corrector-predictor), after the reference's 3-RHS warm-up.  The K
+timed steps run as one captured CUDA graph (``mhd_advance``); the kernel
+breakdown comes from K more steps of the same kernels run uncaptured.  Inputs
 (state 35 fields x 2.1M x 8 B ~ 590 MB) exceed the 126 MB L2, so no flush
 is needed between steps.
+
+The same line carries the batched form (``batched_form``): 64 independent
+2-D Orszag-Tang instances of uneven size advanced 100 steps in one captured
+graph launch after the autotuner, against the plain FP64 path run instance
+by instance.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
@@ -199,31 +206,32 @@ def run_reference(args, rank):
 
 
 def _timed(args, prec, dev, barrier, dist, world):
-    """W untimed + K timed fused steps of the blast in one precision form."""
+    """W untimed + K timed fused steps of the blast in one precision form.
+
+    The timed steps are one captured run (``mhd_advance``: a CUDA graph of K
+    fused steps, grids planned on the device); the per-kernel breakdown and
+    the pair counts come from K more steps of the same kernels run uncaptured
+    with CUDA events around every launch (outside the timed region)."""
     import ctypes
 
     import torch
 
     from src import _abi
-    from src.engine import Engine, params_from_dict
-    from src.particle_array import ParticleArray
+    from src.batch import BatchEngine
+    from src.engine import params_from_dict
 
     ic, prm = blast_case(args.n, prec)
     n = args.n ** 3
     lib = _abi.load()
-    eng = Engine(params_from_dict(prm), ParticleArray("fluid", ic, device=dev))
+    eng = BatchEngine(params_from_dict(prm), [ic])
     eng.warmup()
     eng.begin(eng.initial_dt())
     eng.advance(args.warmup, finish=False)
+    # capture the K-step graph once (runs K steps; the state stays valid)
+    eng.advance(args.steps, finish=False)
     torch.cuda.synchronize()
-    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
-    ms_k = (ctypes.c_double * 6)()
-    cnt_k = (ctypes.c_int64 * 6)()
-    lib.mhd_timing_enable(eng.ctx, 1)
-    lib.mhd_timing_read(eng.ctx, ms_k, cnt_k)
-    pairs, cands = ctypes.c_int64(), ctypes.c_int64()
-    lib.mhd_pair_counts(eng.ctx, ctypes.byref(pairs), ctypes.byref(cands), st)
-    passes0 = len(eng.density_passes)
+    snap = eng.snapshot()
+    replays0 = eng.replays
     launches0 = eng.launches()
     clocks = ClockSampler(dev.index or 0)
     barrier()
@@ -232,13 +240,14 @@ def _timed(args, prec, dev, barrier, dist, world):
     time.sleep(0.3)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
-    eng.advance(args.steps, finish=False)
+    eng.advance(args.steps, finish=False, snapshot=snap)
     e1.record()
     torch.cuda.synchronize()
     barrier()
     clocks.stop()
     ms = e0.elapsed_time(e1)
     launches = eng.launches() - launches0
+    replays = eng.replays - replays0
     ms_max = ms
     if dist:
         import torch.distributed as tdist
@@ -246,15 +255,103 @@ def _timed(args, prec, dev, barrier, dist, world):
         t = torch.tensor([ms], device=dev, dtype=torch.float64)
         tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
         ms_max = float(t.item())
+    # kernel breakdown (uncaptured, identical kernels)
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    ms_k = (ctypes.c_double * 6)()
+    cnt_k = (ctypes.c_int64 * 6)()
+    pairs, cands = ctypes.c_int64(), ctypes.c_int64()
+    lib.mhd_pair_counts(eng.ctx, ctypes.byref(pairs), ctypes.byref(cands), st)
+    lib.mhd_timing_enable(eng.ctx, 1)
+    lib.mhd_timing_read(eng.ctx, ms_k, cnt_k)
+    e0.record()
+    eng.advance(args.steps, finish=False, capture=False)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_unc = e0.elapsed_time(e1)
     lib.mhd_timing_read(eng.ctx, ms_k, cnt_k)
     lib.mhd_pair_counts(eng.ctx, ctypes.byref(pairs), ctypes.byref(cands), st)
     lib.mhd_timing_enable(eng.ctx, 0)
-    passes = eng.density_passes[passes0:]
+    eng.rhs()
+    passes = int(eng.last_stats.density_passes)
     eng.close()
     kern = {k: {"ms_total": ms_k[i], "launches": int(cnt_k[i])} for i, k in enumerate(_abi.TIMING_KINDS)}
     return {"value": world * n * args.steps / (ms_max * 1e-3), "ms_per_step": ms_max / args.steps,
-            "kernels": kern, "launches": launches, "clocks": clocks.summary(), "pairs": pairs.value,
-            "candidates": cands.value, "passes": passes}
+            "ms_per_step_uncaptured": ms_unc / args.steps, "kernels": kern, "launches": launches,
+            "replays": replays, "clocks": clocks.summary(), "pairs": pairs.value, "candidates": cands.value,
+            "passes": passes}
+
+
+def _batched(args, dev):
+    """The batched form: 64 independent 2-D Orszag-Tang instances (N ~ U{32..256},
+    B0 x U[0.8, 1.2], seed 0) advanced 100 steps as one captured graph after
+    the autotuner, against the plain FP64 path run instance by instance."""
+    import torch
+
+    from src.batch import BatchEngine
+    from src.cases.orstang import orszag_tang_batch
+    from src.config import load_config
+    from src.engine import Engine, params_from_dict
+    from src.particle_array import ParticleArray
+    from src.run import CASES
+
+    cfg = load_config(os.path.join(PKG, "configs", "orstang2d.toml"), {k: v.config_type for k, v in CASES.items()})
+    inst, prm, sizes, scales = orszag_tang_batch(cfg, n_inst=args.batch_instances, seed=0)
+    total = int(sum(len(a["x"]) for a in inst))
+    steps = args.batch_steps
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    out, final = {}, {}
+    for prec in ("fp32", "fp64"):
+        eng = BatchEngine(params_from_dict(prm, prec), inst)
+        eng.warmup()
+        eng.begin(eng.initial_dt())
+        t0 = time.perf_counter()
+        tuned = eng.tune(steps=4)
+        tune_s = time.perf_counter() - t0
+        snap = eng.snapshot()
+        eng.advance(steps, finish=True, snapshot=snap)  # capture + first run
+        eng.restore(snap)
+        torch.cuda.synchronize()
+        l0, r0 = eng.launches(), eng.replays
+        ev0.record()
+        eng.advance(steps, finish=True, snapshot=snap)
+        ev1.record()
+        ev1.synchronize()
+        ms = ev0.elapsed_time(ev1)
+        out[prec] = {"value": total * steps / (ms * 1e-3), "ms": ms, "gpu_launches": eng.launches() - l0,
+                     "graph_launches": 1, "replays": eng.replays - r0, "tune_s": tune_s,
+                     "tuned": {"stencil": tuned["stencil"], "force_shape": tuned["force_shape"]}}
+        final[prec] = eng.pa.pull("rho", "u", "v", "Bx", "By", "gid", order="gid")
+        eng.close()
+    # plain FP64 path, one instance at a time (K steps each, summed device time)
+    k_loop = args.batch_loop_steps
+    loop_ms = 0.0
+    for a in inst:
+        eng = Engine(params_from_dict(prm, "fp64"), ParticleArray("fluid", dict(a), device=dev))
+        eng.warmup()
+        eng.begin(eng.initial_dt())
+        torch.cuda.synchronize()
+        ev0.record()
+        eng.advance(k_loop, finish=False)
+        ev1.record()
+        ev1.synchronize()
+        loop_ms += ev0.elapsed_time(ev1)
+        eng.close()
+    loop = total * k_loop / (loop_ms * 1e-3)
+    a, b = final["fp32"], final["fp64"]
+
+    def rel(keys):
+        num = sum(float(np.sum((a[k] - b[k]) ** 2)) for k in keys)
+        den = sum(float(np.sum(b[k] ** 2)) for k in keys)
+        return math.sqrt(num / den)
+
+    return {"workload": f"{len(inst)} x 2-D Orszag-Tang, N x N with N ~ U{{32..256}} (seed 0; sizes "
+                        f"{int(sizes.min())}..{int(sizes.max())}), B0 x U[0.8, 1.2], quintic hfact 1.2, "
+                        f"{total} particles, {steps} steps in one captured graph launch",
+            "particles": total, "steps": steps, "fp32": out["fp32"], "fp64": out["fp64"],
+            "fp64_instance_loop": {"value": loop, "steps_per_instance": k_loop, "ms": loop_ms},
+            "speedup_fp32_vs_fp64_loop": out["fp32"]["value"] / loop,
+            "speedup_fp64_vs_fp64_loop": out["fp64"]["value"] / loop,
+            "fp32_vs_fp64_rel_l2": {"rho": rel(["rho"]), "v": rel(["u", "v"]), "B": rel(["Bx", "By"])}}
 
 
 def _accuracy(args, dev, steps):
@@ -325,6 +422,7 @@ def run_b200(args, rank, world):
     achieved_tf = flops / (force_ms * 1e-3) / 1e12
 
     e2e = run_e2e(args, dev)
+    batched = _batched(args, dev) if (rank == 0 and not dist and args.batch_instances > 0) else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -334,7 +432,6 @@ def run_b200(args, rank, world):
                          f"{ns} particles, {args.cpu_steps} PEC steps after the warm-up, {el:.1f} s"}
 
     if rank == 0:
-        passes = head["passes"]
         line = {
             "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
@@ -344,7 +441,8 @@ def run_b200(args, rank, world):
             "config": {"workload": f"3-D MHD blast {args.n}^3 = {n} particles, cubic kernel hfact 1.2, "
                                    f"alpha [0.1, 1], periodic unit cube", "form": args.precision,
                        "parallelism": "replicas" if world > 1 else "single", "l2_flush": "inputs (~0.6 GB) > L2",
-                       "density_passes_mean": sum(passes) / max(len(passes), 1),
+                       "density_passes_per_rhs": head["passes"], "timed_run": "one captured graph of K fused steps",
+                       "replays": head["replays"], "ms_per_step_uncaptured": head["ms_per_step_uncaptured"],
                        "neighbours_mean": head["pairs"] / (n * args.steps),
                        "list_entries_mean": head["candidates"] / (n * args.steps)},
             "fp64_path": None if base is None else {"value": base["value"], "ms_per_step": base["ms_per_step"],
@@ -364,6 +462,7 @@ def run_b200(args, rank, world):
             "gpu_launches": head["launches"],
             "clocks": head["clocks"],
             "e2e": e2e,
+            "batched_form": batched,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
@@ -431,6 +530,9 @@ def main():
     ap.add_argument("--accuracy-steps", type=int, default=100)
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-instances", type=int, default=64, help="batched form instances (0 skips it)")
+    ap.add_argument("--batch-steps", type=int, default=100)
+    ap.add_argument("--batch-loop-steps", type=int, default=10, help="steps per instance of the FP64 loop")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", "0"))

@@ -178,6 +178,7 @@ void refresh_spec(Ctx* c) {
   S.R = P.R;
   S.grid_margin = c->grid_margin;
   S.list_margin = c->list_margin;
+  S.cell_kappa = c->cell_kappa;
 }
 
 int grow_cell_table(Ctx* c, int64_t cells) {
@@ -219,7 +220,8 @@ int plan_grid(Ctx* c, const MhdState* s, int n, cudaStream_t st) {
     hi[a] = dbl_unorder(q.hi_bits[a]);
   }
   Grid g;
-  if (plan_instance(c->spec, n, dbl_unorder(q.h_max_bits), lo, hi, nullptr, g) != MHD_OK)
+  const double hmax = dbl_unorder(q.h_max_bits);
+  if (plan_instance(c->spec, n, hmax, mean_h(hmax, q.h_sum, n), lo, hi, nullptr, g) != MHD_OK)
     FAIL(MHD_ERR_NONFINITE, "non-finite particle position");
   g.cell_base = 0;
   c->list_cut = g.cut;
@@ -625,6 +627,7 @@ int mhd_ctx_create(const MhdParams* params, int64_t n_max, void** out) {
     const int cap = ((int)(1.5 * vol) + 16 + 7) & ~7;
     ok = ok && dev_alloc(c, &c->posf, c->n_pad) == MHD_OK && dev_alloc(c, &c->cellc, c->n_pad) == MHD_OK;
     ok = ok && dev_alloc(c, &c->nbr_cnt, c->n_pad) == MHD_OK && dev_alloc(c, &c->nbr_hlim, c->n_pad) == MHD_OK &&
+         dev_alloc(c, &c->nbr_gcnt, c->n_pad) == MHD_OK && dev_alloc(c, &c->big_idx, c->n_pad) == MHD_OK &&
          ensure_list_storage(c, cap) == MHD_OK;
   }
   if (ok && cudaMallocHost((void**)&c->h_sc, sizeof(DevScalars)) != cudaSuccess) ok = false;
@@ -645,6 +648,7 @@ int mhd_ctx_create(const MhdParams* params, int64_t n_max, void** out) {
   if (const char* m = getenv("MHD_FORCE_SHAPE")) c->force_shape = std::max(0, std::min(3, atoi(m)));
   if (const char* m = getenv("MHD_STENCIL")) c->stencil = std::max(1, std::min(3, atoi(m)));
   if (const char* m = getenv("MHD_GRAPH_PASSES")) c->graph_passes = std::max(1, std::min(256, atoi(m)));
+  if (const char* m = getenv("MHD_CELL_KAPPA")) c->cell_kappa = std::max(1.0, atof(m));
   *out = c;
   return MHD_OK;
 }
@@ -669,6 +673,8 @@ int mhd_ctx_destroy(void* ctx) {
   cudaFree(c->cellc);
   cudaFree(c->nbr_idx);
   cudaFree(c->nbr_cnt);
+  cudaFree(c->nbr_gcnt);
+  cudaFree(c->big_idx);
   cudaFree(c->nbr_hlim);
   for (double* p : c->spare) cudaFree(p);
   for (auto& e : c->events) {
@@ -950,7 +956,8 @@ int mhd_ctx_set_instances(void* ctx, const MhdState* s, int32_t n_inst, const in
       hi[a] = dbl_unorder(q.hi_bits[a]);
     }
     Grid g;
-    if (plan_instance(c->spec, q.n, dbl_unorder(q.h_max_bits), lo, hi, nullptr, g) != MHD_OK)
+    const double hmax = dbl_unorder(q.h_max_bits);
+    if (plan_instance(c->spec, q.n, hmax, mean_h(hmax, q.h_sum, q.n), lo, hi, nullptr, g) != MHD_OK)
       FAIL(MHD_ERR_NONFINITE, "non-finite particle position");
     int64_t cells = 1;
     for (int a = 0; a < 3; a++) {
@@ -969,6 +976,7 @@ int mhd_ctx_set_instances(void* ctx, const MhdState* s, int32_t n_inst, const in
     base += cells;
     if (base > ((int64_t)1 << 30)) FAIL(MHD_ERR_CAPACITY, "instances need more than 2^30 cells");
     q.h_max_bits = 0ULL;
+    q.h_sum = 0ULL;
     for (int a = 0; a < 3; a++) {
       q.lo_bits[a] = ~0ULL;
       q.hi_bits[a] = 0ULL;

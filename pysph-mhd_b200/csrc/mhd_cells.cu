@@ -68,6 +68,11 @@ __global__ void __launch_bounds__(256) k_reduce_hbox(int n, int chunk, const int
     }
   }
   if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) set_status(sc, MHD_ERR_NONFINITE);
+  // warps whose lanes share one instance combine in registers, then the
+  // block's warps combine in shared memory: one flush per instance and block
+  __shared__ int skey[8];
+  __shared__ HBox sacc[8];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int wkey = __reduce_max_sync(0xffffffffu, key);
   if (__all_sync(0xffffffffu, key < 0 || key == wkey)) {
     for (int o = 16; o > 0; o >>= 1) {
@@ -78,14 +83,70 @@ __global__ void __launch_bounds__(256) k_reduce_hbox(int n, int chunk, const int
         acc.hi[a] = fmax(acc.hi[a], __shfl_xor_sync(0xffffffffu, acc.hi[a], o));
       }
     }
-    if ((threadIdx.x & 31) == 0 && wkey >= 0) acc.flush(is, wkey);
-  } else if (key >= 0) {
-    acc.flush(is, key);
+    if (lane == 0) {
+      skey[warp] = wkey;
+      sacc[warp] = acc;
+    }
+  } else {
+    if (key >= 0) acc.flush(is, key);
+    if (lane == 0) skey[warp] = -1;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int cur = -1;
+    HBox run;
+    run.reset();
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+      const int k = skey[w];
+      if (k < 0) continue;
+      if (k != cur) {
+        if (cur >= 0) run.flush(is, cur);
+        run.reset();
+        cur = k;
+      }
+      const HBox& b = sacc[w];
+      run.hm = fmax(run.hm, b.hm);
+      for (int a = 0; a < 3; a++) {
+        run.lo[a] = fmin(run.lo[a], b.lo[a]);
+        run.hi[a] = fmax(run.hi[a], b.hi[a]);
+      }
+    }
+    if (cur >= 0) run.flush(is, cur);
+  }
+}
+
+// Per-instance sum of h / h_max in 2^-32 units (integer atomics, so the
+// sum and the mean h planned from it do not depend on the order of
+// accumulation).  Runs after k_reduce_hbox.
+__global__ void __launch_bounds__(256) k_reduce_hsum(int n, int chunk, const int* __restrict__ inst,
+                                                     const double* __restrict__ h, InstScalars* is) {
+  const int b0 = blockIdx.x * chunk, b1 = min(n, b0 + chunk);
+  int key = -1;
+  double scale = 0.0;
+  unsigned long long acc = 0ULL;
+  for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
+    const int k = inst ? inst[i] : 0;
+    if (k != key) {
+      if (key >= 0 && acc) atomicAdd(&is[key].h_sum, acc);
+      acc = 0ULL;
+      key = k;
+      scale = 4294967296.0 / dbl_unorder(is[k].h_max_bits);
+    }
+    const double v = h[i] * scale;
+    acc += v > 0.0 ? (unsigned long long)fmin(v, 4294967296.0) : 0ULL;
+  }
+  const int wkey = __reduce_max_sync(0xffffffffu, key);
+  if (__all_sync(0xffffffffu, key < 0 || key == wkey)) {
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0 && wkey >= 0 && acc) atomicAdd(&is[wkey].h_sum, acc);
+  } else if (key >= 0 && acc) {
+    atomicAdd(&is[key].h_sum, acc);
   }
 }
 
 __device__ __forceinline__ void reset_hbox(InstScalars& q) {
   q.h_max_bits = 0ULL;
+  q.h_sum = 0ULL;
   for (int a = 0; a < 3; a++) {
     q.lo_bits[a] = ~0ULL;
     q.hi_bits[a] = 0ULL;
@@ -111,7 +172,7 @@ __global__ void k_plan_grids(int n_inst, PlanSpec S, InstScalars* is, Grid* grid
     hi[a] = dbl_unorder(q.hi_bits[a]);
   }
   Grid g;
-  const int rc = plan_instance(S, q.n, hmax, lo, hi, q.nc_cap, g);
+  const int rc = plan_instance(S, q.n, hmax, mean_h(hmax, q.h_sum, q.n), lo, hi, q.nc_cap, g);
   if (rc != MHD_OK) {
     set_status(sc, rc);
   } else {
@@ -377,7 +438,8 @@ void launch_reduce_hbox(Ctx* c, const MhdState* s, int n, cudaStream_t st) {
   const int blocks = n > 0 ? (ceil_div(n, 256) < 1184 ? ceil_div(n, 256) : 1184) : 1;
   const int chunk = n > 0 ? ceil_div(n, blocks) : 1;
   k_reduce_hbox<<<blocks, 256, 0, st>>>(n, chunk, c->inst, s->x, s->y, s->z, s->h, c->d_inst, c->d_sc);
-  c->launches++;
+  k_reduce_hsum<<<blocks, 256, 0, st>>>(n, chunk, c->inst, s->h, c->d_inst);
+  c->launches += 2;
 }
 
 void launch_reset_hbox(Ctx* c, cudaStream_t st) {

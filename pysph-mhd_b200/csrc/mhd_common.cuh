@@ -33,9 +33,10 @@ struct Grid {
   double cs[3];
   double L[3];  // the instance's periodic box (lo .. lo + L on periodic axes)
   double half[3];
-  double h_plan;  // every h must stay <= h_plan for the grid to be valid
-  double cut;     // list cut-off R * h_max * (1 + margin)
+  double h_plan;  // largest h whose list cut-off the +-sw stencil covers
+  double cut;     // list cut-off R * h_cell * grid_margin * (1 + margin)
   float csf[3];   // cell widths in FP32 (packed-position geometry)
+  float h_bigf;   // particles with FP32 h above this are "big": they search an extended stencil
 };
 
 __device__ __forceinline__ const Grid& grid_of(const Grid* __restrict__ grids, const int* __restrict__ inst, int i) {
@@ -82,6 +83,7 @@ struct DevScalars {
   int passes_done;  // density passes executed in the current group evaluation
   unsigned int ticket;              // last-block counter of the dt reduction
   int events;                       // captured runs: bit 0 = density passes ran out before the group stopped
+  int n_big;                        // big particles met by the last list build
   unsigned long long n_pairs;       // force-pass neighbour pairs (accumulating)
   unsigned long long n_candidates;  // force-pass distance tests (accumulating)
   int n_unconverged[256 + 8];       // per density pass
@@ -98,6 +100,7 @@ struct InstScalars {
   unsigned long long h_max_bits;   // order-mapped; reset to 0 after use
   unsigned long long lo_bits[3];   // bounding box, order-mapped; reset to ~0 / 0 after use
   unsigned long long hi_bits[3];
+  unsigned long long h_sum;        // sum of h / h_max in 2^-32 units (exact, order-independent)
   int nc_cap[3];   // per-axis cell capacity (batched contexts)
   int cell_base;   // first global cell key of the instance
   int n;           // particles of the instance
@@ -239,20 +242,28 @@ struct PlanSpec {
   double R;
   double grid_margin;
   double list_margin;
+  double cell_kappa;  // cells follow min(h_max, cell_kappa * h_mean)
 };
 
-// Uniform grid of one instance from its h_max and bounding box [lo, hi]
-// (used on non-periodic axes): cells at least
-// R * h_max * grid_margin * (1 + list_margin) / stencil wide, at most
+// Uniform grid of one instance from its h_max, mean h and bounding box
+// [lo, hi] (used on non-periodic axes).  The cells follow
+// h_cell = min(h_max, cell_kappa * h_mean), not h_max, so that a few
+// particles with a large h do not coarsen the grid for all: particles with h
+// above h_plan (the largest h the +-stencil covers) are "big" and search an
+// extended stencil of their own.  Cells are at least
+// R * h_cell * grid_margin * (1 + list_margin) / stencil wide, at most
 // 2047/2047/1023 (3-D) or 65535 (2-D) per axis (the packed cell-coordinate
 // widths) and 2^24 in all, and at most nc_cap[a] per axis when nc_cap is
 // given.  Fills everything but cell_base.  Returns MHD_OK or
 // MHD_ERR_NONFINITE.
-__host__ __device__ inline int plan_instance(const PlanSpec& S, int n, double hmax, const double* lo_red,
-                                             const double* hi_red, const int* nc_cap, Grid& g) {
+__host__ __device__ inline int plan_instance(const PlanSpec& S, int n, double hmax, double hmean,
+                                             const double* lo_red, const double* hi_red, const int* nc_cap,
+                                             Grid& g) {
   g = Grid{};
-  if (n <= 0) hmax = 1.0;
-  const double cutoff = mul_rn(mul_rn(mul_rn(S.R, hmax), S.grid_margin), add_rn(1.0, S.list_margin));
+  if (n <= 0) hmax = hmean = 1.0;
+  const double hk = mul_rn(S.cell_kappa, hmean);
+  const double hcell = hk < hmax ? hk : hmax;
+  const double cutoff = mul_rn(mul_rn(mul_rn(S.R, hcell), S.grid_margin), add_rn(1.0, S.list_margin));
   double extent[3];
   for (int a = 0; a < 3; a++) {
     g.periodic[a] = a < S.dim ? S.periodic[a] : 0;
@@ -307,9 +318,15 @@ __host__ __device__ inline int plan_instance(const PlanSpec& S, int n, double hm
     }
   }
   g.h_plan = hplan;
+  g.h_bigf = hplan < 1e30 ? (float)mul_rn(hplan, 1.0 - 1e-5) : INFINITY;
   g.cut = cutoff;
   g.ncells = g.nc[0] * g.nc[1] * g.nc[2];
   return MHD_OK;
+}
+
+// Mean h from the fixed-point sum of h / h_max.
+__host__ __device__ inline double mean_h(double hmax, unsigned long long h_sum, int n) {
+  return n > 0 ? mul_rn(hmax, div_rn((double)h_sum, mul_rn((double)n, 4294967296.0))) : 1.0;
 }
 
 __device__ __forceinline__ void set_status(DevScalars* sc, int code) { atomicCAS(&sc->status, MHD_OK, code); }
@@ -352,44 +369,45 @@ __device__ __forceinline__ int cell_delta(int d, int nc, int periodic) {
 
 // FP32 minimum-image displacement x_i - x_j from packed positions: the cell
 // offset carries the large part exactly, the in-cell offsets the rest.  On a
-// periodic axis with at least 2*sw+1 cells a neighbour is at most sw cells
-// away and the wrapped cell offset selects its image; an axis with fewer
-// cells (scanned whole) can hold pairs nc/2 cells apart, whose image the
-// offset does not decide, so it takes the FP32 minimum image.
+// periodic axis with at least 2*sw+1 cells a pair of normal particles is at
+// most sw cells apart and the wrapped cell offset selects its image; on an
+// axis with fewer cells (scanned whole), or for a pair more than sw cells
+// apart (a big particle's), the FP32 minimum image is taken as well.  The
+// result is exactly antisymmetric in i and j.
+__device__ __forceinline__ float fold_image(float d, float L) {
+  const float hL = 0.5f * L;
+  return d > hL ? d - L : (d < -hL ? d + L : d);
+}
+
 template <int DIM>
 __device__ __forceinline__ void rel_dx(const Grid& G, const float4& pi, int ci, const float4& pj, int cj, float& dx,
                                        float& dy, float& dz) {
   int xi, yi, zi, xj, yj, zj;
   unpack_cell<DIM>(ci, xi, yi, zi);
   unpack_cell<DIM>(cj, xj, yj, zj);
-  dx = (pi.x - pj.x) + (float)cell_delta(xi - xj, G.nc[0], G.periodic[0]) * G.csf[0];
-  dy = (pi.y - pj.y) + (float)cell_delta(yi - yj, G.nc[1], G.periodic[1]) * G.csf[1];
-  dz = DIM == 3 ? (pi.z - pj.z) + (float)cell_delta(zi - zj, G.nc[2], G.periodic[2]) * G.csf[2] : 0.f;
+  const int ex = cell_delta(xi - xj, G.nc[0], G.periodic[0]);
+  const int ey = cell_delta(yi - yj, G.nc[1], G.periodic[1]);
+  const int ez = DIM == 3 ? cell_delta(zi - zj, G.nc[2], G.periodic[2]) : 0;
+  dx = (pi.x - pj.x) + (float)ex * G.csf[0];
+  dy = (pi.y - pj.y) + (float)ey * G.csf[1];
+  dz = DIM == 3 ? (pi.z - pj.z) + (float)ez * G.csf[2] : 0.f;
   const int whole = 2 * G.sw + 1;
-  if (G.periodic[0] && G.nc[0] < whole) {
-    const float L = (float)G.L[0], hL = 0.5f * L;
-    dx = dx > hL ? dx - L : (dx < -hL ? dx + L : dx);
-  }
-  if (G.periodic[1] && G.nc[1] < whole) {
-    const float L = (float)G.L[1], hL = 0.5f * L;
-    dy = dy > hL ? dy - L : (dy < -hL ? dy + L : dy);
-  }
-  if (DIM == 3 && G.periodic[2] && G.nc[2] < whole) {
-    const float L = (float)G.L[2], hL = 0.5f * L;
-    dz = dz > hL ? dz - L : (dz < -hL ? dz + L : dz);
-  }
+  if (G.periodic[0] && (G.nc[0] < whole || abs(ex) > G.sw)) dx = fold_image(dx, (float)G.L[0]);
+  if (G.periodic[1] && (G.nc[1] < whole || abs(ey) > G.sw)) dy = fold_image(dy, (float)G.L[1]);
+  if (DIM == 3 && G.periodic[2] && (G.nc[2] < whole || abs(ez) > G.sw)) dz = fold_image(dz, (float)G.L[2]);
 }
 
-// Calls f(cx, cy, cz, jb, je) for every cell within `cut` of (xi, yi, zi):
-// (cx, cy, cz) are unwrapped cell coordinates (their offset from the
-// particle's own cell selects the periodic image), [jb, je) the cell's range
-// in the sorted order.  Rows farther than `cut` are skipped and each row is
-// trimmed to [x - cut, x + cut].  Axes with fewer than 2*sw+1 cells are
-// scanned whole with their own coordinates (no image selection).
+// Calls f(cx, cy, cz, jb, je) for every cell within `cut` of (xi, yi, zi),
+// searching +-sw cells (cut <= sw cell widths): (cx, cy, cz) are unwrapped
+// cell coordinates (their offset from the particle's own cell selects the
+// periodic image), [jb, je) the cell's range in the sorted order.  Rows
+// farther than `cut` are skipped and each row is trimmed to
+// [x - cut, x + cut].  Axes with fewer than 2*sw+1 cells are scanned whole
+// with their own coordinates (no image selection).
 template <int DIM, class F>
-__device__ __forceinline__ void for_each_cell_trimmed(const Grid& G, const int* __restrict__ cell_start, double xi,
-                                                      double yi, double zi, double cut, F&& f) {
-  const int sw = G.sw, whole = 2 * sw + 1;
+__device__ __forceinline__ void for_each_cell_trimmed(const Grid& G, int sw, const int* __restrict__ cell_start,
+                                                      double xi, double yi, double zi, double cut, F&& f) {
+  const int whole = 2 * sw + 1;
   const int nx = G.nc[0], ny = G.nc[1], nz = G.nc[2];
   const int cy = cell_coord(G, 1, yi);
   const int cz = DIM == 3 ? cell_coord(G, 2, zi) : 0;
@@ -404,6 +422,7 @@ __device__ __forceinline__ void for_each_cell_trimmed(const Grid& G, const int* 
       xl = xl < 0 ? 0 : xl;
       xh = xh >= nx ? nx - 1 : xh;
     }
+    if (xh - xl >= nx) xh = xl + nx - 1;  // never visit a cell twice
   }
   const double cut2 = cut * cut;
   const bool zs = DIM == 3 && nz >= whole, ys = ny >= whole;

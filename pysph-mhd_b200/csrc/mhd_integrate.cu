@@ -222,12 +222,36 @@ __global__ void __launch_bounds__(256) k_dt_reduce(int n, int chunk, const int* 
     m = fmin(m, v);
   }
   if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) set_status(sc, MHD_ERR_NONFINITE);
+  // warp, then block combination: one atomic per instance and block
+  __shared__ int skey[8];
+  __shared__ double smin[8];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int wkey = __reduce_max_sync(0xffffffffu, key);
   if (__all_sync(0xffffffffu, key < 0 || key == wkey)) {
     for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if ((threadIdx.x & 31) == 0 && wkey >= 0) atomicMin(&is[wkey].dt_min_bits, dbl_order(m));
-  } else if (key >= 0) {
-    atomicMin(&is[key].dt_min_bits, dbl_order(m));
+    if (lane == 0) {
+      skey[warp] = wkey;
+      smin[warp] = m;
+    }
+  } else {
+    if (key >= 0) atomicMin(&is[key].dt_min_bits, dbl_order(m));
+    if (lane == 0) skey[warp] = -1;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int cur = -1;
+    double run = INFINITY;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+      const int k = skey[w];
+      if (k < 0) continue;
+      if (k != cur) {
+        if (cur >= 0) atomicMin(&is[cur].dt_min_bits, dbl_order(run));
+        run = INFINITY;
+        cur = k;
+      }
+      run = fmin(run, smin[w]);
+    }
+    if (cur >= 0) atomicMin(&is[cur].dt_min_bits, dbl_order(run));
   }
   __shared__ bool last;
   __syncthreads();

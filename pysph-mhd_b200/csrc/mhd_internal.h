@@ -85,7 +85,8 @@ struct Ctx {
   void* rec[6] = {};
 
   double* spare[kGatherMax] = {};  // replan buffers, allocated on first use
-  double grid_margin = 1.0;        // cells are R * h_max * grid_margin * (1 + list_margin) wide
+  double grid_margin = 1.0;        // cells are R * h_cell * grid_margin * (1 + list_margin) wide
+  double cell_kappa = 1.1;         // h_cell = min(h_max, cell_kappa * h_mean)
 
   // packed FP32 positions relative to the cell origin, and packed cell
   // coordinates, of the sorted particles (written after every sort)
@@ -100,6 +101,8 @@ struct Ctx {
   int list_cap = 0;
   int* nbr_idx = nullptr;
   int* nbr_cnt = nullptr;
+  int* nbr_gcnt = nullptr;  // entries of the gather pass (the rest were scattered)
+  int* big_idx = nullptr;   // big particles of the last build (DevScalars::n_big of them)
   double* nbr_hlim = nullptr;
   int64_t n_pad = 0;  // n_max rounded up to a multiple of 32
   bool lists_checked = false;  // the host knows the current lists are valid

@@ -154,14 +154,56 @@ __global__ void __launch_bounds__(128) k_density_pass(int n, int pass, DevParams
 }
 
 // ------------------------------------------------------- neighbour lists
-// One thread per particle scans the 3^DIM cells around it (uniform work per
-// candidate, only the append is predicated) and appends every j within the
-// margin-enlarged symmetric radius.  Counts beyond `cap` are recorded, not
-// stored, and flag a rebuild with a larger capacity.
-// The test runs in FP32 on the packed positions with a relative slack of
-// 4e-6 on r^2 (FP32 geometry errors are ~1e-7), and a list is declared valid
-// only up to h_i * (1 + margin) * (1 - 1e-4): every pair the exact FP64
-// criterion admits while each h stays within its limit is in the list.
+// A list holds every j within the margin-enlarged symmetric radius
+// R * max(h_i, h_j) * (1 + margin) of the h it was built with.  The tests run
+// in FP32 on the packed positions with a relative slack of 4e-6 on r^2 (FP32
+// geometry errors are ~1e-7), and a list is declared valid only up to
+// h_i * (1 + margin) * (1 - 1e-4): every pair the exact FP64 criterion admits
+// while each h stays within its limit is in the list.  Three passes: gather
+// (each particle's own search), scatter (big particles add themselves where
+// a smaller search cannot reach them), ordering of the scattered entries.
+
+// Grid of the scatter pass (a grid-stride loop over the big particles).
+constexpr int kScatterBlocks = 148 * 4;
+
+// FP32 squared distance from the packed positions, rounded op by op so that
+// it is the same whichever particle of the pair computes it.
+template <int DIM>
+__device__ __forceinline__ float sym_r2(const Grid& G, const float4& pa, int ca, const float4& pb, int cb) {
+  float dx, dy, dz;
+  rel_dx<DIM>(G, pa, ca, pb, cb, dx, dy, dz);
+  return __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+}
+
+// (Rg * h)^2 * slack, rounded op by op.
+__device__ __forceinline__ float reach2(float Rg, float h, float slack) {
+  const float rh = __fmul_rn(Rg, h);
+  return __fmul_rn(__fmul_rn(rh, rh), slack);
+}
+
+// Search half-width and cut-off of a particle: the grid's for a normal
+// particle, its own R * h * (1 + margin) for a big one.
+__device__ __forceinline__ void search_extent(const Grid& G, int dim, float Rg, float h, bool big, int& sw,
+                                              double& cut) {
+  sw = G.sw;
+  cut = G.cut * (1.0 + 1e-6);
+  if (!big) return;
+  cut = (double)Rg * (double)h * (1.0 + 1e-5);
+  for (int a = 0; a < dim; a++) {
+    const int s = (int)ceil(cut * G.inv_cs[a]);
+    sw = s > sw ? s : sw;
+  }
+}
+
+// Gather pass: every particle lists the j it finds in its own search.  A
+// normal particle searches the grid's +-sw stencil and keeps every normal j
+// with r < R * max(h_i, h_j) * (1 + margin); big j are left to the scatter
+// pass.  A big particle searches its own extended stencil and keeps normal j
+// under the same rule and big j within its own R * h_i * (1 + margin).
+// Positions are the packed FP32 cell-relative ones: per cell the particle's
+// position is shifted by the cell offset, so a candidate costs one float4
+// load.  Counts beyond `cap` are recorded, not stored, and flag a rebuild
+// with a larger capacity.
 template <int DIM>
 __global__ void __launch_bounds__(128) k_build_lists(int n, DevParams P, const Grid* __restrict__ grids,
                                                      const int* __restrict__ inst, const int* __restrict__ cell_start,
@@ -169,50 +211,138 @@ __global__ void __launch_bounds__(128) k_build_lists(int n, DevParams P, const G
                                                      const double* __restrict__ z, const double* __restrict__ h,
                                                      const float4* __restrict__ posf, const int* __restrict__ cellc,
                                                      float grow, int cap, int* __restrict__ idx,
-                                                     int* __restrict__ cnt_out, double* __restrict__ hlim,
+                                                     int* __restrict__ cnt_out, int* __restrict__ gcnt_out,
+                                                     double* __restrict__ hlim, int* __restrict__ big_idx,
                                                      DevScalars* sc) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const Grid& G = grid_of(grids, inst, i);
   const float4 pi = posf[i];
-  const float Rg = (float)P.R * grow;
-  const float rhi = Rg * pi.w, rhi2 = rhi * rhi;
+  const int ci = cellc[i];
+  const float Rg = __fmul_rn((float)P.R, grow);
   const float slack = 1.0f + 4e-6f;
+  const float rhi2 = reach2(Rg, pi.w, 1.0f);
+  const float hbig = G.h_bigf;
+  const bool big_i = pi.w > hbig;
+  int sw;
+  double cut;
+  search_extent(G, DIM, Rg, pi.w, big_i, sw, cut);
+  if (big_i) big_idx[atomicAdd(&sc->n_big, 1)] = i;
+  const float own2 = reach2(Rg, pi.w, slack);
   int* __restrict__ row = idx + (size_t)(i >> 5) * cap * 32 + (i & 31);
   int cnt = 0;
   int cxi, cyi, czi;
-  unpack_cell<DIM>(cellc[i], cxi, cyi, czi);
-  // Per cell (unwrapped coordinates) the in-cell position of i shifted by
-  // the cell offset; a candidate then costs one float4 load.
-  const int whole = 2 * G.sw + 1;
+  unpack_cell<DIM>(ci, cxi, cyi, czi);
+  const int whole = 2 * sw + 1;
   const bool mx = G.periodic[0] && G.nc[0] < whole, my = G.periodic[1] && G.nc[1] < whole,
              mz = DIM == 3 && G.periodic[2] && G.nc[2] < whole;
   const float Lx = (float)G.L[0], Ly = (float)G.L[1], Lz = (float)G.L[2];
   const float csx = G.csf[0], csy = G.csf[1], csz = G.csf[2];
-  for_each_cell_trimmed<DIM>(G, cell_start, x[i], y[i], DIM == 3 ? z[i] : 0.0, G.cut * (1.0 + 1e-6),
+  for_each_cell_trimmed<DIM>(G, sw, cell_start, x[i], y[i], DIM == 3 ? z[i] : 0.0, cut,
                              [&](int cxu, int cyu, int czu, int jb, int je) {
     const float sx = pi.x + (float)(cxi - cxu) * csx;
     const float sy = pi.y + (float)(cyi - cyu) * csy;
     const float sz = DIM == 3 ? pi.z + (float)(czi - czu) * csz : 0.f;
     for (int j = jb; j < je; j++) {
       const float4 pj = __ldg(posf + j);
-      float dx = sx - pj.x, dy = sy - pj.y, dz = DIM == 3 ? sz - pj.z : 0.f;
-      if (mx) dx = dx > 0.5f * Lx ? dx - Lx : (dx < -0.5f * Lx ? dx + Lx : dx);
-      if (my) dy = dy > 0.5f * Ly ? dy - Ly : (dy < -0.5f * Ly ? dy + Ly : dy);
-      if (mz) dz = dz > 0.5f * Lz ? dz - Lz : (dz < -0.5f * Lz ? dz + Lz : dz);
-      const float r2 = dx * dx + dy * dy + dz * dz;
-      const float rhj = Rg * pj.w;
-      if (r2 < fmaxf(rhi2, rhj * rhj) * slack) {
+      bool keep;
+      if (pj.w > hbig) {
+        // big j: kept here only by a big i, within i's own reach (the
+        // scatter pass adds it everywhere else)
+        keep = big_i && sym_r2<DIM>(G, pi, ci, pj, __ldg(cellc + j)) < own2;
+      } else {
+        float dx = sx - pj.x, dy = sy - pj.y, dz = DIM == 3 ? sz - pj.z : 0.f;
+        if (mx) dx = dx > 0.5f * Lx ? dx - Lx : (dx < -0.5f * Lx ? dx + Lx : dx);
+        if (my) dy = dy > 0.5f * Ly ? dy - Ly : (dy < -0.5f * Ly ? dy + Ly : dy);
+        if (mz) dz = dz > 0.5f * Lz ? dz - Lz : (dz < -0.5f * Lz ? dz + Lz : dz);
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        const float rhj = Rg * pj.w;
+        keep = r2 < fmaxf(rhi2, rhj * rhj) * slack;
+      }
+      if (keep) {
         if (cnt < cap) row[cnt * 32] = j;
         cnt++;
       }
     }
   });
-  cnt_out[i] = cnt < cap ? cnt : cap;
+  const int stored = cnt < cap ? cnt : cap;
+  cnt_out[i] = stored;
+  gcnt_out[i] = stored;
   hlim[i] = h[i] * (double)grow * (1.0 - 1e-4);
   if (cnt > cap) {
     atomicMax(&sc->list_max, cnt);
     atomicExch(&sc->relist, 1);
+  }
+}
+
+// Scatter pass: every big particle j searches its extended stencil and
+// appends itself to the list of each i with r < R * h_j * (1 + margin) that
+// did not keep j in its own gather pass (every normal i; a big i only beyond
+// its own reach).  The test is the gather pass's, from the other side, with
+// the same op-by-op rounding, so each pair is listed exactly once.
+template <int DIM>
+__global__ void __launch_bounds__(128) k_scatter_big(DevParams P, const Grid* __restrict__ grids,
+                                                     const int* __restrict__ inst, const int* __restrict__ cell_start,
+                                                     const double* __restrict__ x, const double* __restrict__ y,
+                                                     const double* __restrict__ z, const float4* __restrict__ posf,
+                                                     const int* __restrict__ cellc, float grow, int cap,
+                                                     int* __restrict__ idx, int* __restrict__ cnt,
+                                                     const int* __restrict__ big_idx, DevScalars* sc) {
+  const int nb = sc->n_big;
+  const float Rg = __fmul_rn((float)P.R, grow);
+  const float slack = 1.0f + 4e-6f;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nb; t += gridDim.x * blockDim.x) {
+    const int j = big_idx[t];
+    const Grid& G = grid_of(grids, inst, j);
+    const float4 pj = posf[j];
+    const int cj = cellc[j];
+    const float hbig = G.h_bigf;
+    const float reach_j = reach2(Rg, pj.w, slack);
+    int sw;
+    double cut;
+    search_extent(G, DIM, Rg, pj.w, true, sw, cut);
+    for_each_cell_trimmed<DIM>(G, sw, cell_start, x[j], y[j], DIM == 3 ? z[j] : 0.0, cut,
+                               [&](int, int, int, int ib, int ie) {
+      for (int i = ib; i < ie; i++) {
+        if (i == j) continue;
+        const float4 pi = __ldg(posf + i);
+        const float r2 = sym_r2<DIM>(G, pi, __ldg(cellc + i), pj, cj);
+        if (!(r2 < reach_j)) continue;
+        if (pi.w > hbig && r2 < reach2(Rg, pi.w, slack)) continue;  // i kept j itself
+        const int slot = atomicAdd(cnt + i, 1);
+        if (slot < cap) {
+          idx[(size_t)(i >> 5) * cap * 32 + (i & 31) + (size_t)slot * 32] = j;
+        } else {
+          atomicMax(&sc->list_max, slot + 1);
+          atomicExch(&sc->relist, 1);
+        }
+      }
+    });
+  }
+}
+
+// Order the scattered entries of every list by index (the scatter pass
+// appends them in whatever order its atomics resolve) and cap the counts.
+__global__ void __launch_bounds__(128) k_sort_appended(int n, int cap, int* __restrict__ idx, int* __restrict__ cnt,
+                                                       const int* __restrict__ gcnt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int c = cnt[i];
+  if (c > cap) {
+    c = cap;
+    cnt[i] = cap;
+  }
+  const int g = gcnt[i];
+  if (c - g < 2) return;
+  int* __restrict__ row = idx + (size_t)(i >> 5) * cap * 32 + (i & 31);
+  for (int a = g + 1; a < c; a++) {
+    const int v = row[a * 32];
+    int b = a - 1;
+    while (b >= g && row[b * 32] > v) {
+      row[(b + 1) * 32] = row[b * 32];
+      b--;
+    }
+    row[(b + 1) * 32] = v;
   }
 }
 
@@ -258,15 +388,25 @@ void launch_build_lists(Ctx* c, const MhdState* s, int n, cudaStream_t st) {
   if (n <= 0) return;
   TimedScope ts(c, MHD_TIMING_CELLS, st);
   const float grow = (float)(1.0 + c->list_margin);
-  if (c->P.dim == 3)
-    k_build_lists<3><<<(n + 127) / 128, 128, 0, st>>>(n, c->P, c->d_grids, c->inst, c->cell_start, s->x, s->y, s->z,
-                                                     s->h, c->posf, c->cellc, grow, c->list_cap, c->nbr_idx,
-                                                     c->nbr_cnt, c->nbr_hlim, c->d_sc);
-  else
-    k_build_lists<2><<<(n + 127) / 128, 128, 0, st>>>(n, c->P, c->d_grids, c->inst, c->cell_start, s->x, s->y, s->z,
-                                                     s->h, c->posf, c->cellc, grow, c->list_cap, c->nbr_idx,
-                                                     c->nbr_cnt, c->nbr_hlim, c->d_sc);
-  c->launches++;
+  cudaMemsetAsync(&c->d_sc->n_big, 0, sizeof(int), st);
+  const int nb = (n + 127) / 128;
+  if (c->P.dim == 3) {
+    k_build_lists<3><<<nb, 128, 0, st>>>(n, c->P, c->d_grids, c->inst, c->cell_start, s->x, s->y, s->z, s->h,
+                                         c->posf, c->cellc, grow, c->list_cap, c->nbr_idx, c->nbr_cnt, c->nbr_gcnt,
+                                         c->nbr_hlim, c->big_idx, c->d_sc);
+    k_scatter_big<3><<<kScatterBlocks, 128, 0, st>>>(c->P, c->d_grids, c->inst, c->cell_start, s->x, s->y, s->z,
+                                                     c->posf, c->cellc, grow, c->list_cap, c->nbr_idx, c->nbr_cnt,
+                                                     c->big_idx, c->d_sc);
+  } else {
+    k_build_lists<2><<<nb, 128, 0, st>>>(n, c->P, c->d_grids, c->inst, c->cell_start, s->x, s->y, s->z, s->h,
+                                         c->posf, c->cellc, grow, c->list_cap, c->nbr_idx, c->nbr_cnt, c->nbr_gcnt,
+                                         c->nbr_hlim, c->big_idx, c->d_sc);
+    k_scatter_big<2><<<kScatterBlocks, 128, 0, st>>>(c->P, c->d_grids, c->inst, c->cell_start, s->x, s->y, s->z,
+                                                     c->posf, c->cellc, grow, c->list_cap, c->nbr_idx, c->nbr_cnt,
+                                                     c->big_idx, c->d_sc);
+  }
+  k_sort_appended<<<nb, 128, 0, st>>>(n, c->list_cap, c->nbr_idx, c->nbr_cnt, c->nbr_gcnt);
+  c->launches += 3;
 }
 
 // ------------------------------------------------------------- dispatch

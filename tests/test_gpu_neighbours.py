@@ -81,3 +81,46 @@ def test_lists_hold_exact_neighbour_sets_jittered(maker):
     eng.warmup()
     eng.cells_build()
     _check(eng, prm, "jittered after warm-up")
+
+
+def _spread_h(ic, frac, factors, seed):
+    """A few particles get a much larger h: they become the grid's big
+    particles, whose pairs come from the extended search and the scatter."""
+    rng = np.random.default_rng(seed)
+    ic = dict(ic)
+    h = ic["h"].copy()
+    pick = rng.random(h.size) < frac
+    h[pick] *= rng.choice(factors, pick.sum())
+    ic["h"] = h
+    return ic
+
+
+@pytest.mark.parametrize("maker,frac", [(lambda: sc_.orszag_tang_2d(40, "quintic"), 0.03),
+                                        (lambda: sc_.blast_3d(14, "cubic"), 0.02),
+                                        (lambda: sc_.open_blob_2d(30), 0.05),
+                                        (lambda: sc_.blast_3d(12, "cubic"), 0.3)])
+def test_lists_exact_with_a_few_large_h(maker, frac):
+    ic, prm = maker()
+    ic = _spread_h(ic, frac, [1.3, 2.0, 3.5], seed=4)
+    eng = _engine(ic, prm)
+    eng.cells_build()
+    _check(eng, prm, f"large h (fraction {frac})")
+
+
+def test_batched_lists_exact_with_a_few_large_h():
+    from src.batch import BatchEngine
+    from src.engine import params_from_dict
+
+    a, prm = sc_.orszag_tang_2d(24, "quintic", seed=1)
+    b, _ = sc_.orszag_tang_2d(33, "quintic", seed=2)
+    ics = [_spread_h(a, 0.04, [2.0, 3.0], 5), _spread_h(b, 0.02, [1.5, 2.5], 6)]
+    eng = BatchEngine(params_from_dict(prm), ics)
+    eng.cells_build()
+    counts = eng.neighbour_counts().cpu().numpy()
+    for k in range(2):
+        sl = eng.instance(k)
+        st = {f: eng.pa[f][sl].cpu().numpy() for f in ("x", "y", "z", "h")}
+        ref = brute_counts(st["x"], st["y"], st["z"], st["h"], prm)
+        bad = np.nonzero(counts[sl] != ref)[0]
+        assert bad.size == 0, f"instance {k}: {bad.size} particles differ"
+    eng.close()
