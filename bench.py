@@ -257,8 +257,8 @@ def _timed(args, prec, dev, barrier, dist, world):
         ms_max = float(t.item())
     # kernel breakdown (uncaptured, identical kernels)
     st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
-    ms_k = (ctypes.c_double * 6)()
-    cnt_k = (ctypes.c_int64 * 6)()
+    ms_k = (ctypes.c_double * len(_abi.TIMING_KINDS))()
+    cnt_k = (ctypes.c_int64 * len(_abi.TIMING_KINDS))()
     pairs, cands = ctypes.c_int64(), ctypes.c_int64()
     lib.mhd_pair_counts(eng.ctx, ctypes.byref(pairs), ctypes.byref(cands), st)
     lib.mhd_timing_enable(eng.ctx, 1)

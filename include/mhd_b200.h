@@ -117,13 +117,14 @@ typedef struct MhdRhsStats {
 } MhdRhsStats;
 
 /* Kernel families timed with CUDA events when timing is enabled. */
-#define MHD_TIMING_KINDS 6
-#define MHD_TIMING_CELLS 0        /* grid reduction, key, radix sort, cell table, gather */
+#define MHD_TIMING_KINDS 7
+#define MHD_TIMING_CELLS 0        /* cell keys, radix sort, cell table, gather */
 #define MHD_TIMING_DENSITY 1      /* density passes */
 #define MHD_TIMING_PROLOGUE 2     /* force prologue (G2, G3, G5) */
 #define MHD_TIMING_FORCE 3        /* fused force pass (G4, G6-G10) */
 #define MHD_TIMING_DT 4           /* timestep reduction */
 #define MHD_TIMING_INTEGRATE 5    /* integrator stages / corrector-predictor */
+#define MHD_TIMING_LISTS 6        /* neighbour-list build (gather, scatter, ordering) */
 
 /* ---- library and context ---- */
 

@@ -386,7 +386,7 @@ void launch_neighbour_counts(Ctx* c, const MhdState* s, int n, int* out, cudaStr
 
 void launch_build_lists(Ctx* c, const MhdState* s, int n, cudaStream_t st) {
   if (n <= 0) return;
-  TimedScope ts(c, MHD_TIMING_CELLS, st);
+  TimedScope ts(c, MHD_TIMING_LISTS, st);
   const float grow = (float)(1.0 + c->list_margin);
   cudaMemsetAsync(&c->d_sc->n_big, 0, sizeof(int), st);
   const int nb = (n + 127) / 128;

@@ -87,7 +87,7 @@ EXPORTS = (
     "mhd_instance_count", "mhd_clock_set_all", "mhd_clock_get_all", "mhd_advance", "mhd_ctx_tune",
 )
 NOALLOC_MAX_N = 67108864
-TIMING_KINDS = ("cells", "density", "prologue", "force", "dt", "integrate")
+TIMING_KINDS = ("cells", "density", "prologue", "force", "dt", "integrate", "lists")
 
 
 def load(path: str = LIB_PATH):
