@@ -146,7 +146,7 @@ def measured_peaks():
 def profiled_traffic(n, precision):
     """DRAM bytes per force-pass launch from the committed ncu summary, scaled
     to n particles (traffic grows in proportion to the particles processed)."""
-    path = os.path.join(ROOT, "profiles", "force_pass_traffic.json")
+    path = os.path.join(ROOT, "profiles", "force_pass_blast96_traffic.json")
     if not os.path.exists(path):
         return None
     with open(path) as f:
