@@ -285,6 +285,30 @@ int mhd_advance(void* ctx, MhdState* a, MhdState* b, int64_t n, int32_t steps, i
    mhd_ctx_set_instances. */
 int mhd_ctx_tune(void* ctx, int32_t stencil, int32_t force_shape);
 
+/* ---- derivative form (forward mode) ----
+   No counterpart in the reference.  The literal PEC step (MHDStep with the
+   ten groups of src/scheme.py:66-81, single density pass) on dual numbers:
+   every double* of the MhdState points to n records of
+   (1 + MHD_TANGENT_DIRS) doubles {value, d/dp_1, ..., d/dp_DIRS}, p being
+   the caller's parameters (seeded through the initial state and through
+   alpha_max).  The context's parameters must have iterate = 0.  The step
+   size is a plain value: the adaptive rule is not differentiated (frozen
+   dt).  Neighbours: all-pairs search with the exact rule, so
+   n <= MHD_TANGENT_MAX_N.  alpha_max: host array of 1 + MHD_TANGENT_DIRS
+   doubles (value and derivatives), or null for the context's value. */
+#define MHD_TANGENT_DIRS 2
+#define MHD_TANGENT_MAX_N 65536
+int mhd_tangent_dirs(void);
+/* src/application.py:99-108: Bevol = B / rho, psi = 0, predicted copies. */
+int mhd_tangent_sync(void* ctx, MhdState* s, int64_t n, void* stream);
+/* One right-hand side (Integrator.compute_accelerations). */
+int mhd_tangent_rhs(void* ctx, MhdState* s, int64_t n, const double* alpha_max, void* stream);
+/* One PEC step with step size dt (PECIntegrator.one_timestep). */
+int mhd_tangent_step(void* ctx, MhdState* s, int64_t n, double dt, const double* alpha_max, void* stream);
+/* sum_i m_i |B_i|^2 / (2 mu0 rho_i) and its derivatives into
+   energy[1 + MHD_TANGENT_DIRS] (host; synchronising). */
+int mhd_tangent_magnetic_energy(void* ctx, const MhdState* s, int64_t n, double* energy, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

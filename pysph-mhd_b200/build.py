@@ -16,7 +16,10 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libmhd_b200.so")
 OBJ = os.path.join(HERE, "_build")
-SOURCES = ["mhd_abi.cu", "mhd_cells.cu", "mhd_pairs.cu", "mhd_force.cu", "mhd_integrate.cu", "mhd_noalloc.cu"]
+SOURCES = ["mhd_abi.cu", "mhd_cells.cu", "mhd_pairs.cu", "mhd_force.cu", "mhd_integrate.cu", "mhd_noalloc.cu",
+           "mhd_tangent.cu"]
+# The derivative form follows the reference's expression order: no FMA contraction.
+FILE_FLAGS = {"mhd_tangent.cu": ["--fmad=false"]}
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
          "--extended-lambda", "-I", os.path.join(ROOT, "include"), "-I", CSRC]
@@ -35,7 +38,7 @@ def build(force=False, verbose=False):
 
     def compile_one(src):
         obj = os.path.join(OBJ, src.replace(".cu", ".o"))
-        cmd = [NVCC, *FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
+        cmd = [NVCC, *FLAGS, *FILE_FLAGS.get(src, []), "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             cmd += ["-Xptxas", "-v"]
         r = subprocess.run(cmd, capture_output=True, text=True)

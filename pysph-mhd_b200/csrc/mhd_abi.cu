@@ -691,6 +691,7 @@ int mhd_ctx_destroy(void* ctx) {
   cudaFree(c->d_stage);
   drop_graphs(c);
   if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
+  cudaFree(c->tan_work);
   delete c;
   return MHD_OK;
 }

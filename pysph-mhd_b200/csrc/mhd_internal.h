@@ -49,6 +49,7 @@ struct Ctx {
   int64_t generation = 0;         // bumped when a buffer captured by a graph is reallocated
   int graph_passes = 8;           // density passes captured per right-hand side
   cudaStream_t cap_stream = nullptr;
+  void* tan_work = nullptr;  // derivative form: new h / energy partials (dual records)
   struct GraphEntry {
     MhdState a, b;
     int64_t n;

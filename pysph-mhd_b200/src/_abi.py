@@ -85,6 +85,7 @@ EXPORTS = (
     "mhd_corrector_predictor", "mhd_step", "mhd_timing_enable", "mhd_timing_read", "mhd_probe_fma_peak",
     "mhd_pair_counts", "mhd_timestep_noalloc", "mhd_neighbour_counts", "mhd_ctx_set_instances",
     "mhd_instance_count", "mhd_clock_set_all", "mhd_clock_get_all", "mhd_advance", "mhd_ctx_tune",
+    "mhd_tangent_dirs", "mhd_tangent_sync", "mhd_tangent_rhs", "mhd_tangent_step", "mhd_tangent_magnetic_energy",
 )
 NOALLOC_MAX_N = 67108864
 TIMING_KINDS = ("cells", "density", "prologue", "force", "dt", "integrate", "lists")
@@ -141,6 +142,11 @@ def load(path: str = LIB_PATH):
     lib.mhd_clock_get_all.argtypes = [vp, ctypes.POINTER(dbl), ctypes.POINTER(dbl), vp]
     lib.mhd_advance.argtypes = [vp, sp, sp, i64, i32, i32, i32, vp]
     lib.mhd_ctx_tune.argtypes = [vp, i32, i32]
+    dp = ctypes.POINTER(dbl)
+    lib.mhd_tangent_sync.argtypes = [vp, sp, i64, vp]
+    lib.mhd_tangent_rhs.argtypes = [vp, sp, i64, dp, vp]
+    lib.mhd_tangent_step.argtypes = [vp, sp, i64, dbl, dp, vp]
+    lib.mhd_tangent_magnetic_energy.argtypes = [vp, sp, i64, dp, vp]
     _lib = lib
     return lib
 
