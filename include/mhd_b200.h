@@ -309,6 +309,29 @@ int mhd_tangent_step(void* ctx, MhdState* s, int64_t n, double dt, const double*
    energy[1 + MHD_TANGENT_DIRS] (host; synchronising). */
 int mhd_tangent_magnetic_energy(void* ctx, const MhdState* s, int64_t n, double* energy, void* stream);
 
+/* ---- derivative form (reverse mode, checkpointed) ----
+   No counterpart in the reference.  L = sum_i m_i |B_i|^2 / (2 mu0 rho_i)
+   after `steps` literal PEC steps from the state in `s` (plain FP64 fields;
+   single density pass, n <= MHD_TANGENT_MAX_N), and its adjoint:
+   lambda0 = dL/dS_0 over the MHD_ADJOINT_FIELDS step-state fields
+   (mhd_adjoint_field_name order, field-major, device, fields x n) and
+   dL/d alpha_max through the steps.  The step sizes are frozen: on input
+   dts[k] >= 0 is used as given; a negative dts[k] (k >= 1) is replaced by
+   the adaptive rule on the values of the state before step k (clipped to
+   tf), so the forward call returns the sequence it used.  `checkpoints`:
+   device array of (ceil(steps / every) + 1) x fields x n doubles; the
+   forward call keeps the state every `every` steps there, the backward
+   call re-runs each segment from its checkpoint with a tape and walks it
+   backwards.  Local Jacobians come from dual-number evaluation of the same
+   step functions; the energy limiter's time scale is frozen like dt. */
+#define MHD_ADJOINT_FIELDS 24
+int mhd_adjoint_field_count(void);
+const char* mhd_adjoint_field_name(int32_t k);
+int mhd_adjoint_forward(void* ctx, const MhdState* s, int64_t n, int32_t steps, double* dts, int32_t every,
+                        double* checkpoints, double* loss, void* stream);
+int mhd_adjoint_backward(void* ctx, const MhdState* s, int64_t n, int32_t steps, const double* dts, int32_t every,
+                         const double* checkpoints, double* lambda0, double* dloss_dalpha_max, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -17,9 +17,9 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libmhd_b200.so")
 OBJ = os.path.join(HERE, "_build")
 SOURCES = ["mhd_abi.cu", "mhd_cells.cu", "mhd_pairs.cu", "mhd_force.cu", "mhd_integrate.cu", "mhd_noalloc.cu",
-           "mhd_tangent.cu"]
-# The derivative form follows the reference's expression order: no FMA contraction.
-FILE_FLAGS = {"mhd_tangent.cu": ["--fmad=false"]}
+           "mhd_tangent.cu", "mhd_adjoint.cu"]
+# The derivative forms follow the reference's expression order: no FMA contraction.
+FILE_FLAGS = {"mhd_tangent.cu": ["--fmad=false"], "mhd_adjoint.cu": ["--fmad=false"]}
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
          "--extended-lambda", "-I", os.path.join(ROOT, "include"), "-I", CSRC]

@@ -692,6 +692,7 @@ int mhd_ctx_destroy(void* ctx) {
   drop_graphs(c);
   if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
   cudaFree(c->tan_work);
+  cudaFree(c->adj_buf);
   delete c;
   return MHD_OK;
 }

@@ -1,0 +1,944 @@
+// mhd_adjoint.cu -- reverse-mode (adjoint) derivative of the SPMHD step loop.
+//
+// Differentiates L = sum_i m_i |B_i|^2 / (2 mu0 rho_i) after K literal PEC
+// steps (MHDStep + the ten groups of src/scheme.py:66-81, single density
+// pass, step sizes given and frozen) with respect to the state at the first
+// step and to alpha_max.  The forward sweep keeps the 24-field step state
+// every `every` steps (checkpoints); the reverse sweep re-runs each segment
+// from its checkpoint with a tape of the intermediates (predicted state,
+// density, EOS, Cullen-Dehnen and force sums) and walks it backwards.
+//
+// Every stage is a pair sum or a pointwise map of mhd_step_fns.cuh.  Its
+// vector-Jacobian product is formed from the local Jacobian of that map,
+// obtained by evaluating the same function on dual numbers seeded with the
+// identity over the stage's per-particle inputs: pointwise maps and posts
+// per particle, pair terms per pair in gather form (a particle collects the
+// terms in which it is the i side and those in which it is the j side, so
+// there are no atomics).  The energy limiter's time scale (from dt_cfl) is
+// held at its value, like the step size.  Neighbours: all-pairs search with
+// the exact rule.  Compiled with --fmad=false like the forward-mode file.
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "mhd_common.cuh"
+#include "mhd_dual.cuh"
+#include "mhd_internal.h"
+#include "mhd_step_fns.cuh"
+
+namespace mhd {
+namespace adj {
+
+constexpr int kTile = 128;
+constexpr int NS = kStateDirs;  // 24 state fields
+// state field offsets (field-major arrays of n)
+enum { SX = 0, SV = 3, SE = 6, SH = 7, SA1 = 8, SB = 9, SPSI = 12, SA = 13, SAE = 16, SAH = 17, SALOC = 18,
+       SCS = 19, SAB = 20, SAPSI = 23 };
+// tape offsets (per step): the input state, the predicted state, the density
+// pass, the EOS, the Cullen-Dehnen sums and the force sums
+enum { T_S = 0, T_X = 24, T_VH = 27, T_VP = 30, T_EH = 33, T_EP = 34, T_HP = 35, T_A1 = 36, T_BH = 37, T_BP = 40,
+       T_PSIH = 43, T_PSIP = 44, T_RS = 45, T_DW = 46, T_OM = 47, T_HN = 48, T_RHO = 49, T_P = 50, T_CS = 51,
+       T_B = 52, T_CD = 55, T_ALOC = 82, T_FS = 83, T_DTCFL = 97, NT = 98 };
+// workspace offsets: lambdas of the intermediates, the sum adjoints and the
+// lambdas of the rates
+enum { L_X = 0, L_VH = 3, L_VP = 6, L_EH = 9, L_EP = 10, L_HP = 11, L_A1 = 12, L_BH = 13, L_BP = 16, L_PSIH = 19,
+       L_PSIP = 20, L_HN = 21, L_OM = 22, L_RHO = 23, L_P = 24, L_CS = 25, L_B = 26, M_D = 29, M_CD = 31, M_F = 58,
+       L_RATES = 72, NL = 81 };  // L_RATES: au 3, ae, ah, ab 3, apsi
+
+// All j (ascending) with r2 < (R h_i)^2 or r2 < (R h_j)^2 for the positions
+// x, y, z and smoothing lengths h, self included; f(j, x_i - x_j min image).
+template <int DIM, class F>
+__device__ inline void all_pairs(int n, const DevParams& P, int i, const double* x, const double* y, const double* z,
+                                 const double* h, F&& f) {
+  __shared__ double4 sh[kTile];
+  const bool active = i < n;
+  const double xi = active ? x[i] : 0.0, yi = active ? y[i] : 0.0, zi = active && DIM == 3 ? z[i] : 0.0;
+  const double rhi2 = active ? rh2_exact(P.R, h[i]) : 0.0;
+  for (int base = 0; base < n; base += kTile) {
+    const int j = base + threadIdx.x;
+    if (j < n) sh[threadIdx.x] = make_double4(x[j], y[j], DIM == 3 ? z[j] : 0.0, h[j]);
+    __syncthreads();
+    if (active) {
+      const int m = n - base < kTile ? n - base : kTile;
+      for (int t = 0; t < m; t++) {
+        const double4 q = sh[t];
+        const double dx = min_image(xi - q.x, P.L[0], P.half[0], P.periodic[0]);
+        const double dy = min_image(yi - q.y, P.L[1], P.half[1], P.periodic[1]);
+        const double dz = DIM == 3 ? min_image(zi - q.z, P.L[2], P.half[2], P.periodic[2]) : 0.0;
+        const double r2 = r2_exact(dx, dy, dz);
+        if (r2 < rhi2 || r2 < rh2_exact(P.R, q.w)) f(base + t, dx, dy, dz);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <int N>
+__device__ inline Dual<N> seeded(double v, int k) {
+  Dual<N> r(v);
+  if (k >= 0) r.d[k] = 1.0;
+  return r;
+}
+
+struct Args {
+  int n;
+  DevParams P;
+  double dt;
+  double amax;
+  const double* m;
+  const int* itype;
+  const double* s_in;      // forward: S_n (NS x n)
+  double* s_out;           // forward: S_{n+1}
+  const double* tape;      // this step's tape (NT x n)
+  double* tape_w;          // forward: tape written
+  const double* lam_next;  // reverse: lambda(S_{n+1})
+  double* lam;             // reverse: lambda(S_n)
+  double* w;               // reverse: workspace (NL x n)
+  double* g_amax;          // reverse: per-particle dL/d alpha_max (accumulating over steps)
+  const double* s_final;   // reverse, last step: S_K (loss terms)
+  double* dta_out;         // forward: dt_adapt of the step (adaptive step sizes)
+};
+
+#define TP(k, i) a.tape_w[(size_t)(k) * a.n + (i)]
+#define TR(k, i) a.tape[(size_t)(k) * a.n + (i)]
+#define SI(k, i) a.s_in[(size_t)(k) * a.n + (i)]
+#define SO(k, i) a.s_out[(size_t)(k) * a.n + (i)]
+#define LN(k, i) a.lam_next[(size_t)(k) * a.n + (i)]
+#define LS(k, i) a.lam[(size_t)(k) * a.n + (i)]
+#define W(k, i) a.w[(size_t)(k) * a.n + (i)]
+
+template <class D>
+__device__ inline StepState<D> state_at(const double* s, int n, int i, int seed_base) {
+  StepState<D> q;
+  auto g = [&](int k) { return seeded<sizeof(D) / sizeof(double) - 1>(s[(size_t)k * n + i], seed_base < 0 ? -1 : k); };
+  for (int c = 0; c < 3; c++) {
+    q.x[c] = g(SX + c);
+    q.v[c] = g(SV + c);
+    q.bev[c] = g(SB + c);
+    q.a[c] = g(SA + c);
+    q.abev[c] = g(SAB + c);
+  }
+  q.e = g(SE);
+  q.h = g(SH);
+  q.alpha1 = g(SA1);
+  q.psi = g(SPSI);
+  q.ae = g(SAE);
+  q.ah = g(SAH);
+  q.aloc = g(SALOC);
+  q.cs = g(SCS);
+  q.apsi = g(SAPSI);
+  return q;
+}
+
+__device__ inline StepState<double> state_values(const double* s, int n, int i) {
+  StepState<double> q;
+  auto g = [&](int k) { return s[(size_t)k * n + i]; };
+  for (int c = 0; c < 3; c++) {
+    q.x[c] = g(SX + c);
+    q.v[c] = g(SV + c);
+    q.bev[c] = g(SB + c);
+    q.a[c] = g(SA + c);
+    q.abev[c] = g(SAB + c);
+  }
+  q.e = g(SE);
+  q.h = g(SH);
+  q.alpha1 = g(SA1);
+  q.psi = g(SPSI);
+  q.ae = g(SAE);
+  q.ah = g(SAH);
+  q.aloc = g(SALOC);
+  q.cs = g(SCS);
+  q.apsi = g(SAPSI);
+  return q;
+}
+
+// Side of particle i from a tape, as dual numbers seeded at `base` (or not).
+template <class D>
+__device__ inline Side<D> side_at(const double* t, int n, int i, int base) {
+  auto g = [&](int k, int s) {
+    D r(t[(size_t)k * n + i]);
+    if (base >= 0) r.d[base + s] = 1.0;
+    return r;
+  };
+  Side<D> s;
+  s.h = g(T_HN, 0);
+  s.rho = g(T_RHO, 1);
+  s.p = g(T_P, 2);
+  s.omega = g(T_OM, 3);
+  s.cs = g(T_CS, 4);
+  for (int c = 0; c < 3; c++) {
+    s.b[c] = g(T_B + c, 5 + c);
+    s.v[c] = g(T_VP + c, 8 + c);
+  }
+  s.e = g(T_EP, 11);
+  s.alpha = g(T_A1, 12);
+  s.psi = g(T_PSIP, 13);
+  return s;
+}
+
+__device__ inline Side<double> side_values(const double* t, int n, int i) {
+  auto g = [&](int k) { return t[(size_t)k * n + i]; };
+  Side<double> s;
+  s.h = g(T_HN);
+  s.rho = g(T_RHO);
+  s.p = g(T_P);
+  s.omega = g(T_OM);
+  s.cs = g(T_CS);
+  for (int c = 0; c < 3; c++) {
+    s.b[c] = g(T_B + c);
+    s.v[c] = g(T_VP + c);
+  }
+  s.e = g(T_EP);
+  s.alpha = g(T_A1);
+  s.psi = g(T_PSIP);
+  return s;
+}
+
+// ====================================================== taped forward step
+__global__ void __launch_bounds__(256) k_f_predict(Args a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n) return;
+  for (int k = 0; k < NS; k++) TP(T_S + k, i) = SI(k, i);
+  const StepState<double> s = state_values(a.s_in, a.n, i);
+  Predicted<double> o;
+  f_predict(a.P, s, a.itype[i] == 1, a.dt, o);
+  for (int c = 0; c < 3; c++) {
+    TP(T_X + c, i) = o.x[c];
+    TP(T_VH + c, i) = o.vhalf[c];
+    TP(T_VP + c, i) = o.vpred[c];
+    TP(T_BH + c, i) = o.bhalf[c];
+    TP(T_BP + c, i) = o.bpred[c];
+  }
+  TP(T_EH, i) = o.ehalf;
+  TP(T_EP, i) = o.epred;
+  TP(T_HP, i) = o.h;
+  TP(T_A1, i) = o.alpha1;
+  TP(T_PSIH, i) = o.psihalf;
+  TP(T_PSIP, i) = o.psipred;
+}
+
+template <int K, int DIM>
+__global__ void __launch_bounds__(kTile) k_f_density(Args a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = a.n;
+  const double* X = a.tape_w + (size_t)T_X * n;
+  const double* HP = a.tape_w + (size_t)T_HP * n;
+  double rho = 0.0, dwdh = 0.0;
+  const double hi = i < n ? HP[i] : 1.0;
+  all_pairs<DIM>(n, a.P, i, X, X + n, X + 2 * n, HP, [&](int j, double dx, double dy, double dz) {
+    const double xij[3] = {dx, dy, dz};
+    f_density_pair<K, DIM>(a.P.norm, xij, hi, a.m[j], rho, dwdh);
+  });
+  if (i >= n) return;
+  double om, hn;
+  f_density_post<DIM>(a.P.hfact, hi, a.m[i], rho, dwdh, om, hn);
+  TP(T_RS, i) = rho;
+  TP(T_DW, i) = dwdh;
+  TP(T_OM, i) = om;
+  TP(T_HN, i) = hn;
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(256) k_f_prologue(Args a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n) return;
+  const double bp[3] = {TP(T_BP, i), TP(T_BP + 1, i), TP(T_BP + 2, i)};
+  double rho, p, cs, b[3];
+  f_prologue<DIM>(a.P, TP(T_HN, i), a.m[i], TP(T_EP, i), bp, rho, p, cs, b);
+  TP(T_RHO, i) = rho;
+  TP(T_P, i) = p;
+  TP(T_CS, i) = cs;
+  for (int c = 0; c < 3; c++) TP(T_B + c, i) = b[c];
+}
+
+template <int K, int DIM>
+__global__ void __launch_bounds__(kTile) k_f_cd(Args a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = a.n;
+  const double* X = a.tape_w + (size_t)T_X * n;
+  const double* HN = a.tape_w + (size_t)T_HN * n;
+  double r[6] = {}, vv[9] = {}, aa[9] = {};
+  const int ii = i < n ? i : 0;
+  const double hi = HN[ii];
+  all_pairs<DIM>(n, a.P, i, X, X + n, X + 2 * n, HN, [&](int j, double dx, double dy, double dz) {
+    const double xij[3] = {dx, dy, dz};
+    double dv[3], da[3];
+    for (int c = 0; c < 3; c++) {
+      dv[c] = TP(T_VP + c, i) - TP(T_VP + c, j);
+      da[c] = SI(SA + c, i) - SI(SA + c, j);
+    }
+    f_cd_pair<K, DIM>(a.P.norm, xij, hi, a.m[j], dv, da, r, vv, aa);
+  });
+  if (i >= n) return;
+  for (int k = 0; k < 6; k++) TP(T_CD + k, i) = r[k];
+  for (int k = 0; k < 9; k++) {
+    TP(T_CD + 6 + k, i) = vv[k];
+    TP(T_CD + 15 + k, i) = aa[k];
+  }
+  TP(T_ALOC, i) = f_cd_post(r, vv, aa, TP(T_OM, i), TP(T_RHO, i), hi, TP(T_CS, i), a.amax, a.P.alpha_min);
+}
+
+template <int K, int DIM>
+__global__ void __launch_bounds__(kTile) k_f_force(Args a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = a.n;
+  const double* X = a.tape_w + (size_t)T_X * n;
+  const double* HN = a.tape_w + (size_t)T_HN * n;
+  const Side<double> I = side_values(a.tape_w, n, i < n ? i : 0);
+  FSums<double> S;
+  S.zero();
+  all_pairs<DIM>(n, a.P, i, X, X + n, X + 2 * n, HN, [&](int j, double dx, double dy, double dz) {
+    const double xij[3] = {dx, dy, dz};
+    f_force_pair<K, DIM>(a.P, I, side_values(a.tape_w, n, j), a.m[j], xij, S);
+  });
+  if (i >= n) return;
+  double* sp[kFSumDirs];
+  fsum_ptrs(S, sp);
+  for (int k = 0; k < kFSumDirs; k++) TP(T_FS + k, i) = *sp[k];
+  TP(T_DTCFL, i) = S.dtcfl;
+  FOut<double> o;
+  f_force_post<DIM>(a.P, I, S, o);
+  // S_{n+1}: the rates, stage2 (src/integrator.py:68-82) and the carried fields
+  const double dtb2 = a.itype[i] == 1 ? 0.5 * a.dt : 0.0;
+  for (int c = 0; c < 3; c++) {
+    SO(SX + c, i) = TP(T_X + c, i);
+    SO(SA + c, i) = o.au[c];
+    SO(SAB + c, i) = o.ab[c];
+    SO(SV + c, i) = TP(T_VH + c, i) + dtb2 * o.au[c];
+    SO(SB + c, i) = TP(T_BH + c, i) + dtb2 * o.ab[c];
+  }
+  SO(SE, i) = TP(T_EH, i) + dtb2 * o.ae;
+  SO(SPSI, i) = TP(T_PSIH, i) + dtb2 * o.apsi;
+  SO(SH, i) = TP(T_HN, i);
+  SO(SA1, i) = TP(T_A1, i);
+  SO(SAE, i) = o.ae;
+  SO(SAH, i) = o.ah;
+  SO(SALOC, i) = TP(T_ALOC, i);
+  SO(SCS, i) = TP(T_CS, i);
+  SO(SAPSI, i) = o.apsi;
+  if (a.dta_out) a.dta_out[i] = o.dta;
+}
+
+// min over particles (one block): the adaptive step size.
+__global__ void __launch_bounds__(256) k_min(int n, const double* v, double* out) {
+  __shared__ double sh[256];
+  double m = INFINITY;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) m = fmin(m, v[i]);
+  sh[threadIdx.x] = m;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] = fmin(sh[threadIdx.x], sh[threadIdx.x + o]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = sh[0];
+}
+
+// L = sum m |Bevol rho|^2 / (2 mu0 rho) with rho of the last right-hand side.
+__global__ void __launch_bounds__(256) k_f_energy(int n, double mu0, const double* m, const double* s,
+                                                  const double* tape, double* part) {
+  __shared__ double sh[256];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double e = 0.0;
+  if (i < n) {
+    const double rho = tape[(size_t)T_RHO * n + i];
+    double b2 = 0.0;
+    for (int c = 0; c < 3; c++) {
+      const double b = s[(size_t)(SB + c) * n + i] * rho;
+      b2 += b * b;
+    }
+    e = m[i] * b2 / (2.0 * mu0 * rho);
+  }
+  sh[threadIdx.x] = e;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+
+__global__ void k_sum_blocks(int nb, const double* part, double* out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double s = 0.0;
+  for (int b = 0; b < nb; b++) s += part[b];
+  *out = s;
+}
+
+// ============================================================ reverse step
+// Loss seed: lambda(Bevol_K) = m Bevol rho / mu0 (the rho term goes to the
+// last step's EOS, see k_r_correct).
+__global__ void __launch_bounds__(256) k_r_seed(Args a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n) return;
+  double* lam = const_cast<double*>(a.lam_next);
+  for (int k = 0; k < NS; k++) lam[(size_t)k * a.n + i] = 0.0;
+  const double rho = TR(T_RHO, i);
+  for (int c = 0; c < 3; c++)
+    lam[(size_t)(SB + c) * a.n + i] = a.m[i] * a.s_final[(size_t)(SB + c) * a.n + i] * rho / a.P.mu0;
+}
+
+// Stage2 and the carried fields (the forward k_f_force tail) reversed.
+__global__ void __launch_bounds__(256) k_r_correct(Args a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n) return;
+  for (int k = 0; k < NL; k++) W(k, i) = 0.0;
+  for (int k = 0; k < NS; k++) LS(k, i) = 0.0;
+  const double dtb2 = a.itype[i] == 1 ? 0.5 * a.dt : 0.0;
+  for (int c = 0; c < 3; c++) {
+    W(L_X + c, i) = LN(SX + c, i);
+    W(L_VH + c, i) = LN(SV + c, i);
+    W(L_RATES + c, i) = LN(SA + c, i) + dtb2 * LN(SV + c, i);
+    W(L_BH + c, i) = LN(SB + c, i);
+    W(L_RATES + 5 + c, i) = LN(SAB + c, i) + dtb2 * LN(SB + c, i);
+  }
+  W(L_EH, i) = LN(SE, i);
+  W(L_RATES + 3, i) = LN(SAE, i) + dtb2 * LN(SE, i);
+  W(L_RATES + 4, i) = LN(SAH, i);
+  W(L_PSIH, i) = LN(SPSI, i);
+  W(L_RATES + 8, i) = LN(SAPSI, i) + dtb2 * LN(SPSI, i);
+  W(L_HN, i) = LN(SH, i);
+  W(L_A1, i) = LN(SA1, i);
+  W(L_CS, i) = LN(SCS, i);
+  if (a.s_final) {
+    double b2 = 0.0;
+    for (int c = 0; c < 3; c++) {
+      const double b = a.s_final[(size_t)(SB + c) * a.n + i];
+      b2 += b * b;
+    }
+    W(L_RHO, i) += a.m[i] * b2 / (2.0 * a.P.mu0);
+  }
+}
+
+// Force posts (G6 post, G7, G9 post, G10) reversed: lambda of the side of i
+// and the sum adjoints mu_F.
+template <int DIM>
+__global__ void __launch_bounds__(64) k_r_force_post(Args a) {
+  using D = Dual<kSideDirs + kFSumDirs>;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n) return;
+  const Side<D> I = side_at<D>(a.tape, a.n, i, 0);
+  FSums<D> S;
+  S.zero();
+  D* sp[kFSumDirs];
+  fsum_ptrs(S, sp);
+  for (int k = 0; k < kFSumDirs; k++) *sp[k] = seeded<kSideDirs + kFSumDirs>(TR(T_FS + k, i), kSideDirs + k);
+  S.dtcfl = D(TR(T_DTCFL, i));
+  FOut<D> o;
+  f_force_post<DIM>(a.P, I, S, o);
+  const D* out[kFOutDirs] = {&o.au[0], &o.au[1], &o.au[2], &o.ae, &o.ah, &o.ab[0], &o.ab[1], &o.ab[2], &o.apsi};
+  double g[kSideDirs + kFSumDirs];
+  for (int d = 0; d < kSideDirs + kFSumDirs; d++) {
+    double s = 0.0;
+    for (int q = 0; q < kFOutDirs; q++) s += W(L_RATES + q, i) * out[q]->d[d];
+    g[d] = s;
+  }
+  W(L_HN, i) += g[0];
+  W(L_RHO, i) += g[1];
+  W(L_P, i) += g[2];
+  W(L_OM, i) += g[3];
+  W(L_CS, i) += g[4];
+  for (int c = 0; c < 3; c++) {
+    W(L_B + c, i) += g[5 + c];
+    W(L_VP + c, i) += g[8 + c];
+  }
+  W(L_EP, i) += g[11];
+  W(L_A1, i) += g[12];
+  W(L_PSIP, i) += g[13];
+  for (int k = 0; k < kFSumDirs; k++) W(M_F + k, i) = g[kSideDirs + k];
+}
+
+__device__ inline void add_side(const Args& a, int i, const double* g, double sign_x, const double* gx) {
+  W(L_HN, i) += g[0];
+  W(L_RHO, i) += g[1];
+  W(L_P, i) += g[2];
+  W(L_OM, i) += g[3];
+  W(L_CS, i) += g[4];
+  for (int c = 0; c < 3; c++) {
+    W(L_B + c, i) += g[5 + c];
+    W(L_VP + c, i) += g[8 + c];
+    W(L_X + c, i) += sign_x * gx[c];
+  }
+  W(L_EP, i) += g[11];
+  W(L_A1, i) += g[12];
+  W(L_PSIP, i) += g[13];
+}
+
+// Force pair terms reversed, gather form: particle k collects the terms of
+// the pairs (k, j) through its i side and x_k, and of the pairs (j, k)
+// through its j side and x_k.
+template <int K, int DIM>
+__global__ void __launch_bounds__(kTile) k_r_force_pair(Args a) {
+  using D = Dual<kSideDirs + 3>;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = a.n;
+  const double* X = a.tape + (size_t)T_X * n;
+  const double* HN = a.tape + (size_t)T_HN * n;
+  const int kk = k < n ? k : 0;
+  const Side<D> Kseed = side_at<D>(a.tape, n, kk, 0);
+  const Side<D> Kval = side_at<D>(a.tape, n, kk, -1);
+  double gs[kSideDirs] = {}, gx[3] = {};
+  all_pairs<DIM>(n, a.P, k, X, X + n, X + 2 * n, HN, [&](int j, double dx, double dy, double dz) {
+    const Side<D> Jval = side_at<D>(a.tape, n, j, -1);
+    // (k, j): k is the i side
+    {
+      const D xij[3] = {seeded<kSideDirs + 3>(dx, kSideDirs), seeded<kSideDirs + 3>(dy, kSideDirs + 1),
+                        seeded<kSideDirs + 3>(dz, kSideDirs + 2)};
+      FSums<D> S;
+      S.zero();
+      f_force_pair<K, DIM>(a.P, Kseed, Jval, D(a.m[j]), xij, S);
+      D* sp[kFSumDirs];
+      fsum_ptrs(S, sp);
+      for (int d = 0; d < kSideDirs + 3; d++) {
+        double s = 0.0;
+        for (int q = 0; q < kFSumDirs; q++) s += W(M_F + q, k) * sp[q]->d[d];
+        if (d < kSideDirs) gs[d] += s;
+        else gx[d - kSideDirs] += s;
+      }
+    }
+    // (j, k): k is the j side, x_j - x_k = -(dx, dy, dz)
+    {
+      const D xji[3] = {seeded<kSideDirs + 3>(-dx, kSideDirs), seeded<kSideDirs + 3>(-dy, kSideDirs + 1),
+                        seeded<kSideDirs + 3>(-dz, kSideDirs + 2)};
+      FSums<D> S;
+      S.zero();
+      f_force_pair<K, DIM>(a.P, Jval, Kseed, D(a.m[k]), xji, S);
+      D* sp[kFSumDirs];
+      fsum_ptrs(S, sp);
+      for (int d = 0; d < kSideDirs + 3; d++) {
+        double s = 0.0;
+        for (int q = 0; q < kFSumDirs; q++) s += W(M_F + q, j) * sp[q]->d[d];
+        if (d < kSideDirs) gs[d] += s;
+        else gx[d - kSideDirs] -= s;
+      }
+    }
+  });
+  (void)Kval;
+  if (k >= n) return;
+  add_side(a, k, gs, 1.0, gx);
+}
+
+// Cullen-Dehnen post reversed: the sum adjoints mu_CD and the lambdas of
+// Omega, rho, h, cs; alpha_max's derivative accumulates per particle.
+__global__ void __launch_bounds__(64) k_r_cd_post(Args a) {
+  using D = Dual<32>;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n) return;
+  D r[6], vv[9], aa[9];
+  for (int k = 0; k < 6; k++) r[k] = seeded<32>(TR(T_CD + k, i), k);
+  for (int k = 0; k < 9; k++) {
+    vv[k] = seeded<32>(TR(T_CD + 6 + k, i), 6 + k);
+    aa[k] = seeded<32>(TR(T_CD + 15 + k, i), 15 + k);
+  }
+  const D om = seeded<32>(TR(T_OM, i), 27), rho = seeded<32>(TR(T_RHO, i), 28);
+  const D h = seeded<32>(TR(T_HN, i), 29), cs = seeded<32>(TR(T_CS, i), 30);
+  const D amax = seeded<32>(a.amax, 31);
+  const D al = f_cd_post(r, vv, aa, om, rho, h, cs, amax, a.P.alpha_min);
+  const double lam = LN(SALOC, i);
+  for (int k = 0; k < 27; k++) W(M_CD + k, i) = lam * al.d[k];
+  W(L_OM, i) += lam * al.d[27];
+  W(L_RHO, i) += lam * al.d[28];
+  W(L_HN, i) += lam * al.d[29];
+  W(L_CS, i) += lam * al.d[30];
+  a.g_amax[i] += lam * al.d[31];
+}
+
+// Cullen-Dehnen pair terms reversed (gather form, as the force pairs).
+template <int K, int DIM>
+__global__ void __launch_bounds__(kTile) k_r_cd_pair(Args a) {
+  using D = Dual<10>;  // x_ij 3, h_i, dv 3, da 3
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = a.n;
+  const double* X = a.tape + (size_t)T_X * n;
+  const double* HN = a.tape + (size_t)T_HN * n;
+  const int kk = k < n ? k : 0;
+  double gx[3] = {}, gh = 0.0, gv[3] = {}, ga[3] = {};
+  all_pairs<DIM>(n, a.P, k, X, X + n, X + 2 * n, HN, [&](int j, double dx, double dy, double dz) {
+    for (int side = 0; side < 2; side++) {
+      // side 0: pair (k, j); side 1: pair (j, k)
+      const int ii = side ? j : kk, jj = side ? kk : j;
+      const double sgn = side ? -1.0 : 1.0;
+      const D xij[3] = {seeded<10>(sgn * dx, 0), seeded<10>(sgn * dy, 1), seeded<10>(sgn * dz, 2)};
+      const D hi = seeded<10>(HN[ii], side ? -1 : 3);
+      D dv[3], da[3];
+      for (int c = 0; c < 3; c++) {
+        dv[c] = seeded<10>(TR(T_VP + c, ii) - TR(T_VP + c, jj), 4 + c);
+        da[c] = seeded<10>(TR(T_S + SA + c, ii) - TR(T_S + SA + c, jj), 7 + c);
+      }
+      D r[6], vv[9], aa[9];
+      for (int q = 0; q < 6; q++) r[q] = D(0.0);
+      for (int q = 0; q < 9; q++) vv[q] = aa[q] = D(0.0);
+      f_cd_pair<K, DIM>(a.P.norm, xij, hi, D(a.m[jj]), dv, da, r, vv, aa);
+      double g[10] = {};
+      for (int d = 0; d < 10; d++) {
+        double s = 0.0;
+        for (int q = 0; q < 6; q++) s += W(M_CD + q, ii) * r[q].d[d];
+        for (int q = 0; q < 9; q++) s += W(M_CD + 6 + q, ii) * vv[q].d[d] + W(M_CD + 15 + q, ii) * aa[q].d[d];
+        g[d] = s;
+      }
+      for (int c = 0; c < 3; c++) {
+        gx[c] += sgn * g[c];
+        gv[c] += sgn * g[4 + c];
+        ga[c] += sgn * g[7 + c];
+      }
+      if (!side) gh += g[3];
+    }
+  });
+  if (k >= n) return;
+  for (int c = 0; c < 3; c++) {
+    W(L_X + c, k) += gx[c];
+    W(L_VP + c, k) += gv[c];
+    LS(SA + c, k) += ga[c];
+  }
+  W(L_HN, k) += gh;
+}
+
+// EOS and magnetic-state reconstruction reversed.
+template <int DIM>
+__global__ void __launch_bounds__(256) k_r_prologue(Args a) {
+  using D = Dual<5>;  // h, epred, bpred 3
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n) return;
+  const D h = seeded<5>(TR(T_HN, i), 0), ep = seeded<5>(TR(T_EP, i), 1);
+  const D bp[3] = {seeded<5>(TR(T_BP, i), 2), seeded<5>(TR(T_BP + 1, i), 3), seeded<5>(TR(T_BP + 2, i), 4)};
+  D rho, p, cs, b[3];
+  f_prologue<DIM>(a.P, h, D(a.m[i]), ep, bp, rho, p, cs, b);
+  double g[5];
+  for (int d = 0; d < 5; d++)
+    g[d] = W(L_RHO, i) * rho.d[d] + W(L_P, i) * p.d[d] + W(L_CS, i) * cs.d[d] + W(L_B, i) * b[0].d[d] +
+           W(L_B + 1, i) * b[1].d[d] + W(L_B + 2, i) * b[2].d[d];
+  W(L_HN, i) += g[0];
+  W(L_EP, i) += g[1];
+  for (int c = 0; c < 3; c++) W(L_BP + c, i) += g[2 + c];
+}
+
+// Density post reversed: lambda(h before the pass) and mu_D.
+template <int DIM>
+__global__ void __launch_bounds__(256) k_r_density_post(Args a) {
+  using D = Dual<3>;  // h, rho_sum, dwdh
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n) return;
+  const D h = seeded<3>(TR(T_HP, i), 0), rho = seeded<3>(TR(T_RS, i), 1), dw = seeded<3>(TR(T_DW, i), 2);
+  D om, hn;
+  f_density_post<DIM>(a.P.hfact, h, D(a.m[i]), rho, dw, om, hn);
+  double g[3];
+  for (int d = 0; d < 3; d++) g[d] = W(L_OM, i) * om.d[d] + W(L_HN, i) * hn.d[d];
+  W(L_HP, i) += g[0];
+  W(M_D, i) = g[1];
+  W(M_D + 1, i) = g[2];
+}
+
+// Density pair terms reversed (gather form).
+template <int K, int DIM>
+__global__ void __launch_bounds__(kTile) k_r_density_pair(Args a) {
+  using D = Dual<4>;  // x_ij 3, h_i
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = a.n;
+  const double* X = a.tape + (size_t)T_X * n;
+  const double* HP = a.tape + (size_t)T_HP * n;
+  const int kk = k < n ? k : 0;
+  double gx[3] = {}, gh = 0.0;
+  all_pairs<DIM>(n, a.P, k, X, X + n, X + 2 * n, HP, [&](int j, double dx, double dy, double dz) {
+    for (int side = 0; side < 2; side++) {
+      const int ii = side ? j : kk, jj = side ? kk : j;
+      const double sgn = side ? -1.0 : 1.0;
+      const D xij[3] = {seeded<4>(sgn * dx, 0), seeded<4>(sgn * dy, 1), seeded<4>(sgn * dz, 2)};
+      const D hi = seeded<4>(HP[ii], side ? -1 : 3);
+      D rho(0.0), dw(0.0);
+      f_density_pair<K, DIM>(a.P.norm, xij, hi, D(a.m[jj]), rho, dw);
+      for (int c = 0; c < 3; c++) gx[c] += sgn * (W(M_D, ii) * rho.d[c] + W(M_D + 1, ii) * dw.d[c]);
+      if (!side) gh += W(M_D, ii) * rho.d[3] + W(M_D + 1, ii) * dw.d[3];
+    }
+  });
+  if (k >= n) return;
+  for (int c = 0; c < 3; c++) W(L_X + c, k) += gx[c];
+  W(L_HP, k) += gh;
+}
+
+// initialize + stage1 + wrap reversed: lambda(S_n).
+__global__ void __launch_bounds__(64) k_r_predict(Args a) {
+  using D = Dual<NS>;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n) return;
+  const StepState<D> s = state_at<D>(a.tape + (size_t)T_S * a.n, a.n, i, 0);
+  Predicted<D> o;
+  f_predict(a.P, s, a.itype[i] == 1, a.dt, o);
+  for (int d = 0; d < NS; d++) {
+    double g = 0.0;
+    for (int c = 0; c < 3; c++)
+      g += W(L_X + c, i) * o.x[c].d[d] + W(L_VH + c, i) * o.vhalf[c].d[d] + W(L_VP + c, i) * o.vpred[c].d[d] +
+           W(L_BH + c, i) * o.bhalf[c].d[d] + W(L_BP + c, i) * o.bpred[c].d[d];
+    g += W(L_EH, i) * o.ehalf.d[d] + W(L_EP, i) * o.epred.d[d] + W(L_HP, i) * o.h.d[d] + W(L_A1, i) * o.alpha1.d[d] +
+         W(L_PSIH, i) * o.psihalf.d[d] + W(L_PSIP, i) * o.psipred.d[d];
+    LS(d, i) += g;
+  }
+}
+
+// Gather S_0 from a state's fields into the checkpoint layout.
+__global__ void __launch_bounds__(256) k_pack_state(int n, MhdState s, double* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double* f[NS] = {s.x,      s.y,      s.z,      s.u,    s.v,  s.w,  s.e,  s.h,
+                         s.alpha1, s.Bevolx, s.Bevoly, s.Bevolz, s.psi, s.au, s.av, s.aw,
+                         s.ae,     s.ah,     s.alphaloc, s.cs, s.aBevolx, s.aBevoly, s.aBevolz, s.apsi};
+  for (int k = 0; k < NS; k++) out[(size_t)k * n + i] = f[k][i];
+}
+
+#undef TP
+#undef TR
+#undef SI
+#undef SO
+#undef LN
+#undef LS
+#undef W
+
+template <int K, int DIM>
+static void forward_step(const Args& a, cudaStream_t st) {
+  const int nb = (a.n + kTile - 1) / kTile, np = (a.n + 255) / 256;
+  k_f_predict<<<np, 256, 0, st>>>(a);
+  k_f_density<K, DIM><<<nb, kTile, 0, st>>>(a);
+  k_f_prologue<DIM><<<np, 256, 0, st>>>(a);
+  k_f_cd<K, DIM><<<nb, kTile, 0, st>>>(a);
+  k_f_force<K, DIM><<<nb, kTile, 0, st>>>(a);
+}
+
+template <int K, int DIM>
+static void reverse_step(const Args& a, cudaStream_t st) {
+  const int nb = (a.n + kTile - 1) / kTile, np = (a.n + 255) / 256, n64 = (a.n + 63) / 64;
+  k_r_correct<<<np, 256, 0, st>>>(a);
+  k_r_force_post<DIM><<<n64, 64, 0, st>>>(a);
+  k_r_force_pair<K, DIM><<<nb, kTile, 0, st>>>(a);
+  k_r_cd_post<<<n64, 64, 0, st>>>(a);
+  k_r_cd_pair<K, DIM><<<nb, kTile, 0, st>>>(a);
+  k_r_prologue<DIM><<<np, 256, 0, st>>>(a);
+  k_r_density_post<DIM><<<np, 256, 0, st>>>(a);
+  k_r_density_pair<K, DIM><<<nb, kTile, 0, st>>>(a);
+  k_r_predict<<<n64, 64, 0, st>>>(a);
+}
+
+#define MHD_A_DISPATCH(FN, ...)                                                                   \
+  do {                                                                                            \
+    const int d3 = c->P.dim == 3;                                                                 \
+    switch (c->P.kernel) {                                                                        \
+      case MHD_KERNEL_CUBIC: d3 ? FN<0, 3>(__VA_ARGS__) : FN<0, 2>(__VA_ARGS__); break;           \
+      case MHD_KERNEL_QUINTIC: d3 ? FN<1, 3>(__VA_ARGS__) : FN<1, 2>(__VA_ARGS__); break;         \
+      case MHD_KERNEL_WENDLAND_C2: d3 ? FN<2, 3>(__VA_ARGS__) : FN<2, 2>(__VA_ARGS__); break;     \
+      case MHD_KERNEL_WENDLAND_C4: d3 ? FN<3, 3>(__VA_ARGS__) : FN<3, 2>(__VA_ARGS__); break;     \
+      case MHD_KERNEL_WENDLAND_C6: d3 ? FN<4, 3>(__VA_ARGS__) : FN<4, 2>(__VA_ARGS__); break;     \
+      case MHD_KERNEL_GAUSSIAN: d3 ? FN<5, 3>(__VA_ARGS__) : FN<5, 2>(__VA_ARGS__); break;        \
+      default: d3 ? FN<6, 3>(__VA_ARGS__) : FN<6, 2>(__VA_ARGS__); break;                         \
+    }                                                                                             \
+  } while (0)
+
+}  // namespace adj
+}  // namespace mhd
+
+using namespace mhd;
+using namespace mhd::adj;
+
+namespace {
+
+#define A_FAIL(code, msg) \
+  do {                    \
+    c->err = (msg);       \
+    return (code);        \
+  } while (0)
+#define A_CK(call)                                                 \
+  do {                                                             \
+    cudaError_t e_ = (call);                                       \
+    if (e_ != cudaSuccess) {                                       \
+      c->err = std::string(#call) + ": " + cudaGetErrorString(e_); \
+      return MHD_ERR_CUDA;                                         \
+    }                                                              \
+  } while (0)
+
+const char* const kAdjointFields[NS] = {"x",  "y",  "z",  "u",  "v",  "w",        "e",   "h",
+                                        "alpha1", "Bevolx", "Bevoly", "Bevolz", "psi", "au", "av", "aw",
+                                        "ae", "ah", "alphaloc", "cs", "aBevolx", "aBevoly", "aBevolz", "apsi"};
+
+// Workspace of the adjoint: two states, `every` tapes, the reverse
+// workspace, two lambdas, the per-particle alpha_max derivative, partials.
+struct AdjLayout {
+  size_t state[2], tape, w, lam[2], g_amax, dta, part, total;
+};
+
+AdjLayout layout(int64_t n, int every) {
+  AdjLayout L;
+  size_t off = 0;
+  auto take = [&](size_t cnt) {
+    const size_t o = off;
+    off += (cnt + 31) & ~(size_t)31;
+    return o;
+  };
+  L.state[0] = take(NS * n);
+  L.state[1] = take(NS * n);
+  L.tape = take((size_t)every * NT * n);
+  L.w = take(NL * n);
+  L.lam[0] = take(NS * n);
+  L.lam[1] = take(NS * n);
+  L.g_amax = take(n);
+  L.dta = take(n);
+  L.part = take(n / 256 + 64);
+  L.total = off;
+  return L;
+}
+
+int check_adjoint(Ctx* c, const MhdState* s, int64_t n, int steps, const double* dts, int every, bool adaptive) {
+  if (!s || !s->m || !s->itype) A_FAIL(MHD_ERR_INVALID, "state, m or itype is null");
+  if (n < 1 || n > c->n_max || n > MHD_TANGENT_MAX_N)
+    A_FAIL(MHD_ERR_INVALID, "n must be in [1, min(n_max, MHD_TANGENT_MAX_N)]");
+  if (c->P.iterate) A_FAIL(MHD_ERR_INVALID, "the adjoint needs the single density pass (iterate = 0)");
+  if (steps < 1 || !dts) A_FAIL(MHD_ERR_INVALID, "steps must be >= 1 and dts non-null");
+  if (every < 1 || every > 256) A_FAIL(MHD_ERR_INVALID, "every must be in [1, 256]");
+  for (int k = 0; k < steps; k++) {
+    if (adaptive && k > 0 && dts[k] < 0.0) continue;
+    if (!(dts[k] >= 0.0) || !isfinite(dts[k])) A_FAIL(MHD_ERR_INVALID, "step sizes must be finite and >= 0");
+  }
+  const AdjLayout L = layout(n, every);
+  if (c->adj_size < L.total) {
+    cudaFree(c->adj_buf);
+    c->adj_buf = nullptr;
+    c->adj_size = 0;
+    A_CK(cudaMalloc(&c->adj_buf, sizeof(double) * L.total));
+    c->adj_size = L.total;
+  }
+  return MHD_OK;
+}
+
+Args base_args(Ctx* c, const MhdState* s, int64_t n, double amax) {
+  Args a;
+  memset(&a, 0, sizeof a);
+  a.n = (int)n;
+  a.P = c->P;
+  a.amax = amax;
+  a.m = s->m;
+  a.itype = s->itype;
+  return a;
+}
+
+// Run steps [k0, k1) from `s0` with tapes (tape slot t - k0); returns the
+// state buffer holding S_{k1}.  A negative dts[t + 1] is replaced by the
+// adaptive rule (min dt_adapt, clipped so that time + dt <= tf).
+double* run_segment(Ctx* c, Args a, const AdjLayout& L, const double* s0, int k0, int k1, double* dts, int steps,
+                    double& time, cudaStream_t st) {
+  double* buf = (double*)c->adj_buf;
+  const double* cur = s0;
+  int which = 0;
+  for (int t = k0; t < k1; t++) {
+    a.s_in = cur;
+    a.s_out = buf + L.state[which];
+    a.tape_w = buf + L.tape + (size_t)(t - k0) * NT * a.n;
+    a.dt = dts[t];
+    a.dta_out = buf + L.dta;
+    MHD_A_DISPATCH(forward_step, a, st);
+    c->launches += 5;
+    time += dts[t];
+    if (t + 1 < steps && dts[t + 1] < 0.0) {
+      k_min<<<1, 256, 0, st>>>(a.n, buf + L.dta, buf + L.part);
+      c->launches++;
+      double dmin = 0.0;
+      if (cudaMemcpyAsync(&dmin, buf + L.part, sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+          cudaStreamSynchronize(st) != cudaSuccess)
+        return nullptr;
+      dts[t + 1] = time + dmin > c->P.tf ? c->P.tf - time : dmin;
+    }
+    cur = a.s_out;
+    which ^= 1;
+  }
+  return const_cast<double*>(cur);
+}
+
+}  // namespace
+
+extern "C" {
+
+int mhd_adjoint_field_count(void) { return NS; }
+const char* mhd_adjoint_field_name(int32_t k) { return (k >= 0 && k < NS) ? kAdjointFields[k] : nullptr; }
+
+int mhd_adjoint_forward(void* ctx, const MhdState* s, int64_t n, int32_t steps, double* dts, int32_t every,
+                        double* checkpoints, double* loss, void* stream) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return MHD_ERR_INVALID;
+  int rc = check_adjoint(c, s, n, steps, dts, every, true);
+  if (rc != MHD_OK) return rc;
+  if (!checkpoints || !loss) A_FAIL(MHD_ERR_INVALID, "checkpoints and loss must be non-null");
+  const cudaStream_t st = (cudaStream_t)stream;
+  const AdjLayout L = layout(n, every);
+  double* buf = (double*)c->adj_buf;
+  const int np = (int)((n + 255) / 256);
+  k_pack_state<<<np, 256, 0, st>>>((int)n, *s, checkpoints);
+  c->launches++;
+  Args a = base_args(c, s, n, c->P.alpha_max);
+  const double* cur = checkpoints;
+  const int nseg = (steps + every - 1) / every;
+  double time = 0.0;
+  for (int g = 0; g < nseg; g++) {
+    const int k0 = g * every, k1 = k0 + every < steps ? k0 + every : steps;
+    double* end = run_segment(c, a, L, cur, k0, k1, dts, steps, time, st);
+    if (!end) A_FAIL(MHD_ERR_CUDA, "adaptive step size read-back failed");
+    double* next_cp = checkpoints + (size_t)(g + 1) * NS * n;
+    A_CK(cudaMemcpyAsync(next_cp, end, sizeof(double) * NS * n, cudaMemcpyDeviceToDevice, st));
+    cur = next_cp;
+    if (g == nseg - 1) {
+      const double* last_tape = buf + L.tape + (size_t)(k1 - 1 - k0) * NT * n;
+      k_f_energy<<<np, 256, 0, st>>>((int)n, c->P.mu0, s->m, cur, last_tape, buf + L.part);
+      k_sum_blocks<<<1, 32, 0, st>>>(np, buf + L.part, buf + L.part + np);
+      c->launches += 2;
+    }
+  }
+  A_CK(cudaGetLastError());
+  A_CK(cudaMemcpyAsync(loss, buf + L.part + np, sizeof(double), cudaMemcpyDeviceToHost, st));
+  A_CK(cudaStreamSynchronize(st));
+  return MHD_OK;
+}
+
+int mhd_adjoint_backward(void* ctx, const MhdState* s, int64_t n, int32_t steps, const double* dts, int32_t every,
+                         const double* checkpoints, double* lambda0, double* dloss_dalpha_max, void* stream) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return MHD_ERR_INVALID;
+  int rc = check_adjoint(c, s, n, steps, dts, every, false);
+  if (rc != MHD_OK) return rc;
+  if (!checkpoints || !lambda0 || !dloss_dalpha_max) A_FAIL(MHD_ERR_INVALID, "output pointers must be non-null");
+  double* dts_w = const_cast<double*>(dts);  // all >= 0: run_segment only reads them
+  const cudaStream_t st = (cudaStream_t)stream;
+  const AdjLayout L = layout(n, every);
+  double* buf = (double*)c->adj_buf;
+  const int np = (int)((n + 255) / 256);
+  A_CK(cudaMemsetAsync(buf + L.g_amax, 0, sizeof(double) * n, st));
+  Args a = base_args(c, s, n, c->P.alpha_max);
+  a.w = buf + L.w;
+  a.g_amax = buf + L.g_amax;
+  double* lam_next = buf + L.lam[0];
+  double* lam = buf + L.lam[1];
+  const int nseg = (steps + every - 1) / every;
+  for (int g = nseg - 1; g >= 0; g--) {
+    const int k0 = g * every, k1 = k0 + every < steps ? k0 + every : steps;
+    double time = 0.0;
+    const double* s_end = run_segment(c, a, L, checkpoints + (size_t)g * NS * n, k0, k1, dts_w, steps, time, st);
+    for (int t = k1 - 1; t >= k0; t--) {
+      Args r = a;
+      r.tape = buf + L.tape + (size_t)(t - k0) * NT * n;
+      r.dt = dts[t];
+      r.lam_next = lam_next;
+      r.lam = lam;
+      r.s_final = t == steps - 1 ? s_end : nullptr;
+      if (t == steps - 1) {
+        k_r_seed<<<np, 256, 0, st>>>(r);
+        c->launches++;
+      }
+      MHD_A_DISPATCH(reverse_step, r, st);
+      c->launches += 9;
+      double* tmp = lam_next;
+      lam_next = lam;
+      lam = tmp;
+    }
+  }
+  A_CK(cudaGetLastError());
+  A_CK(cudaMemcpyAsync(lambda0, lam_next, sizeof(double) * NS * n, cudaMemcpyDeviceToDevice, st));
+  k_sum_blocks<<<1, 32, 0, st>>>((int)n, buf + L.g_amax, buf + L.part);
+  c->launches++;
+  A_CK(cudaMemcpyAsync(dloss_dalpha_max, buf + L.part, sizeof(double), cudaMemcpyDeviceToHost, st));
+  A_CK(cudaStreamSynchronize(st));
+  return MHD_OK;
+}
+
+}  // extern "C"

@@ -130,4 +130,17 @@ __host__ __device__ inline Dual<N> pow(const Dual<N>& a, double e) {
   return r;
 }
 
+// Scalar-generic spellings: one name for double and for Dual<N>, for code
+// written over either (the global math functions cannot be overloaded in
+// this namespace without ambiguity).
+__host__ __device__ inline double gsqrt(double a) { return ::sqrt(a); }
+__host__ __device__ inline double gfabs(double a) { return ::fabs(a); }
+__host__ __device__ inline double gpow(double a, double e) { return ::pow(a, e); }
+template <int N>
+__host__ __device__ inline Dual<N> gsqrt(const Dual<N>& a) { return sqrt(a); }
+template <int N>
+__host__ __device__ inline Dual<N> gfabs(const Dual<N>& a) { return fabs(a); }
+template <int N>
+__host__ __device__ inline Dual<N> gpow(const Dual<N>& a, double e) { return pow(a, e); }
+
 }  // namespace mhd

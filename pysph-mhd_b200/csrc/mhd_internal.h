@@ -50,6 +50,8 @@ struct Ctx {
   int graph_passes = 8;           // density passes captured per right-hand side
   cudaStream_t cap_stream = nullptr;
   void* tan_work = nullptr;  // derivative form: new h / energy partials (dual records)
+  void* adj_buf = nullptr;   // adjoint: states, tapes, reverse workspace (doubles)
+  size_t adj_size = 0;
   struct GraphEntry {
     MhdState a, b;
     int64_t n;

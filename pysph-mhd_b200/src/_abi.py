@@ -86,6 +86,7 @@ EXPORTS = (
     "mhd_pair_counts", "mhd_timestep_noalloc", "mhd_neighbour_counts", "mhd_ctx_set_instances",
     "mhd_instance_count", "mhd_clock_set_all", "mhd_clock_get_all", "mhd_advance", "mhd_ctx_tune",
     "mhd_tangent_dirs", "mhd_tangent_sync", "mhd_tangent_rhs", "mhd_tangent_step", "mhd_tangent_magnetic_energy",
+    "mhd_adjoint_field_count", "mhd_adjoint_field_name", "mhd_adjoint_forward", "mhd_adjoint_backward",
 )
 NOALLOC_MAX_N = 67108864
 TIMING_KINDS = ("cells", "density", "prologue", "force", "dt", "integrate", "lists")
@@ -147,6 +148,10 @@ def load(path: str = LIB_PATH):
     lib.mhd_tangent_rhs.argtypes = [vp, sp, i64, dp, vp]
     lib.mhd_tangent_step.argtypes = [vp, sp, i64, dbl, dp, vp]
     lib.mhd_tangent_magnetic_energy.argtypes = [vp, sp, i64, dp, vp]
+    lib.mhd_adjoint_field_name.restype = ctypes.c_char_p
+    lib.mhd_adjoint_field_name.argtypes = [i32]
+    lib.mhd_adjoint_forward.argtypes = [vp, sp, i64, i32, dp, i32, vp, dp, vp]
+    lib.mhd_adjoint_backward.argtypes = [vp, sp, i64, i32, dp, i32, vp, vp, dp, vp]
     _lib = lib
     return lib
 

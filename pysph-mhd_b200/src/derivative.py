@@ -13,9 +13,16 @@ through the initial state (a seed direction per property) or through
 step must be the single pass (``density = "single"``), which keeps the map
 smooth.
 
+Reverse mode (adjoint) over the step loop: ``AdjointEngine`` runs the steps
+keeping the state every ``every`` steps and then the adjoint sweep
+(``mhd_adjoint_*``), re-running each segment from its checkpoint.  The
+warm-up before the first step is differentiated in forward mode and joined
+to the adjoint at the first step's state.
+
 ``MagneticEnergy`` wraps a whole run as a ``torch.autograd.Function`` of
 (amplitude, alpha_max) for the circularly polarised Alfven wave: the final
-magnetic energy sum m |B|^2 / (2 mu0 rho) after ``steps`` steps.
+magnetic energy sum m |B|^2 / (2 mu0 rho) after ``steps`` steps, gradient by
+the checkpointed adjoint.
 """
 
 from __future__ import annotations
@@ -217,19 +224,135 @@ def magnetic_energy_and_gradient(config, amplitude: float, alpha_max: float, ste
         eng.close()
 
 
+class AdjointEngine:
+    """Reverse mode over the step loop (``mhd_adjoint_*``): the forward sweep
+    keeps the step state every ``every`` steps, the backward sweep re-runs
+    each segment from its checkpoint with a tape and returns dL/dS_0 and
+    dL/dalpha_max for L = sum m |B|^2 / (2 mu0 rho) after the last step."""
+
+    def __init__(self, params: _abi.MhdParams, n: int):
+        if params.iterate:
+            raise ValueError('the adjoint needs density = "single" (params.iterate = 0)')
+        self.lib = _abi.load()
+        self.params = params
+        self.n = n
+        self.ctx = ctypes.c_void_p()
+        _abi.check(self.lib.mhd_ctx_create(ctypes.byref(params), n, ctypes.byref(self.ctx)), None)
+        self.fields = [self.lib.mhd_adjoint_field_name(k).decode() for k in range(self.lib.mhd_adjoint_field_count())]
+
+    def close(self):
+        if self.ctx:
+            self.lib.mhd_ctx_destroy(self.ctx)
+            self.ctx = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream(self):
+        return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    def _state(self, values: dict):
+        S = _abi.state_type()
+        s = S()
+        for f, t in values.items():
+            setattr(s, f, ctypes.c_void_p(t.data_ptr()))
+        return s
+
+    def forward(self, values: dict, steps: int, dts, every: int):
+        """values: contiguous device tensors of the step-state fields, m and
+        itype.  dts: step sizes, None or negative entries for the adaptive
+        rule.  Returns (loss, step sizes used, checkpoints)."""
+        s = self._state(values)
+        d = [-1.0] * steps if dts is None else [float(x) for x in dts]
+        if d[0] < 0:
+            raise ValueError("the first step size must be given")
+        arr = (ctypes.c_double * steps)(*d)
+        nseg = (steps + every - 1) // every
+        cps = torch.empty((nseg + 1, len(self.fields), self.n), dtype=torch.float64, device=values["x"].device)
+        loss = ctypes.c_double()
+        _abi.check(self.lib.mhd_adjoint_forward(self.ctx, ctypes.byref(s), self.n, steps, arr, every,
+                                                ctypes.c_void_p(cps.data_ptr()), ctypes.byref(loss), self.stream),
+                   self.ctx)
+        return loss.value, list(arr), cps
+
+    def backward(self, values: dict, steps: int, dts, every: int, checkpoints):
+        s = self._state(values)
+        arr = (ctypes.c_double * steps)(*[float(x) for x in dts])
+        lam = torch.empty((len(self.fields), self.n), dtype=torch.float64, device=values["x"].device)
+        dam = ctypes.c_double()
+        _abi.check(self.lib.mhd_adjoint_backward(self.ctx, ctypes.byref(s), self.n, steps, arr, every,
+                                                 ctypes.c_void_p(checkpoints.data_ptr()),
+                                                 ctypes.c_void_p(lam.data_ptr()), ctypes.byref(dam), self.stream),
+                   self.ctx)
+        return lam, dam.value
+
+
+def _warm_start(config, amplitude, alpha_max):
+    """Warm-up in forward mode: the state at the first step (values) and its
+    derivatives with respect to (amplitude, alpha_max)."""
+    from .engine import params_from_dict
+
+    ic, seed, prm = alfven_case(config, amplitude, alpha_max)
+    params = params_from_dict(prm)
+    te = TangentEngine(params, TangentState(ic, seed), alpha_max_seed=[0.0, 1.0])
+    te.warmup()
+    dt0 = te.initial_dt()
+    return params, te, dt0
+
+
+def magnetic_energy_adjoint(config, amplitude: float, alpha_max: float, steps: int, every: int = 16, dts=None):
+    """The same loss and gradient as ``magnetic_energy_and_gradient``, by the
+    checkpointed adjoint over the steps (the warm-up in forward mode)."""
+    params, te, dt0 = _warm_start(config, amplitude, alpha_max)
+    ae = AdjointEngine(params, te.ts.n)
+    try:
+        values = {f: te.ts[f][:, 0].contiguous() for f in ae.fields}
+        values["m"] = te.ts["m"][:, 0].contiguous()
+        values["itype"] = te.ts["itype"]
+        loss, used, cps = ae.forward(values, steps, [dt0] + [-1.0] * (steps - 1) if dts is None else dts, every)
+        lam, dam = ae.backward(values, steps, used, every, cps)
+        tan = torch.stack([te.ts[f][:, 1:] for f in ae.fields])  # fields x n x DIRS
+        grad = torch.einsum("fn,fnd->d", lam, tan).cpu().numpy()
+        grad[1] += dam
+        return loss, grad, used
+    finally:
+        ae.close()
+        te.close()
+
+
 class MagneticEnergy(torch.autograd.Function):
     """Final magnetic energy of the 2-D Alfven wave as a differentiable
     function of (amplitude, alpha_max): ``MagneticEnergy.apply(a, am, config,
-    steps)``.  The forward pass runs the dual-number simulation once and
-    keeps the gradient; backward scales it by the incoming gradient."""
+    steps, every)``.  Forward: the warm-up in forward mode, then the steps
+    with the state kept every ``every`` steps.  Backward: the adjoint sweep,
+    re-running each segment from its checkpoint, contracted with the
+    warm-up's derivatives."""
 
     @staticmethod
-    def forward(ctx, amplitude, alpha_max, config, steps):
-        value, grad, _ = magnetic_energy_and_gradient(config, float(amplitude), float(alpha_max), int(steps))
-        ctx.save_for_backward(torch.as_tensor(grad, dtype=torch.float64))
-        return torch.as_tensor(value, dtype=torch.float64)
+    def forward(ctx, amplitude, alpha_max, config, steps, every=16):
+        params, te, dt0 = _warm_start(config, float(amplitude), float(alpha_max))
+        ae = AdjointEngine(params, te.ts.n)
+        values = {f: te.ts[f][:, 0].contiguous() for f in ae.fields}
+        values["m"] = te.ts["m"][:, 0].contiguous()
+        values["itype"] = te.ts["itype"]
+        loss, used, cps = ae.forward(values, int(steps), [dt0] + [-1.0] * (int(steps) - 1), int(every))
+        ctx.engines = (te, ae)
+        ctx.values, ctx.used, ctx.cps, ctx.steps, ctx.every = values, used, cps, int(steps), int(every)
+        return torch.as_tensor(loss, dtype=torch.float64)
 
     @staticmethod
     def backward(ctx, g):
-        (grad,) = ctx.saved_tensors
-        return g * grad[0], g * grad[1], None, None
+        te, ae = ctx.engines
+        try:
+            lam, dam = ae.backward(ctx.values, ctx.steps, ctx.used, ctx.every, ctx.cps)
+            tan = torch.stack([te.ts[f][:, 1:] for f in ae.fields])
+            grad = torch.einsum("fn,fnd->d", lam, tan).cpu()
+            grad[1] += dam
+        finally:
+            ae.close()
+            te.close()
+        return g * grad[0], g * grad[1], None, None, None
