@@ -35,9 +35,15 @@ def build(force=False, verbose=False):
         if os.path.getmtime(OUT) >= newest:
             return OUT
     os.makedirs(OBJ, exist_ok=True)
+    headers = [p for p in _deps() if not p.endswith(".cu")]
+    newest_header = max(os.path.getmtime(p) for p in headers)
 
     def compile_one(src):
         obj = os.path.join(OBJ, src.replace(".cu", ".o"))
+        if not force and not verbose and os.path.exists(obj):
+            # an object is current when newer than its source and every header
+            if os.path.getmtime(obj) >= max(newest_header, os.path.getmtime(os.path.join(CSRC, src))):
+                return obj, ""
         cmd = [NVCC, *FLAGS, *FILE_FLAGS.get(src, []), "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             cmd += ["-Xptxas", "-v"]

@@ -470,4 +470,77 @@ __device__ __forceinline__ void for_each_cell_trimmed(const Grid& G, int sw, con
   }
 }
 
+// The cells for_each_cell_trimmed visits, a stencil row at a time: calls
+// f(yu, zu, jb, je, xoff) for every contiguous piece of a row's trimmed
+// x-range, [jb, je) the particles of the piece in sorted order and xoff the
+// offset that turns a particle's own cell x into its unwrapped coordinate
+// (-nx, 0 or +nx; 0 on an axis scanned whole).  Pieces come in ascending
+// unwrapped x, so a caller sees the particles in the order of
+// for_each_cell_trimmed.
+template <int DIM, class F>
+__device__ __forceinline__ void for_each_row_trimmed(const Grid& G, int sw, const int* __restrict__ cell_start,
+                                                     double xi, double yi, double zi, double cut, F&& f) {
+  const int whole = 2 * sw + 1;
+  const int nx = G.nc[0], ny = G.nc[1], nz = G.nc[2];
+  const int cy = cell_coord(G, 1, yi);
+  const int cz = DIM == 3 ? cell_coord(G, 2, zi) : 0;
+  int xl, xh;
+  if (nx < whole) {
+    xl = 0;
+    xh = nx - 1;
+  } else {
+    xl = (int)floor((xi - cut - G.lo[0]) * G.inv_cs[0]);
+    xh = (int)floor((xi + cut - G.lo[0]) * G.inv_cs[0]);
+    if (!G.periodic[0]) {
+      xl = xl < 0 ? 0 : xl;
+      xh = xh >= nx ? nx - 1 : xh;
+    }
+    if (xh - xl >= nx) xh = xl + nx - 1;  // never visit a cell twice
+  }
+  const double cut2 = cut * cut;
+  const bool zs = DIM == 3 && nz >= whole, ys = ny >= whole;
+  const int zlo = DIM == 3 ? (zs ? cz - sw : 0) : 0, zhi = DIM == 3 ? (zs ? cz + sw : nz - 1) : 0;
+  const int ylo = ys ? cy - sw : 0, yhi = ys ? cy + sw : ny - 1;
+  for (int zu = zlo; zu <= zhi; zu++) {
+    int zc = zu;
+    double dzm = 0.0;
+    if (zs) {
+      const double c_lo = G.lo[2] + zu * G.cs[2], c_hi = c_lo + G.cs[2];
+      dzm = zi < c_lo ? c_lo - zi : (zi > c_hi ? zi - c_hi : 0.0);
+      if (dzm * dzm >= cut2) continue;
+      if (zc < 0 || zc >= nz) {
+        if (!G.periodic[2]) continue;
+        zc = zc < 0 ? zc + nz : zc - nz;
+      }
+    }
+    for (int yu = ylo; yu <= yhi; yu++) {
+      int yc = yu;
+      if (ys) {
+        const double c_lo = G.lo[1] + yu * G.cs[1], c_hi = c_lo + G.cs[1];
+        const double dym = yi < c_lo ? c_lo - yi : (yi > c_hi ? yi - c_hi : 0.0);
+        if (dym * dym + dzm * dzm >= cut2) continue;
+        if (yc < 0 || yc >= ny) {
+          if (!G.periodic[1]) continue;
+          yc = yc < 0 ? yc + ny : yc - ny;
+        }
+      }
+      const int base = G.cell_base + (zc * ny + yc) * nx;
+      // [xl, xh] in unwrapped cells: at most three pieces (below 0, inside,
+      // above nx - 1)
+      if (xl < 0) {
+        const int a = xl + nx, b = (xh < 0 ? xh : -1) + nx;
+        f(yu, zu, cell_start[base + a], cell_start[base + b + 1], -nx);
+      }
+      if (xh >= 0 && xl < nx) {
+        const int a = xl < 0 ? 0 : xl, b = xh >= nx ? nx - 1 : xh;
+        f(yu, zu, cell_start[base + a], cell_start[base + b + 1], 0);
+      }
+      if (xh >= nx) {
+        const int a = (xl >= nx ? xl : nx) - nx, b = xh - nx;
+        f(yu, zu, cell_start[base + a], cell_start[base + b + 1], nx);
+      }
+    }
+  }
+}
+
 }  // namespace mhd

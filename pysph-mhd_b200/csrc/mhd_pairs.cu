@@ -227,7 +227,11 @@ __global__ void __launch_bounds__(128) k_build_lists(int n, DevParams P, const G
   int sw;
   double cut;
   search_extent(G, DIM, Rg, pi.w, big_i, sw, cut);
-  if (big_i) big_idx[atomicAdd(&sc->n_big, 1)] = i;
+  if (big_i) {
+    // its extended search runs in k_build_lists_big, one warp per particle
+    big_idx[atomicAdd(&sc->n_big, 1)] = i;
+    return;
+  }
   const float own2 = reach2(Rg, pi.w, slack);
   int* __restrict__ row = idx + (size_t)(i >> 5) * cap * 32 + (i & 31);
   int cnt = 0;
@@ -238,13 +242,17 @@ __global__ void __launch_bounds__(128) k_build_lists(int n, DevParams P, const G
              mz = DIM == 3 && G.periodic[2] && G.nc[2] < whole;
   const float Lx = (float)G.L[0], Ly = (float)G.L[1], Lz = (float)G.L[2];
   const float csx = G.csf[0], csy = G.csf[1], csz = G.csf[2];
-  for_each_cell_trimmed<DIM>(G, sw, cell_start, x[i], y[i], DIM == 3 ? z[i] : 0.0, cut,
-                             [&](int cxu, int cyu, int czu, int jb, int je) {
-    const float sx = pi.x + (float)(cxi - cxu) * csx;
+  // One contiguous index range per stencil row piece: the x shift of a
+  // candidate follows from its packed cell x and the piece's image offset.
+  constexpr int xmask = DIM == 3 ? 2047 : 65535;
+  for_each_row_trimmed<DIM>(G, sw, cell_start, x[i], y[i], DIM == 3 ? z[i] : 0.0, cut,
+                            [&](int cyu, int czu, int jb, int je, int xoff) {
     const float sy = pi.y + (float)(cyi - cyu) * csy;
     const float sz = DIM == 3 ? pi.z + (float)(czi - czu) * csz : 0.f;
+    const int cxo = cxi - xoff;
     for (int j = jb; j < je; j++) {
       const float4 pj = __ldg(posf + j);
+      const float sx = pi.x + (float)(cxo - (__ldg(cellc + j) & xmask)) * csx;
       bool keep;
       if (pj.w > hbig) {
         // big j: kept here only by a big i, within i's own reach (the
@@ -288,10 +296,12 @@ __global__ void __launch_bounds__(128) k_scatter_big(DevParams P, const Grid* __
                                                      const int* __restrict__ cellc, float grow, int cap,
                                                      int* __restrict__ idx, int* __restrict__ cnt,
                                                      const int* __restrict__ big_idx, DevScalars* sc) {
-  const int nb = sc->n_big;
+  // one warp per big particle: the lanes take consecutive candidates
+  const int nb = sc->n_big, lane = threadIdx.x & 31;
   const float Rg = __fmul_rn((float)P.R, grow);
   const float slack = 1.0f + 4e-6f;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nb; t += gridDim.x * blockDim.x) {
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < nb; t += nwarps) {
     const int j = big_idx[t];
     const Grid& G = grid_of(grids, inst, j);
     const float4 pj = posf[j];
@@ -301,9 +311,9 @@ __global__ void __launch_bounds__(128) k_scatter_big(DevParams P, const Grid* __
     int sw;
     double cut;
     search_extent(G, DIM, Rg, pj.w, true, sw, cut);
-    for_each_cell_trimmed<DIM>(G, sw, cell_start, x[j], y[j], DIM == 3 ? z[j] : 0.0, cut,
-                               [&](int, int, int, int ib, int ie) {
-      for (int i = ib; i < ie; i++) {
+    for_each_row_trimmed<DIM>(G, sw, cell_start, x[j], y[j], DIM == 3 ? z[j] : 0.0, cut,
+                              [&](int, int, int ib, int ie, int) {
+      for (int i = ib + lane; i < ie; i += 32) {
         if (i == j) continue;
         const float4 pi = __ldg(posf + i);
         const float r2 = sym_r2<DIM>(G, pi, __ldg(cellc + i), pj, cj);
@@ -318,6 +328,90 @@ __global__ void __launch_bounds__(128) k_scatter_big(DevParams P, const Grid* __
         }
       }
     });
+  }
+}
+
+// Gather pass of the big particles, one warp per particle: the lanes test
+// consecutive candidates of each row piece and append the kept ones in
+// candidate order (ballot prefix), so the list is what a single thread
+// scanning the extended stencil would write.
+template <int DIM>
+__global__ void __launch_bounds__(128) k_build_lists_big(DevParams P, const Grid* __restrict__ grids,
+                                                         const int* __restrict__ inst,
+                                                         const int* __restrict__ cell_start,
+                                                         const double* __restrict__ x, const double* __restrict__ y,
+                                                         const double* __restrict__ z, const double* __restrict__ h,
+                                                         const float4* __restrict__ posf,
+                                                         const int* __restrict__ cellc, float grow, int cap,
+                                                         int* __restrict__ idx, int* __restrict__ cnt_out,
+                                                         int* __restrict__ gcnt_out, double* __restrict__ hlim,
+                                                         const int* __restrict__ big_idx, DevScalars* sc) {
+  const int nb = sc->n_big, lane = threadIdx.x & 31;
+  const float Rg = __fmul_rn((float)P.R, grow);
+  const float slack = 1.0f + 4e-6f;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  constexpr int xmask = DIM == 3 ? 2047 : 65535;
+  for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < nb; t += nwarps) {
+    const int i = big_idx[t];
+    const Grid& G = grid_of(grids, inst, i);
+    const float4 pi = posf[i];
+    const int ci = cellc[i];
+    const float rhi2 = reach2(Rg, pi.w, 1.0f), own2 = reach2(Rg, pi.w, slack);
+    const float hbig = G.h_bigf;
+    int sw;
+    double cut;
+    search_extent(G, DIM, Rg, pi.w, true, sw, cut);
+    int cxi, cyi, czi;
+    unpack_cell<DIM>(ci, cxi, cyi, czi);
+    const int whole = 2 * sw + 1;
+    const bool mx = G.periodic[0] && G.nc[0] < whole, my = G.periodic[1] && G.nc[1] < whole,
+               mz = DIM == 3 && G.periodic[2] && G.nc[2] < whole;
+    const float Lx = (float)G.L[0], Ly = (float)G.L[1], Lz = (float)G.L[2];
+    const float csx = G.csf[0], csy = G.csf[1], csz = G.csf[2];
+    int* __restrict__ row = idx + (size_t)(i >> 5) * cap * 32 + (i & 31);
+    int cnt = 0;
+    for_each_row_trimmed<DIM>(G, sw, cell_start, x[i], y[i], DIM == 3 ? z[i] : 0.0, cut,
+                              [&](int cyu, int czu, int jb, int je, int xoff) {
+      const float sy = pi.y + (float)(cyi - cyu) * csy;
+      const float sz = DIM == 3 ? pi.z + (float)(czi - czu) * csz : 0.f;
+      const int cxo = cxi - xoff;
+      for (int t0 = jb; t0 < je; t0 += 32) {
+        const int j = t0 + lane;
+        bool keep = false;
+        if (j < je) {
+          const float4 pj = __ldg(posf + j);
+          const int cjj = __ldg(cellc + j);
+          if (pj.w > hbig) {
+            keep = sym_r2<DIM>(G, pi, ci, pj, cjj) < own2;
+          } else {
+            const float sx = pi.x + (float)(cxo - (cjj & xmask)) * csx;
+            float dx = sx - pj.x, dy = sy - pj.y, dz = DIM == 3 ? sz - pj.z : 0.f;
+            if (mx) dx = dx > 0.5f * Lx ? dx - Lx : (dx < -0.5f * Lx ? dx + Lx : dx);
+            if (my) dy = dy > 0.5f * Ly ? dy - Ly : (dy < -0.5f * Ly ? dy + Ly : dy);
+            if (mz) dz = dz > 0.5f * Lz ? dz - Lz : (dz < -0.5f * Lz ? dz + Lz : dz);
+            const float r2 = dx * dx + dy * dy + dz * dz;
+            const float rhj = Rg * pj.w;
+            keep = r2 < fmaxf(rhi2, rhj * rhj) * slack;
+          }
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, keep);
+        if (keep) {
+          const int pos = cnt + __popc(bal & ((1u << lane) - 1u));
+          if (pos < cap) row[pos * 32] = j;
+        }
+        cnt += __popc(bal);
+      }
+    });
+    if (lane == 0) {
+      const int stored = cnt < cap ? cnt : cap;
+      cnt_out[i] = stored;
+      gcnt_out[i] = stored;
+      hlim[i] = h[i] * (double)grow * (1.0 - 1e-4);
+      if (cnt > cap) {
+        atomicMax(&sc->list_max, cnt);
+        atomicExch(&sc->relist, 1);
+      }
+    }
   }
 }
 
@@ -394,6 +488,10 @@ void launch_build_lists(Ctx* c, const MhdState* s, int n, cudaStream_t st) {
     k_build_lists<3><<<nb, 128, 0, st>>>(n, c->P, c->d_grids, c->inst, c->cell_start, s->x, s->y, s->z, s->h,
                                          c->posf, c->cellc, grow, c->list_cap, c->nbr_idx, c->nbr_cnt, c->nbr_gcnt,
                                          c->nbr_hlim, c->big_idx, c->d_sc);
+    k_build_lists_big<3><<<kScatterBlocks, 128, 0, st>>>(c->P, c->d_grids, c->inst, c->cell_start, s->x, s->y,
+                                                         s->z, s->h, c->posf, c->cellc, grow, c->list_cap,
+                                                         c->nbr_idx, c->nbr_cnt, c->nbr_gcnt, c->nbr_hlim,
+                                                         c->big_idx, c->d_sc);
     k_scatter_big<3><<<kScatterBlocks, 128, 0, st>>>(c->P, c->d_grids, c->inst, c->cell_start, s->x, s->y, s->z,
                                                      c->posf, c->cellc, grow, c->list_cap, c->nbr_idx, c->nbr_cnt,
                                                      c->big_idx, c->d_sc);
@@ -401,12 +499,16 @@ void launch_build_lists(Ctx* c, const MhdState* s, int n, cudaStream_t st) {
     k_build_lists<2><<<nb, 128, 0, st>>>(n, c->P, c->d_grids, c->inst, c->cell_start, s->x, s->y, s->z, s->h,
                                          c->posf, c->cellc, grow, c->list_cap, c->nbr_idx, c->nbr_cnt, c->nbr_gcnt,
                                          c->nbr_hlim, c->big_idx, c->d_sc);
+    k_build_lists_big<2><<<kScatterBlocks, 128, 0, st>>>(c->P, c->d_grids, c->inst, c->cell_start, s->x, s->y,
+                                                         s->z, s->h, c->posf, c->cellc, grow, c->list_cap,
+                                                         c->nbr_idx, c->nbr_cnt, c->nbr_gcnt, c->nbr_hlim,
+                                                         c->big_idx, c->d_sc);
     k_scatter_big<2><<<kScatterBlocks, 128, 0, st>>>(c->P, c->d_grids, c->inst, c->cell_start, s->x, s->y, s->z,
                                                      c->posf, c->cellc, grow, c->list_cap, c->nbr_idx, c->nbr_cnt,
                                                      c->big_idx, c->d_sc);
   }
   k_sort_appended<<<nb, 128, 0, st>>>(n, c->list_cap, c->nbr_idx, c->nbr_cnt, c->nbr_gcnt);
-  c->launches += 3;
+  c->launches += 4;
 }
 
 // ------------------------------------------------------------- dispatch
