@@ -649,6 +649,7 @@ int mhd_ctx_create(const MhdParams* params, int64_t n_max, void** out) {
   if (const char* m = getenv("MHD_STENCIL")) c->stencil = std::max(1, std::min(3, atoi(m)));
   if (const char* m = getenv("MHD_GRAPH_PASSES")) c->graph_passes = std::max(1, std::min(256, atoi(m)));
   if (const char* m = getenv("MHD_CELL_KAPPA")) c->cell_kappa = std::max(1.0, atof(m));
+  if (const char* m = getenv("MHD_LIST_MARGIN")) c->list_margin = std::max(0.005, std::min(0.5, atof(m)));
   *out = c;
   return MHD_OK;
 }

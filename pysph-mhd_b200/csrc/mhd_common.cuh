@@ -34,7 +34,7 @@ struct Grid {
   double L[3];  // the instance's periodic box (lo .. lo + L on periodic axes)
   double half[3];
   double h_plan;  // largest h whose list cut-off the +-sw stencil covers
-  double cut;     // list cut-off R * h_cell * grid_margin * (1 + margin)
+  double cut;     // search reach of a normal particle: R (1 + margin) h_plan (>= the planned cutoff)
   float csf[3];   // cell widths in FP32 (packed-position geometry)
   float h_bigf;   // particles with FP32 h above this are "big": they search an extended stencil
 };
@@ -319,7 +319,10 @@ __host__ __device__ inline int plan_instance(const PlanSpec& S, int n, double hm
   }
   g.h_plan = hplan;
   g.h_bigf = hplan < 1e30 ? (float)mul_rn(hplan, 1.0 - 1e-5) : INFINITY;
-  g.cut = cutoff;
+  // A normal particle (h <= h_plan) reaches up to R (1 + margin) h_plan,
+  // which the rounding of the cell count can put above the planned cutoff.
+  g.cut = hplan < 1e30 ? mul_rn(mul_rn(S.R, add_rn(1.0, S.list_margin)), hplan) : cutoff;
+  if (g.cut < cutoff) g.cut = cutoff;
   g.ncells = g.nc[0] * g.nc[1] * g.nc[2];
   return MHD_OK;
 }

@@ -99,8 +99,12 @@ struct Ctx {
   int force_shape = -1;  // launch-shape variant of the force pass (kForceShapes); -1 = per-precision default
   double list_cut = 0;   // R * h_max * (1 + list_margin) of the current grid
 
-  // compacted neighbour lists (NbrList layout), built with every grid
-  double list_margin = 0.05;
+  // compacted neighbour lists (NbrList layout), built with every grid.  The
+  // margin covers h growth during the density iteration (far below 2 % per
+  // step in practice; more triggers a rebuild); larger margins pull in whole
+  // lattice shells (at 5 %, the sqrt(6) shell of a cubic lattice with
+  // R h = 2.4 dx: 42 % more entries).
+  double list_margin = 0.02;
   int list_cap = 0;
   int* nbr_idx = nullptr;
   int* nbr_cnt = nullptr;

@@ -107,6 +107,33 @@ def test_lists_exact_with_a_few_large_h(maker, frac):
     _check(eng, prm, f"large h (fraction {frac})")
 
 
+@pytest.mark.parametrize("maker", [lambda: sc_.orszag_tang_2d(36, "quintic"), lambda: sc_.blast_3d(12, "cubic"),
+                                   lambda: sc_.open_blob_2d(24)])
+@pytest.mark.parametrize("spread", [0.15, 0.6])
+def test_lists_exact_with_continuously_spread_h(maker, spread):
+    # h spread continuously: many particles fall between the h the cells follow
+    # and the largest h their stencil covers, others become big
+    ic, prm = maker()
+    rng = np.random.default_rng(int(spread * 100))
+    ic = dict(ic, h=ic["h"] * (1.0 + spread * rng.random(ic["h"].size)))
+    eng = _engine(ic, prm)
+    eng.cells_build()
+    _check(eng, prm, f"continuous h spread {spread}")
+
+
+def test_lists_exact_through_steps_open_blob():
+    # an expanding open blob: h grows at its rim from step to step
+    ic, prm = sc_.open_blob_2d(20)
+    eng = _engine(ic, prm)
+    eng.warmup()
+    dt, t = eng.initial_dt(), 0.0
+    for _ in range(4):
+        eng.step(dt)
+        t += dt
+        dt = eng.timestep(t)
+        _check(eng, prm, "open blob after a step")
+
+
 def test_batched_lists_exact_with_a_few_large_h():
     from src.batch import BatchEngine
     from src.engine import params_from_dict
