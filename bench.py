@@ -22,6 +22,7 @@ graph launch after the autotuner, against the plain FP64 path run instance
 by instance.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+    python bench.py --workload ot128|briowu   # the 2-D Orszag-Tang and Brio-Wu measurements
 
 Multi-GPU: "replicas only" -- every rank advances its own independent blast
 (the per-instance update does not shard without a halo exchange); value is
@@ -430,6 +431,140 @@ def _derivative(args, dev):
                     "dL/dalpha_max = 0 exactly (also by differences)"}
 
 
+def _app_case(name, nx=None, precision=None):
+    """A case of the application layer from its TOML config (initial state and
+    kernel parameters)."""
+    from dataclasses import replace
+
+    from src.config import load_config
+    from src.run import CASES
+
+    cfg = load_config(os.path.join(PKG, "configs", f"{name}.toml"), {k: v.config_type for k, v in CASES.items()})
+    if nx is not None:
+        cfg = replace(cfg, case=replace(cfg.case, nx=nx))
+    app = CASES[cfg.case.name](cfg)
+    ic = app.create_mhd_particles()
+    prm = app.scheme.kernel_params(app.create_domain(), app.tf)
+    if precision:
+        prm = dict(prm, precision=precision)
+    return ic, prm, cfg
+
+
+def run_workload(args):
+    """The other measured configurations, one JSON line each:
+    ot128  -- 2-D Orszag-Tang 128^2, quintic, 50 steps: FP64 on the GPU and the
+              CPU oracle (FP64, OpenMP) on the same case;
+    briowu -- 2-D Brio-Wu 4096 x 128 slab to t = 0.1: the FP32 form against the
+              FP64 path, relative L2 error per field."""
+    import torch
+
+    from src.batch import BatchEngine
+    from src.engine import params_from_dict
+
+    def run_gpu(ic, prm, steps=None, until=None):
+        """`steps` captured fused steps (timed on a replay of the captured
+        run), or steps until t = `until` as the reference's solver loop takes
+        them: captured chunks of 100 while more than 150 steps of the current
+        dt remain, then single steps up to the one clipped to `until`."""
+        eng = BatchEngine(params_from_dict(prm), [ic])
+        eng.warmup()
+        eng.begin(eng.initial_dt())
+        done = 0
+        if steps is not None:
+            snap = eng.snapshot()
+            eng.advance(steps, finish=True, snapshot=snap)  # capture + first run
+            eng.restore(snap)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            eng.advance(steps, finish=True, snapshot=snap)
+            done = steps
+        else:
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            while True:
+                t, dt = (float(a[0]) for a in eng.clocks())
+                if t + dt >= until * (1.0 - 1e-14) or dt <= 0.0:
+                    eng.advance(1, finish=True, capture=False)
+                    done += 1
+                    break
+                if (until - t) > 150.0 * dt:
+                    eng.advance(100, finish=False)
+                    done += 100
+                else:
+                    eng.advance(1, finish=False, capture=False)
+                    done += 1
+        torch.cuda.synchronize()
+        el = time.perf_counter() - t0
+        t, dt = (float(a[0]) for a in eng.clocks())
+        out = eng.pa.pull("x", "rho", "u", "v", "w", "Bx", "By", "Bz", "e", "gid", order="gid")
+        eng.close()
+        return out, el, done, t + dt
+
+    if args.workload == "ot128":
+        import oracle
+
+        ic, prm, _ = _app_case("orstang2d", precision="fp64")
+        n = len(ic["x"])
+        steps = 50
+        gpu, el, _, _ = run_gpu(ic, prm, steps=steps)
+        oracle.build()
+        s = oracle.State(dict(ic, gid=np.arange(n, dtype=float)))
+        o = oracle.Oracle(prm, exact_order=False, nthreads=cpu_cores())
+        o.warmup(s)
+        t0 = time.perf_counter()
+        o.run(s, steps, tf=prm["tf"])
+        cel = time.perf_counter() - t0
+        rel = {k: float(np.linalg.norm(gpu[k] - s[k]) / max(np.linalg.norm(s[k]), 1e-300))
+               for k in ("rho", "u", "v", "Bx", "By")}
+        print(json.dumps({"workload": f"2-D Orszag-Tang 128^2 = {n} particles, quintic hfact 1.2, {steps} steps, FP64",
+                          "gpu_fp64": {"value": n * steps / el, "unit": UNIT},
+                          "cpu_oracle_fp64": {"value": n * steps / cel, "unit": UNIT, "cores": cpu_cores()},
+                          "gpu_vs_cpu_rel_l2": rel}), flush=True)
+    else:
+        # The FP32 form against the FP64 path, and as a control the FP64 path
+        # against itself with the free particles' x moved by 1e-10 of the left
+        # spacing: a shock tube's post-shock particle noise amplifies any
+        # perturbation, so the control's error is the floor that rounding of
+        # either kind reaches.  Errors per particle and of the x profile
+        # (means over 500 bins across [-0.5, 0.5], the quantity a shock-tube
+        # plot shows).
+        ic, prm, cfg = _app_case("mhdshock2d")
+        n = len(ic["x"])
+        dx = 0.5 / cfg.case.nx
+        free = ic["itype"] == 1
+        pert = dict(ic, x=ic["x"] + np.where(free, 1e-10 * dx * np.random.default_rng(0).uniform(-1, 1, n), 0.0))
+        fields = ("rho", "u", "v", "e", "By", "Bx")
+        edges = np.linspace(-0.5, 0.5, 501)
+
+        def profile(o, k):
+            idx = np.clip(np.digitize(o["x"], edges) - 1, 0, 499)
+            inside = (o["x"] >= -0.5) & (o["x"] < 0.5)
+            s = np.bincount(idx[inside], o[k][inside], 500)
+            c = np.bincount(idx[inside], None, 500)
+            return s / np.maximum(c, 1)
+
+        def errors(a, b):
+            part = {k: float(np.linalg.norm(a[k] - b[k]) / max(np.linalg.norm(b[k]), 1e-300)) for k in fields}
+            prof = {}
+            for k in fields:
+                pa_, pb_ = profile(a, k), profile(b, k)
+                prof[k] = float(np.linalg.norm(pa_ - pb_) / max(np.linalg.norm(pb_), 1e-300))
+            return {"particles": part, "x_profile": prof}
+
+        report = {}
+        for until in (0.02, prm["tf"]):
+            res = {}
+            for name, prec, init in (("fp64", "fp64", ic), ("fp32", "fp32", ic), ("fp64_perturbed", "fp64", pert)):
+                res[name] = run_gpu(init, dict(prm, precision=prec, tf=until), until=until)
+            report[f"t={until}"] = {
+                "steps": {k: r[2] for k, r in res.items()}, "t_end": {k: r[3] for k, r in res.items()},
+                "rate": {k: n * r[2] / r[1] for k, r in res.items()},
+                "fp32_vs_fp64": errors(res["fp32"][0], res["fp64"][0]),
+                "fp64_perturbed_vs_fp64": errors(res["fp64_perturbed"][0], res["fp64"][0])}
+        print(json.dumps({"workload": f"2-D Brio-Wu {n} particles (4096 x 128 left lattice, right at density 1/8), "
+                                      f"gamma 2, quintic hfact 1.0", "unit": UNIT, "runs": report}), flush=True)
+
+
 def run_b200(args, rank, world):
     import ctypes
 
@@ -587,11 +722,16 @@ def main():
     ap.add_argument("--batch-steps", type=int, default=100)
     ap.add_argument("--batch-loop-steps", type=int, default=10, help="steps per instance of the FP64 loop")
     ap.add_argument("--derivative-steps", type=int, default=200, help="derivative form steps (0 skips it)")
+    ap.add_argument("--workload", default="blast", choices=("blast", "ot128", "briowu"),
+                    help="blast: the benchmark line; ot128 / briowu: the other measured configurations")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
-    if args.impl == "reference":
+    if args.workload != "blast":
+        if rank == 0:
+            run_workload(args)
+    elif args.impl == "reference":
         run_reference(args, rank)
     else:
         run_b200(args, rank, world)
