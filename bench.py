@@ -234,6 +234,9 @@ def _timed(args, prec, dev, barrier, dist, world):
     snap = eng.snapshot()
     replays0 = eng.replays
     launches0 = eng.launches()
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    listed, rebuilt = ctypes.c_int64(), ctypes.c_int64()
+    lib.mhd_list_counts(eng.ctx, ctypes.byref(listed), ctypes.byref(rebuilt), st)
     clocks = ClockSampler(dev.index or 0)
     barrier()
     torch.cuda.synchronize()
@@ -247,6 +250,7 @@ def _timed(args, prec, dev, barrier, dist, world):
     barrier()
     clocks.stop()
     ms = e0.elapsed_time(e1)
+    lib.mhd_list_counts(eng.ctx, ctypes.byref(listed), ctypes.byref(rebuilt), st)
     launches = eng.launches() - launches0
     replays = eng.replays - replays0
     ms_max = ms
@@ -257,7 +261,6 @@ def _timed(args, prec, dev, barrier, dist, world):
         tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
         ms_max = float(t.item())
     # kernel breakdown (uncaptured, identical kernels)
-    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
     ms_k = (ctypes.c_double * len(_abi.TIMING_KINDS))()
     cnt_k = (ctypes.c_int64 * len(_abi.TIMING_KINDS))()
     pairs, cands = ctypes.c_int64(), ctypes.c_int64()
@@ -279,7 +282,7 @@ def _timed(args, prec, dev, barrier, dist, world):
     return {"value": world * n * args.steps / (ms_max * 1e-3), "ms_per_step": ms_max / args.steps,
             "ms_per_step_uncaptured": ms_unc / args.steps, "kernels": kern, "launches": launches,
             "replays": replays, "clocks": clocks.summary(), "pairs": pairs.value, "candidates": cands.value,
-            "passes": passes}
+            "passes": passes, "lists_rebuilt": rebuilt.value / max(listed.value, 1)}
 
 
 def _batched(args, dev):
@@ -631,7 +634,8 @@ def run_b200(args, rank, world):
                        "density_passes_per_rhs": head["passes"], "timed_run": "one captured graph of K fused steps",
                        "replays": head["replays"], "ms_per_step_uncaptured": head["ms_per_step_uncaptured"],
                        "neighbours_mean": head["pairs"] / (n * args.steps),
-                       "list_entries_mean": head["candidates"] / (n * args.steps)},
+                       "list_entries_mean": head["candidates"] / (n * args.steps),
+                       "lists_rebuilt_fraction": head["lists_rebuilt"]},
             "fp64_path": None if base is None else {"value": base["value"], "ms_per_step": base["ms_per_step"],
                                                     "kernels_ms_per_step": {k: v["ms_total"] / args.steps for k, v
                                                                             in base["kernels"].items()}},

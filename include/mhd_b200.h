@@ -161,6 +161,13 @@ int mhd_probe_fma_peak(int32_t precision, double* flops_per_second, void* stream
    since the previous call (synchronises, then resets). */
 int mhd_pair_counts(void* ctx, int64_t* pairs, int64_t* candidates, void* stream);
 
+/* Particles whose neighbour lists were built or carried over across a sort
+   (`listed`), and of those the lists built afresh (`rebuilt`), over all
+   list builds since the previous call (synchronises, then resets).  No
+   reference counterpart: PySPH rebuilds every neighbour structure on every
+   update (its NNPS), which this library does when MHD_LIST_REUSE=0. */
+int mhd_list_counts(void* ctx, int64_t* listed, int64_t* rebuilt, void* stream);
+
 /* ---- neighbour search ----
    Sort the particles of `src` by cell of the neighbour grid (Morton-free
    linear cell order, stable LSD radix sort + prefix scan) and write the

@@ -184,10 +184,16 @@ void refresh_spec(Ctx* c) {
 int grow_cell_table(Ctx* c, int64_t cells) {
   if (cells + 1 <= c->cell_cap) return MHD_OK;
   if (c->cell_start) cudaFree(c->cell_start);
+  for (unsigned*& p : c->cell_scr) {
+    cudaFree(p);
+    p = nullptr;
+  }
   c->cell_start = nullptr;
   c->cell_cap = 0;
   const int64_t want = cells + 1 + (cells >> 2);
-  if (dev_alloc(c, &c->cell_start, want) != MHD_OK) return MHD_ERR_CUDA;
+  if (dev_alloc(c, &c->cell_start, want) != MHD_OK || dev_alloc(c, &c->cell_scr[0], want) != MHD_OK ||
+      dev_alloc(c, &c->cell_scr[1], want) != MHD_OK)
+    return MHD_ERR_CUDA;
   c->cell_cap = want;
   c->generation++;
   return MHD_OK;
@@ -281,11 +287,17 @@ int alloc_instances(Ctx* c, int n_inst, const int64_t* start) {
 
 // Allocate (or grow) the neighbour-list storage for `cap` entries per particle.
 int ensure_list_storage(Ctx* c, int cap) {
-  if (cap <= c->list_cap && c->nbr_idx) return MHD_OK;
-  cudaFree(c->nbr_idx);
+  if (cap <= c->list_cap && c->slots[0].idx && c->slots[1].idx) return MHD_OK;
+  for (Ctx::ListSlot& S : c->slots) {
+    cudaFree(S.idx);
+    S.idx = nullptr;
+    S.key = nullptr;  // no lists to carry over
+  }
   c->nbr_idx = nullptr;
   c->list_cap = 0;
-  if (dev_alloc(c, &c->nbr_idx, c->n_pad * (int64_t)cap) != MHD_OK) return MHD_ERR_CUDA;
+  for (Ctx::ListSlot& S : c->slots)
+    if (dev_alloc(c, &S.idx, c->n_pad * (int64_t)cap) != MHD_OK) return MHD_ERR_CUDA;
+  c->nbr_idx = c->slots[0].idx;
   c->list_cap = cap;
   c->generation++;
   return MHD_OK;
@@ -313,7 +325,7 @@ int sort_into(Ctx* c, const MhdState* src, MhdState* dst, int n, cudaStream_t st
     launch_gather(c, a, n, st);
   }
   launch_pack_positions(c, dst, n, st);
-  launch_build_lists(c, dst, n, st);
+  launch_build_lists(c, dst, n, st, src);
   c->lists_checked = false;
   CK(cudaGetLastError());
   return MHD_OK;
@@ -354,7 +366,7 @@ int resort_in_place(Ctx* c, MhdState* s, int n, cudaStream_t st) {
     CK(cudaMemcpyAsync(s->itype, itmp, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, st));
   }
   launch_pack_positions(c, s, n, st);
-  launch_build_lists(c, s, n, st);
+  launch_build_lists(c, s, n, st, nullptr);
   c->lists_checked = false;
   CK(cudaGetLastError());
   return MHD_OK;
@@ -626,9 +638,15 @@ int mhd_ctx_create(const MhdParams* params, int64_t n_max, void** out) {
     const double vol = params->dim == 3 ? 4.0 / 3.0 * M_PI * rr * rr * rr : M_PI * rr * rr;
     const int cap = ((int)(1.5 * vol) + 16 + 7) & ~7;
     ok = ok && dev_alloc(c, &c->posf, c->n_pad) == MHD_OK && dev_alloc(c, &c->cellc, c->n_pad) == MHD_OK;
-    ok = ok && dev_alloc(c, &c->nbr_cnt, c->n_pad) == MHD_OK && dev_alloc(c, &c->nbr_hlim, c->n_pad) == MHD_OK &&
-         dev_alloc(c, &c->nbr_gcnt, c->n_pad) == MHD_OK && dev_alloc(c, &c->big_idx, c->n_pad) == MHD_OK &&
-         ensure_list_storage(c, cap) == MHD_OK;
+    ok = ok && dev_alloc(c, &c->nbr_hlim, c->n_pad) == MHD_OK && dev_alloc(c, &c->big_idx, c->n_pad) == MHD_OK &&
+         dev_alloc(c, &c->new_of_old, c->n_pad) == MHD_OK && dev_alloc(c, &c->nbr_mark, c->n_pad) == MHD_OK;
+    for (Ctx::ListSlot& S : c->slots)
+      ok = ok && dev_alloc(c, &S.cnt, c->n_pad) == MHD_OK && dev_alloc(c, &S.gcnt, c->n_pad) == MHD_OK &&
+           dev_alloc(c, &S.xr, 3 * c->n_pad) == MHD_OK && dev_alloc(c, &S.hm, c->n_pad) == MHD_OK &&
+           dev_alloc(c, &S.md, c->n_pad) == MHD_OK;
+    ok = ok && ensure_list_storage(c, cap) == MHD_OK;
+    c->nbr_cnt = c->slots[0].cnt;
+    c->nbr_gcnt = c->slots[0].gcnt;
   }
   if (ok && cudaMallocHost((void**)&c->h_sc, sizeof(DevScalars)) != cudaSuccess) ok = false;
   const int64_t one[2] = {0, N};
@@ -650,6 +668,7 @@ int mhd_ctx_create(const MhdParams* params, int64_t n_max, void** out) {
   if (const char* m = getenv("MHD_GRAPH_PASSES")) c->graph_passes = std::max(1, std::min(256, atoi(m)));
   if (const char* m = getenv("MHD_CELL_KAPPA")) c->cell_kappa = std::max(1.0, atof(m));
   if (const char* m = getenv("MHD_LIST_MARGIN")) c->list_margin = std::max(0.005, std::min(0.5, atof(m)));
+  if (const char* m = getenv("MHD_LIST_REUSE")) c->list_reuse = atoi(m) != 0;
   *out = c;
   return MHD_OK;
 }
@@ -672,9 +691,17 @@ int mhd_ctx_destroy(void* ctx) {
   for (void* p : c->rec) cudaFree(p);
   cudaFree(c->posf);
   cudaFree(c->cellc);
-  cudaFree(c->nbr_idx);
-  cudaFree(c->nbr_cnt);
-  cudaFree(c->nbr_gcnt);
+  for (Ctx::ListSlot& S : c->slots) {
+    cudaFree(S.idx);
+    cudaFree(S.cnt);
+    cudaFree(S.gcnt);
+    cudaFree(S.xr);
+    cudaFree(S.hm);
+    cudaFree(S.md);
+  }
+  cudaFree(c->new_of_old);
+  cudaFree(c->nbr_mark);
+  for (unsigned* p : c->cell_scr) cudaFree(p);
   cudaFree(c->big_idx);
   cudaFree(c->nbr_hlim);
   for (double* p : c->spare) cudaFree(p);
@@ -751,6 +778,18 @@ int mhd_pair_counts(void* ctx, int64_t* pairs, int64_t* candidates, void* stream
   if (pairs) *pairs = (int64_t)c->h_sc->n_pairs;
   if (candidates) *candidates = (int64_t)c->h_sc->n_candidates;
   CK(cudaMemsetAsync(&c->d_sc->n_pairs, 0, 2 * sizeof(unsigned long long), st));
+  return MHD_OK;
+}
+
+int mhd_list_counts(void* ctx, int64_t* listed, int64_t* rebuilt, void* stream) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return MHD_ERR_INVALID;
+  const cudaStream_t st = S(stream);
+  CK(cudaMemcpyAsync(c->h_sc, c->d_sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (listed) *listed = (int64_t)c->h_sc->n_listed;
+  if (rebuilt) *rebuilt = (int64_t)c->h_sc->n_rebuilt;
+  CK(cudaMemsetAsync(&c->d_sc->n_listed, 0, 2 * sizeof(unsigned long long), st));
   return MHD_OK;
 }
 
@@ -995,6 +1034,7 @@ int mhd_ctx_set_instances(void* ctx, const MhdState* s, int32_t n_inst, const in
   c->key_cells = (int)base;
   c->batched = true;
   c->generation++;
+  c->layout_gen++;
   return MHD_OK;
 }
 

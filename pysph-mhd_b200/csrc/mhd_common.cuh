@@ -87,6 +87,8 @@ struct DevScalars {
   unsigned long long n_pairs;       // force-pass neighbour pairs (accumulating)
   unsigned long long n_candidates;  // force-pass distance tests (accumulating)
   int n_unconverged[256 + 8];       // per density pass
+  unsigned long long n_listed;      // particles whose lists were built or carried over (accumulating)
+  unsigned long long n_rebuilt;     // of those, lists built afresh (accumulating)
 };
 
 // Device-resident scalars of one instance: its step clock and the
@@ -479,7 +481,10 @@ __device__ __forceinline__ void for_each_cell_trimmed(const Grid& G, int sw, con
 // offset that turns a particle's own cell x into its unwrapped coordinate
 // (-nx, 0 or +nx; 0 on an axis scanned whole).  Pieces come in ascending
 // unwrapped x, so a caller sees the particles in the order of
-// for_each_cell_trimmed.
+// for_each_cell_trimmed.  Where the x-range is not the whole axis, a row
+// keeps only its cells within sqrt(cut^2 - dym^2 - dzm^2) of xi (dym, dzm
+// the distances to the row's cell box): a subset of the full range in the
+// same order, missing only particles farther than cut.
 template <int DIM, class F>
 __device__ __forceinline__ void for_each_row_trimmed(const Grid& G, int sw, const int* __restrict__ cell_start,
                                                      double xi, double yi, double zi, double cut, F&& f) {
@@ -487,18 +492,20 @@ __device__ __forceinline__ void for_each_row_trimmed(const Grid& G, int sw, cons
   const int nx = G.nc[0], ny = G.nc[1], nz = G.nc[2];
   const int cy = cell_coord(G, 1, yi);
   const int cz = DIM == 3 ? cell_coord(G, 2, zi) : 0;
-  int xl, xh;
+  int xl0, xh0;
+  bool xtrim = false;
   if (nx < whole) {
-    xl = 0;
-    xh = nx - 1;
+    xl0 = 0;
+    xh0 = nx - 1;
   } else {
-    xl = (int)floor((xi - cut - G.lo[0]) * G.inv_cs[0]);
-    xh = (int)floor((xi + cut - G.lo[0]) * G.inv_cs[0]);
+    xl0 = (int)floor((xi - cut - G.lo[0]) * G.inv_cs[0]);
+    xh0 = (int)floor((xi + cut - G.lo[0]) * G.inv_cs[0]);
     if (!G.periodic[0]) {
-      xl = xl < 0 ? 0 : xl;
-      xh = xh >= nx ? nx - 1 : xh;
+      xl0 = xl0 < 0 ? 0 : xl0;
+      xh0 = xh0 >= nx ? nx - 1 : xh0;
     }
-    if (xh - xl >= nx) xh = xl + nx - 1;  // never visit a cell twice
+    if (xh0 - xl0 >= nx) xh0 = xl0 + nx - 1;  // never visit a cell twice
+    else xtrim = true;
   }
   const double cut2 = cut * cut;
   const bool zs = DIM == 3 && nz >= whole, ys = ny >= whole;
@@ -518,9 +525,10 @@ __device__ __forceinline__ void for_each_row_trimmed(const Grid& G, int sw, cons
     }
     for (int yu = ylo; yu <= yhi; yu++) {
       int yc = yu;
+      double dym = 0.0;
       if (ys) {
         const double c_lo = G.lo[1] + yu * G.cs[1], c_hi = c_lo + G.cs[1];
-        const double dym = yi < c_lo ? c_lo - yi : (yi > c_hi ? yi - c_hi : 0.0);
+        dym = yi < c_lo ? c_lo - yi : (yi > c_hi ? yi - c_hi : 0.0);
         if (dym * dym + dzm * dzm >= cut2) continue;
         if (yc < 0 || yc >= ny) {
           if (!G.periodic[1]) continue;
@@ -528,6 +536,15 @@ __device__ __forceinline__ void for_each_row_trimmed(const Grid& G, int sw, cons
         }
       }
       const int base = G.cell_base + (zc * ny + yc) * nx;
+      int xl = xl0, xh = xh0;
+      if (xtrim) {
+        const double wx = sqrt(cut2 - (dym * dym + dzm * dzm));
+        const int a = (int)floor((xi - wx - G.lo[0]) * G.inv_cs[0]);
+        const int b = (int)floor((xi + wx - G.lo[0]) * G.inv_cs[0]);
+        xl = a > xl ? a : xl;
+        xh = b < xh ? b : xh;
+        if (xl > xh) continue;
+      }
       // [xl, xh] in unwrapped cells: at most three pieces (below 0, inside,
       // above nx - 1)
       if (xl < 0) {

@@ -106,11 +106,40 @@ struct Ctx {
   // R h = 2.4 dx: 42 % more entries).
   double list_margin = 0.02;
   int list_cap = 0;
+  // current lists: the arrays of the slot built last
   int* nbr_idx = nullptr;
   int* nbr_cnt = nullptr;
   int* nbr_gcnt = nullptr;  // entries of the gather pass (the rest were scattered)
   int* big_idx = nullptr;   // big particles of the last build (DevScalars::n_big of them)
   double* nbr_hlim = nullptr;
+
+  // Lists persist across sorts in two slots, one per state buffer the caller
+  // alternates between (keyed by the buffer's x array): the sort into a
+  // buffer carries each list of the other buffer's slot to its particle's
+  // new place, renumbered through the sort, where no pair it lacks can have
+  // come within range, and rebuilds the rest.  Per particle a slot keeps an
+  // epoch reference position xr, the largest distance md from it seen
+  // since, and the smallest h hm seen since (see k_track).
+  struct ListSlot {
+    const double* key = nullptr;  // x array of the state whose order the lists follow
+    int64_t n = -1;
+    int64_t layout = -1;          // layout_gen when built
+    uint64_t use = 0;
+    int* idx = nullptr;
+    int* cnt = nullptr;
+    int* gcnt = nullptr;
+    double* xr = nullptr;  // 3 x n_pad
+    double* hm = nullptr;
+    float* md = nullptr;
+  };
+  ListSlot slots[2];
+  uint64_t slot_clock = 0;
+  int64_t layout_gen = 0;     // bumped when the particle layout (instances) changes
+  bool list_reuse = true;     // MHD_LIST_REUSE=0: rebuild every list on every sort
+  int* new_of_old = nullptr;  // inverse of the last sort's permutation
+  int* nbr_mark = nullptr;    // per particle: dirty, then "rebuild"
+  unsigned* cell_scr[2] = {nullptr, nullptr};  // per-cell scratch (cell_cap entries each)
+  int64_t last_rebuilt = -1;  // lists rebuilt by the last build (-1: not counted)
   int64_t n_pad = 0;  // n_max rounded up to a multiple of 32
   bool lists_checked = false;  // the host knows the current lists are valid
   NbrList lists() const { return NbrList{nbr_idx, nbr_cnt, nbr_hlim, list_cap}; }
@@ -162,7 +191,10 @@ void launch_gather(Ctx* c, const GatherSet& gs, int n, cudaStream_t st);
 
 void launch_reset_hbox(Ctx* c, cudaStream_t st);
 void launch_plan_grids(Ctx* c, cudaStream_t st);
-void launch_build_lists(Ctx* c, const MhdState* s, int n, cudaStream_t st);
+// Lists of the sorted particles of s; src is the state s was sorted from
+// (its slot's lists are carried over where they stay valid), or null for a
+// full rebuild.
+void launch_build_lists(Ctx* c, const MhdState* s, int n, cudaStream_t st, const MhdState* src);
 void launch_pack_positions(Ctx* c, const MhdState* s, int n, cudaStream_t st);
 void launch_neighbour_counts(Ctx* c, const MhdState* s, int n, int* out, cudaStream_t st);
 // density pass `pass` (0-based) reading h_in, writing h_out

@@ -213,9 +213,10 @@ __global__ void __launch_bounds__(128) k_build_lists(int n, DevParams P, const G
                                                      float grow, int cap, int* __restrict__ idx,
                                                      int* __restrict__ cnt_out, int* __restrict__ gcnt_out,
                                                      double* __restrict__ hlim, int* __restrict__ big_idx,
-                                                     DevScalars* sc) {
+                                                     const int* __restrict__ mark, DevScalars* sc) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  if (mark && !mark[i]) return;  // list carried over
   const Grid& G = grid_of(grids, inst, i);
   const float4 pi = posf[i];
   const int ci = cellc[i];
@@ -295,7 +296,8 @@ __global__ void __launch_bounds__(128) k_scatter_big(DevParams P, const Grid* __
                                                      const double* __restrict__ z, const float4* __restrict__ posf,
                                                      const int* __restrict__ cellc, float grow, int cap,
                                                      int* __restrict__ idx, int* __restrict__ cnt,
-                                                     const int* __restrict__ big_idx, DevScalars* sc) {
+                                                     const int* __restrict__ big_idx, const int* __restrict__ mark,
+                                                     const int* __restrict__ gcnt, DevScalars* sc) {
   // one warp per big particle: the lanes take consecutive candidates
   const int nb = sc->n_big, lane = threadIdx.x & 31;
   const float Rg = __fmul_rn((float)P.R, grow);
@@ -319,9 +321,18 @@ __global__ void __launch_bounds__(128) k_scatter_big(DevParams P, const Grid* __
         const float r2 = sym_r2<DIM>(G, pi, __ldg(cellc + i), pj, cj);
         if (!(r2 < reach_j)) continue;
         if (pi.w > hbig && r2 < reach2(Rg, pi.w, slack)) continue;  // i kept j itself
+        int* __restrict__ irow = idx + (size_t)(i >> 5) * cap * 32 + (i & 31);
+        if (mark && !mark[i]) {
+          // a carried-over list may hold j already (its appended entries
+          // of this build start after gcnt)
+          const int g = gcnt[i];
+          bool held = false;
+          for (int e = 0; e < g && !held; e++) held = irow[(size_t)e * 32] == j;
+          if (held) continue;
+        }
         const int slot = atomicAdd(cnt + i, 1);
         if (slot < cap) {
-          idx[(size_t)(i >> 5) * cap * 32 + (i & 31) + (size_t)slot * 32] = j;
+          irow[(size_t)slot * 32] = j;
         } else {
           atomicMax(&sc->list_max, slot + 1);
           atomicExch(&sc->relist, 1);
@@ -440,6 +451,184 @@ __global__ void __launch_bounds__(128) k_sort_appended(int n, int cap, int* __re
   }
 }
 
+// ------------------------------------------------- lists across sorts
+// A list built at time t_b holds every j with r(t_b) < R (1 + margin)
+// (1 - 1e-4) max(h_i(t_b), h_j(t_b)).  Every particle k keeps an epoch: a
+// reference position xr_k, md_k = the largest |x_k - xr_k| seen since, and
+// hm_k = the smallest h_k seen since (h at the start of each right-hand
+// side).  Any particle moved by at most 2 md since any time of its epoch, so
+// a pair absent from a list has r(now) >= R (1 + margin)(1 - 1e-4) hm - 4 D,
+// D the largest md of the two, and the list stays valid while
+//   h_k <= hlim_k = (1 + margin)(1 - 1e-4) hm_k - 4 D_k / R
+// for every k, D_k the largest md in the cells within sw + 1 of k's cell
+// (every partner within reach, one cell of slack).  A particle failing the
+// test (with a quarter of the margin as headroom for the coming density
+// iteration), and every big particle, is dirty: it starts a new epoch, and
+// every list within sw + 1 cells of it is rebuilt, so no list built before
+// that epoch can lack it while it is in reach.  Big particles (rebuilt every
+// time) append themselves to carried-over lists that lack them.  md is also
+// recorded in the cell of xr: if the state was changed behind the lists'
+// back, the particle now at an index is not the one the lists name, and the
+// distance between the two marks both places.
+
+__device__ __forceinline__ int cell_key(const Grid& G, double x, double y, double z) {
+  const int cx = cell_coord(G, 0, x), cy = cell_coord(G, 1, y), cz = cell_coord(G, 2, z);
+  return G.cell_base + (cz * G.nc[1] + cy) * G.nc[0] + cx;
+}
+
+// Warp-aggregated add of the active lanes' flags to a device counter.
+__device__ __forceinline__ void count_lanes(unsigned long long* ctr, bool flag) {
+  const unsigned act = __activemask();
+  const unsigned b = __ballot_sync(act, flag);
+  if ((int)(threadIdx.x & 31) == __ffs(act) - 1 && b) atomicAdd(ctr, (unsigned long long)__popc(b));
+}
+
+// Epoch bookkeeping of sorted particle k (source index o = perm[k]): xr, hm
+// and md carried from the old slot and updated; md marked in the cells of x
+// and xr.  With `full` every epoch starts now.
+template <int DIM>
+__global__ void __launch_bounds__(256) k_track(int n, int full, const Grid* __restrict__ grids,
+                                               const int* __restrict__ inst, const int* __restrict__ perm,
+                                               const double* __restrict__ x, const double* __restrict__ y,
+                                               const double* __restrict__ z, const double* __restrict__ h,
+                                               const double* __restrict__ xr_old, const double* __restrict__ hm_old,
+                                               const float* __restrict__ md_old, double* __restrict__ xr_new,
+                                               double* __restrict__ hm_new, float* __restrict__ md_new, int64_t pad,
+                                               int* __restrict__ new_of_old, unsigned* __restrict__ cell_md,
+                                               DevScalars* sc) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  count_lanes(&sc->n_listed, true);
+  const double xk = x[k], yk = y[k], zk = DIM == 3 ? z[k] : 0.0, hk = h[k];
+  if (full) {
+    count_lanes(&sc->n_rebuilt, true);
+    xr_new[k] = xk;
+    xr_new[pad + k] = yk;
+    xr_new[2 * pad + k] = zk;
+    hm_new[k] = hk;
+    md_new[k] = 0.f;
+    return;
+  }
+  const Grid& G = grid_of(grids, inst, k);
+  const int o = perm[k];
+  new_of_old[o] = k;
+  const double rx = xr_old[o], ry = xr_old[pad + o], rz = DIM == 3 ? xr_old[2 * pad + o] : 0.0;
+  const double dx = min_image(xk - rx, G.L[0], G.half[0], G.periodic[0]);
+  const double dy = min_image(yk - ry, G.L[1], G.half[1], G.periodic[1]);
+  const double dz = DIM == 3 ? min_image(zk - rz, G.L[2], G.half[2], G.periodic[2]) : 0.0;
+  float m = __double2float_ru(sqrt(dx * dx + dy * dy + dz * dz));
+  const float mo = md_old[o];
+  m = mo > m ? mo : m;
+  if (!(m <= 3.0e38f)) m = INFINITY;  // non-finite: moved arbitrarily far
+  const double hmo = hm_old[o];
+  xr_new[k] = rx;
+  xr_new[pad + k] = ry;
+  xr_new[2 * pad + k] = rz;
+  hm_new[k] = hmo < hk ? hmo : hk;
+  md_new[k] = m;
+  const unsigned bits = __float_as_uint(m);
+  if (bits) {
+    atomicMax(cell_md + cell_key(G, xk, yk, zk), bits);
+    atomicMax(cell_md + cell_key(G, rx, ry, rz), bits);
+  }
+}
+
+// out = the max of `in` over the cells within sw + 1 along one axis of each
+// instance's grid (periodic wrap; an axis of at most 2 (sw + 1) + 1 cells is
+// taken whole).  Values are non-negative FP32 bit patterns or flags.
+__global__ void __launch_bounds__(256) k_dilate(int ncells, int n_inst, const Grid* __restrict__ grids, int axis,
+                                                const unsigned* __restrict__ in, unsigned* __restrict__ out) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncells) return;
+  int lo = 0, hi = n_inst - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (grids[mid].cell_base <= c) lo = mid;
+    else hi = mid - 1;
+  }
+  const Grid& G = grids[lo];
+  const int local = c - G.cell_base;
+  if (local >= G.ncells) {
+    out[c] = 0u;
+    return;
+  }
+  const int nx = G.nc[0], ny = G.nc[1];
+  const int coord = axis == 0 ? local % nx : (axis == 1 ? (local / nx) % ny : local / (nx * ny));
+  const int stride = axis == 0 ? 1 : (axis == 1 ? nx : nx * ny);
+  const int nc = G.nc[axis], base = c - coord * stride, w = G.sw + 1;
+  unsigned m = 0u;
+  if (nc <= 2 * w + 1) {
+    for (int t = 0; t < nc; t++) m = max(m, in[base + t * stride]);
+  } else {
+    for (int d = -w; d <= w; d++) {
+      int t = coord + d;
+      if (t < 0 || t >= nc) {
+        if (!G.periodic[axis]) continue;
+        t = t < 0 ? t + nc : t - nc;
+      }
+      m = max(m, in[base + t * stride]);
+    }
+  }
+  out[c] = m;
+}
+
+// Dirty particles: big ones, and those whose limit leaves no headroom.
+// Writes the limit (the density iteration's check) and flags the cells.
+__global__ void __launch_bounds__(256) k_mark(int n, DevParams P, const Grid* __restrict__ grids,
+                                              const int* __restrict__ inst, const uint32_t* __restrict__ keys,
+                                              const double* __restrict__ h, const float4* __restrict__ posf,
+                                              const double* __restrict__ hm, const unsigned* __restrict__ cell_md,
+                                              double grow1, double headroom, double* __restrict__ hlim,
+                                              int* __restrict__ mark, unsigned* __restrict__ cell_dirty) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const Grid& G = grid_of(grids, inst, k);
+  const uint32_t key = keys[k];
+  const double D = (double)__uint_as_float(cell_md[key]);
+  const double lim = grow1 * hm[k] - 4.0 * D / P.R;
+  const bool dirty = posf[k].w > G.h_bigf || !(h[k] * headroom <= lim);
+  hlim[k] = lim;
+  mark[k] = dirty ? 1 : 0;
+  if (dirty) cell_dirty[key] = 1u;
+}
+
+// Carry the clean lists over (entry j of the source order becomes
+// new_of_old[j]); a dirty particle starts a new epoch; mark becomes "rebuild"
+// for dirty particles and every particle within sw + 1 cells of one.
+__global__ void __launch_bounds__(256) k_remap(int n, int cap, const int* __restrict__ perm,
+                                               const uint32_t* __restrict__ keys, const int* __restrict__ new_of_old,
+                                               const unsigned* __restrict__ cell_dirty, int* __restrict__ mark,
+                                               const double* __restrict__ x, const double* __restrict__ y,
+                                               const double* __restrict__ z, const double* __restrict__ h,
+                                               double* __restrict__ xr_new, double* __restrict__ hm_new,
+                                               float* __restrict__ md_new, int64_t pad,
+                                               const int* __restrict__ idx_old, const int* __restrict__ cnt_old,
+                                               int* __restrict__ idx_new, int* __restrict__ cnt_new,
+                                               int* __restrict__ gcnt_new, DevScalars* sc) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int dirty = mark[k];
+  if (dirty) {
+    xr_new[k] = x[k];
+    xr_new[pad + k] = y[k];
+    xr_new[2 * pad + k] = z[k];
+    hm_new[k] = h[k];
+    md_new[k] = 0.f;
+  }
+  const bool rebuild = dirty || cell_dirty[keys[k]] != 0u;
+  mark[k] = rebuild ? 1 : 0;
+  count_lanes(&sc->n_rebuilt, rebuild);
+  if (rebuild) return;
+  const int o = perm[k];
+  int c = cnt_old[o];
+  c = c < cap ? c : cap;
+  const int* __restrict__ src = idx_old + (size_t)(o >> 5) * cap * 32 + (o & 31);
+  int* __restrict__ dst = idx_new + (size_t)(k >> 5) * cap * 32 + (k & 31);
+  for (int e = 0; e < c; e++) dst[(size_t)e * 32] = new_of_old[src[(size_t)e * 32]];
+  cnt_new[k] = c;
+  gcnt_new[k] = c;
+}
+
 // Neighbours of each particle under the exact FP64 rule of the oracle
 // (r2 < (R h_i)^2 or r2 < (R h_j)^2, self included), counted over its list.
 template <int DIM>
@@ -478,37 +667,85 @@ void launch_neighbour_counts(Ctx* c, const MhdState* s, int n, int* out, cudaStr
   c->launches++;
 }
 
-void launch_build_lists(Ctx* c, const MhdState* s, int n, cudaStream_t st) {
+// Max of a per-cell array over the cells within sw + 1 of each cell, one
+// axis at a time between `in` and `tmp`; returns the buffer holding it.
+static unsigned* dilate_cells(Ctx* c, unsigned* in, unsigned* tmp, cudaStream_t st) {
+  const int nb = (c->key_cells + 255) / 256;
+  for (int a = 0; a < c->P.dim; a++) {
+    k_dilate<<<nb, 256, 0, st>>>(c->key_cells, c->n_inst, c->d_grids, a, in, tmp);
+    unsigned* t = in;
+    in = tmp;
+    tmp = t;
+  }
+  c->launches += c->P.dim;
+  return in;
+}
+
+template <int DIM>
+static void build_lists_dim(Ctx* c, const MhdState* s, int n, cudaStream_t st, const Ctx::ListSlot* O,
+                            Ctx::ListSlot& S) {
+  const float grow = (float)(1.0 + c->list_margin);
+  const int nb = (n + 127) / 128, nb256 = (n + 255) / 256;
+  const int64_t pad = c->n_pad;
+  const bool full = O == nullptr;
+  int* mark = nullptr;
+  if (!full) cudaMemsetAsync(c->cell_scr[0], 0, sizeof(unsigned) * c->key_cells, st);
+  k_track<DIM><<<nb256, 256, 0, st>>>(n, full ? 1 : 0, c->d_grids, c->inst, c->perm, s->x, s->y, s->z, s->h,
+                                      full ? nullptr : O->xr, full ? nullptr : O->hm, full ? nullptr : O->md, S.xr,
+                                      S.hm, S.md, pad, c->new_of_old, c->cell_scr[0], c->d_sc);
+  c->launches++;
+  if (!full) {
+    unsigned* md_dil = dilate_cells(c, c->cell_scr[0], c->cell_scr[1], st);
+    unsigned* flags = md_dil == c->cell_scr[0] ? c->cell_scr[1] : c->cell_scr[0];
+    cudaMemsetAsync(flags, 0, sizeof(unsigned) * c->key_cells, st);
+    k_mark<<<nb256, 256, 0, st>>>(n, c->P, c->d_grids, c->inst, c->sorted_keys, s->h, c->posf, S.hm, md_dil,
+                                  (double)grow * (1.0 - 1e-4), 1.0 + 0.25 * c->list_margin, c->nbr_hlim,
+                                  c->nbr_mark, flags);
+    unsigned* dirty_dil = dilate_cells(c, flags, md_dil, st);
+    k_remap<<<nb256, 256, 0, st>>>(n, c->list_cap, c->perm, c->sorted_keys, c->new_of_old, dirty_dil, c->nbr_mark,
+                                   s->x, s->y, s->z, s->h, S.xr, S.hm, S.md, pad, O->idx, O->cnt, S.idx, S.cnt,
+                                   S.gcnt, c->d_sc);
+    c->launches += 2;
+    mark = c->nbr_mark;
+  }
+  k_build_lists<DIM><<<nb, 128, 0, st>>>(n, c->P, c->d_grids, c->inst, c->cell_start, s->x, s->y, s->z, s->h,
+                                         c->posf, c->cellc, grow, c->list_cap, S.idx, S.cnt, S.gcnt, c->nbr_hlim,
+                                         c->big_idx, mark, c->d_sc);
+  k_build_lists_big<DIM><<<kScatterBlocks, 128, 0, st>>>(c->P, c->d_grids, c->inst, c->cell_start, s->x, s->y,
+                                                         s->z, s->h, c->posf, c->cellc, grow, c->list_cap, S.idx,
+                                                         S.cnt, S.gcnt, c->nbr_hlim, c->big_idx, c->d_sc);
+  k_scatter_big<DIM><<<kScatterBlocks, 128, 0, st>>>(c->P, c->d_grids, c->inst, c->cell_start, s->x, s->y, s->z,
+                                                     c->posf, c->cellc, grow, c->list_cap, S.idx, S.cnt,
+                                                     c->big_idx, mark, S.gcnt, c->d_sc);
+  k_sort_appended<<<nb, 128, 0, st>>>(n, c->list_cap, S.idx, S.cnt, S.gcnt);
+  c->launches += 4;
+}
+
+void launch_build_lists(Ctx* c, const MhdState* s, int n, cudaStream_t st, const MhdState* src) {
   if (n <= 0) return;
   TimedScope ts(c, MHD_TIMING_LISTS, st);
-  const float grow = (float)(1.0 + c->list_margin);
-  cudaMemsetAsync(&c->d_sc->n_big, 0, sizeof(int), st);
-  const int nb = (n + 127) / 128;
-  if (c->P.dim == 3) {
-    k_build_lists<3><<<nb, 128, 0, st>>>(n, c->P, c->d_grids, c->inst, c->cell_start, s->x, s->y, s->z, s->h,
-                                         c->posf, c->cellc, grow, c->list_cap, c->nbr_idx, c->nbr_cnt, c->nbr_gcnt,
-                                         c->nbr_hlim, c->big_idx, c->d_sc);
-    k_build_lists_big<3><<<kScatterBlocks, 128, 0, st>>>(c->P, c->d_grids, c->inst, c->cell_start, s->x, s->y,
-                                                         s->z, s->h, c->posf, c->cellc, grow, c->list_cap,
-                                                         c->nbr_idx, c->nbr_cnt, c->nbr_gcnt, c->nbr_hlim,
-                                                         c->big_idx, c->d_sc);
-    k_scatter_big<3><<<kScatterBlocks, 128, 0, st>>>(c->P, c->d_grids, c->inst, c->cell_start, s->x, s->y, s->z,
-                                                     c->posf, c->cellc, grow, c->list_cap, c->nbr_idx, c->nbr_cnt,
-                                                     c->big_idx, c->d_sc);
-  } else {
-    k_build_lists<2><<<nb, 128, 0, st>>>(n, c->P, c->d_grids, c->inst, c->cell_start, s->x, s->y, s->z, s->h,
-                                         c->posf, c->cellc, grow, c->list_cap, c->nbr_idx, c->nbr_cnt, c->nbr_gcnt,
-                                         c->nbr_hlim, c->big_idx, c->d_sc);
-    k_build_lists_big<2><<<kScatterBlocks, 128, 0, st>>>(c->P, c->d_grids, c->inst, c->cell_start, s->x, s->y,
-                                                         s->z, s->h, c->posf, c->cellc, grow, c->list_cap,
-                                                         c->nbr_idx, c->nbr_cnt, c->nbr_gcnt, c->nbr_hlim,
-                                                         c->big_idx, c->d_sc);
-    k_scatter_big<2><<<kScatterBlocks, 128, 0, st>>>(c->P, c->d_grids, c->inst, c->cell_start, s->x, s->y, s->z,
-                                                     c->posf, c->cellc, grow, c->list_cap, c->nbr_idx, c->nbr_cnt,
-                                                     c->big_idx, c->d_sc);
+  // the slot of s (or the least recently used one not holding src's lists)
+  int nw = -1, od = -1;
+  for (int k = 0; k < 2; k++) {
+    if (c->slots[k].key == s->x) nw = k;
+    if (src && c->slots[k].key == src->x) od = k;
   }
-  k_sort_appended<<<nb, 128, 0, st>>>(n, c->list_cap, c->nbr_idx, c->nbr_cnt, c->nbr_gcnt);
-  c->launches += 4;
+  if (nw < 0 || nw == od) nw = od >= 0 ? 1 - od : (c->slots[0].use <= c->slots[1].use ? 0 : 1);
+  const bool carry = c->list_reuse && od >= 0 && c->slots[od].n == n && c->slots[od].layout == c->layout_gen;
+  Ctx::ListSlot& S = c->slots[nw];
+  S.key = nullptr;
+  c->nbr_idx = S.idx;
+  c->nbr_cnt = S.cnt;
+  c->nbr_gcnt = S.gcnt;
+  cudaMemsetAsync(&c->d_sc->n_big, 0, sizeof(int), st);
+  if (c->P.dim == 3)
+    build_lists_dim<3>(c, s, n, st, carry ? &c->slots[od] : nullptr, S);
+  else
+    build_lists_dim<2>(c, s, n, st, carry ? &c->slots[od] : nullptr, S);
+  S.key = s->x;
+  S.n = n;
+  S.layout = c->layout_gen;
+  S.use = ++c->slot_clock;
 }
 
 // ------------------------------------------------------------- dispatch

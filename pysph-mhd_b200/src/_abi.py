@@ -83,7 +83,7 @@ EXPORTS = (
     "mhd_launch_count", "mhd_cells_build", "mhd_density_iterate", "mhd_force_pass", "mhd_rhs", "mhd_timestep",
     "mhd_clock_set", "mhd_clock_get", "mhd_step_initialize", "mhd_step_stage1", "mhd_step_stage2",
     "mhd_corrector_predictor", "mhd_step", "mhd_timing_enable", "mhd_timing_read", "mhd_probe_fma_peak",
-    "mhd_pair_counts", "mhd_timestep_noalloc", "mhd_neighbour_counts", "mhd_ctx_set_instances",
+    "mhd_pair_counts", "mhd_list_counts", "mhd_timestep_noalloc", "mhd_neighbour_counts", "mhd_ctx_set_instances",
     "mhd_instance_count", "mhd_clock_set_all", "mhd_clock_get_all", "mhd_advance", "mhd_ctx_tune",
     "mhd_tangent_dirs", "mhd_tangent_sync", "mhd_tangent_rhs", "mhd_tangent_step", "mhd_tangent_magnetic_energy",
     "mhd_adjoint_field_count", "mhd_adjoint_field_name", "mhd_adjoint_forward", "mhd_adjoint_backward",
@@ -134,6 +134,7 @@ def load(path: str = LIB_PATH):
     lib.mhd_timing_read.argtypes = [vp, ctypes.POINTER(dbl), ctypes.POINTER(i64)]
     lib.mhd_probe_fma_peak.argtypes = [i32, ctypes.POINTER(dbl), vp]
     lib.mhd_pair_counts.argtypes = [vp, ctypes.POINTER(i64), ctypes.POINTER(i64), vp]
+    lib.mhd_list_counts.argtypes = [vp, ctypes.POINTER(i64), ctypes.POINTER(i64), vp]
     lib.mhd_timestep_noalloc.argtypes = [vp, i64, dbl, dbl, vp, vp]
     lib.mhd_neighbour_counts.argtypes = [vp, sp, i64, vp, vp]
     lib.mhd_ctx_set_instances.argtypes = [vp, sp, i32, ctypes.POINTER(i64), dbl, vp]
