@@ -275,6 +275,13 @@ def _timed(args, prec, dev, barrier, dist, world):
     lib.mhd_timing_read(eng.ctx, ms_k, cnt_k)
     lib.mhd_pair_counts(eng.ctx, ctypes.byref(pairs), ctypes.byref(cands), st)
     lib.mhd_timing_enable(eng.ctx, 0)
+    if args.profile_steps > 0:
+        # steady-state steps bracketed for a profiler started with
+        # --profile-from-start off (outside every timed region)
+        torch.cuda.profiler.start()
+        eng.advance(args.profile_steps, finish=False, capture=False)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
     eng.rhs()
     passes = int(eng.last_stats.density_passes)
     eng.close()
@@ -721,6 +728,8 @@ def main():
                     help="form timed as the headline value (the FP64 path is timed beside it)")
     ap.add_argument("--accuracy-steps", type=int, default=100)
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--profile-steps", type=int, default=0,
+                    help="uncaptured steps run between cudaProfilerStart/Stop after the timing (0: none)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-instances", type=int, default=64, help="batched form instances (0 skips it)")
     ap.add_argument("--batch-steps", type=int, default=100)

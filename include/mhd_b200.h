@@ -157,8 +157,9 @@ int mhd_timing_read(void* ctx, double* ms, int64_t* launches);
    pipe on the current device: the compute roof of the pair passes. */
 int mhd_probe_fma_peak(int32_t precision, double* flops_per_second, void* stream);
 
-/* Neighbour pairs (self included) and distance tests of all force passes
-   since the previous call (synchronises, then resets). */
+/* Neighbour pairs (self included) and distance tests of the force passes
+   run with timing enabled (mhd_timing_enable) since the previous call
+   (synchronises, then resets). */
 int mhd_pair_counts(void* ctx, int64_t* pairs, int64_t* candidates, void* stream);
 
 /* Particles whose neighbour lists were built or carried over across a sort

@@ -135,7 +135,7 @@ constexpr int kForceShapeCount = 4;
 
 template <int K, int DIM, class T, int SHAPE>
 __global__ void __launch_bounds__(kForceShapes[SHAPE][0], kForceShapes[SHAPE][1])
-    k_force_pass(int n, DevParams P, NbrList L, ForceRecords<T> R, ForceOut<T> o, DevScalars* sc) {
+    k_force_pass(int n, DevParams P, NbrList L, ForceRecords<T> R, ForceOut<T> o, DevScalars* sc, int count) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const Grid& G = grid_of(R.grids, R.inst, i);
@@ -176,6 +176,14 @@ __global__ void __launch_bounds__(kForceShapes[SHAPE][0], kForceShapes[SHAPE][1]
   for (int k = 0; k < cnt; k++) {
     const int j = row[k * 32];
     ncand++;
+    if (j == i) {
+      // the self pair: every sum term carries a zero kernel gradient or a
+      // zero displacement; only the signal speed max(vw_i - 2 dot, 0) = vw_i
+      // enters dt_cfl
+      npair++;
+      dtc = fmax(dtc, vwi);
+      continue;
+    }
     T dx, dy, dz, r, inv_r0;
     if constexpr (sizeof(T) == 4) {
       // FP32 geometry from the packed positions; FP32 neighbour test
@@ -235,7 +243,10 @@ __global__ void __launch_bounds__(kForceShapes[SHAPE][0], kForceShapes[SHAPE][1]
       vzx += dvz * cx; vzy += dvz * cy;
       axx += dax * cx; ayy += day * cy;
     }
-    // ---- MHDAccelerations.loop (r-hat is zero below 1e-8 here)
+    // ---- MHDAccelerations.loop (r-hat is zero below 1e-8 here); its
+    // momentum and energy terms join the magnetic ones below in one
+    // compensated add per sum
+    T mf, fei;
     {
       const bool far = r >= (T)kInteractionDistanceEpsilon;
       const T dot = far ? vdotx * inv_r : zero;
@@ -250,7 +261,7 @@ __global__ void __launch_bounds__(kForceShapes[SHAPE][0], kForceShapes[SHAPE][1]
       c = fmax(c, zero);
       dtc = fmax(dtc, c);
       T fcoef = PI * ti + j1.x * tj;
-      T fei = mj * PI * ti * vdotx;
+      fei = mj * PI * ti * vdotx;
       if (dot < zero) {
         const T vsigav_i = fmax(AI - two * dot, zero);
         const T vsigav_j = fmax(j1.y - two * dot, zero);
@@ -259,13 +270,9 @@ __global__ void __launch_bounds__(kForceShapes[SHAPE][0], kForceShapes[SHAPE][1]
         fcoef += qi * omegai * ti + qj * omegaj * tj;
         fei += mj * qi * dot * grad_i;
       }
-      const T mf = mj * fcoef;
-      fx.add(-mf * dx);
-      fy.add(-mf * dy);
-      fz.add(-mf * dz);
+      mf = mj * fcoef;
       const T eij = epi - j2.w;
       fei += ac * vsig2 * eij * (half * mj * (irhoi * grad_i + irhoj * grad_j));
-      fe.add(fei);
     }
     // ---- MagneticStressAccelerations.loop and MagneticStateRates.loop
     {
@@ -291,13 +298,13 @@ __global__ void __launch_bounds__(kForceShapes[SHAPE][0], kForceShapes[SHAPE][1]
       const T vsig_b = fast_sqrt(tx * tx + ty * ty + tz * tz);
       const T diss = half * (pmi + pmj) * vsig_b * ar;
       const T dpsi = pmi * psichi + pmj * j4.w;
-      fx.add(-rux * gradp + ms * (brxi * si + j5.x * sj));
-      fy.add(-ruy * gradp + ms * (bryi * si + j5.y * sj));
-      fz.add(-ruz * gradp + ms * (brzi * si + j5.z * sj));
+      fx.add(-mf * dx + (-rux * gradp + ms * (brxi * si + j5.x * sj)));
+      fy.add(-mf * dy + (-ruy * gradp + ms * (bryi * si + j5.y * sj)));
+      fz.add(-mf * dz + (-ruz * gradp + ms * (brzi * si + j5.z * sj)));
       bxr.add(d_brho * dvx + diss * dbx - dpsi * rux);
       byr.add(d_brho * dvy + diss * dby - dpsi * ruy);
       bzr.add(d_brho * dvz + diss * dbz - dpsi * ruz);
-      fe.add(-half * delta_b2 * diss * inv_mu0);
+      fe.add(fei + (-half * delta_b2 * diss * inv_mu0));
       dbs.add(pmi * proj_bi + pmj * proj_bj);
       dbd.add(-mj * proj_db * grad_i);
     }
@@ -416,11 +423,13 @@ __global__ void __launch_bounds__(kForceShapes[SHAPE][0], kForceShapes[SHAPE][1]
   o.apsi[i] = apsi;
   o.divBsymm[i] = rhoi_d * dbsv;
   o.divBdiff[i] = dbdv;
-  const unsigned mask = __activemask();
-  const unsigned sp = __reduce_add_sync(mask, npair), sc_ = __reduce_add_sync(mask, ncand);
-  if ((int)(threadIdx.x & 31) == __ffs(mask) - 1) {
-    atomicAdd(&sc->n_pairs, (unsigned long long)sp);
-    atomicAdd(&sc->n_candidates, (unsigned long long)sc_);
+  if (count) {
+    const unsigned mask = __activemask();
+    const unsigned sp = __reduce_add_sync(mask, npair), sc_ = __reduce_add_sync(mask, ncand);
+    if ((int)(threadIdx.x & 31) == __ffs(mask) - 1) {
+      atomicAdd(&sc->n_pairs, (unsigned long long)sp);
+      atomicAdd(&sc->n_candidates, (unsigned long long)sc_);
+    }
   }
   (void)rhoi;
 }
@@ -468,11 +477,12 @@ static void force_launch_t(Ctx* c, const ForceOut<T>& o, int n, cudaStream_t st)
   const int s = c->force_shape >= 0 ? c->force_shape : (sizeof(T) == 4 ? 2 : 0);
   const int bs = kForceShapes[s][0];
   const int grid = (n + bs - 1) / bs;
+  const int cnt = c->timing ? 1 : 0;  // pair counters only while timing
   switch (s) {
-    case 1: k_force_pass<K, DIM, T, 1><<<grid, bs, 0, st>>>(n, c->P, c->lists(), records<T>(c), o, c->d_sc); break;
-    case 2: k_force_pass<K, DIM, T, 2><<<grid, bs, 0, st>>>(n, c->P, c->lists(), records<T>(c), o, c->d_sc); break;
-    case 3: k_force_pass<K, DIM, T, 3><<<grid, bs, 0, st>>>(n, c->P, c->lists(), records<T>(c), o, c->d_sc); break;
-    default: k_force_pass<K, DIM, T, 0><<<grid, bs, 0, st>>>(n, c->P, c->lists(), records<T>(c), o, c->d_sc);
+    case 1: k_force_pass<K, DIM, T, 1><<<grid, bs, 0, st>>>(n, c->P, c->lists(), records<T>(c), o, c->d_sc, cnt); break;
+    case 2: k_force_pass<K, DIM, T, 2><<<grid, bs, 0, st>>>(n, c->P, c->lists(), records<T>(c), o, c->d_sc, cnt); break;
+    case 3: k_force_pass<K, DIM, T, 3><<<grid, bs, 0, st>>>(n, c->P, c->lists(), records<T>(c), o, c->d_sc, cnt); break;
+    default: k_force_pass<K, DIM, T, 0><<<grid, bs, 0, st>>>(n, c->P, c->lists(), records<T>(c), o, c->d_sc, cnt);
   }
 }
 

@@ -476,13 +476,6 @@ __device__ __forceinline__ int cell_key(const Grid& G, double x, double y, doubl
   return G.cell_base + (cz * G.nc[1] + cy) * G.nc[0] + cx;
 }
 
-// Warp-aggregated add of the active lanes' flags to a device counter.
-__device__ __forceinline__ void count_lanes(unsigned long long* ctr, bool flag) {
-  const unsigned act = __activemask();
-  const unsigned b = __ballot_sync(act, flag);
-  if ((int)(threadIdx.x & 31) == __ffs(act) - 1 && b) atomicAdd(ctr, (unsigned long long)__popc(b));
-}
-
 // Epoch bookkeeping of sorted particle k (source index o = perm[k]): xr, hm
 // and md carried from the old slot and updated; md marked in the cells of x
 // and xr.  With `full` every epoch starts now.
@@ -498,10 +491,12 @@ __global__ void __launch_bounds__(256) k_track(int n, int full, const Grid* __re
                                                DevScalars* sc) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
-  count_lanes(&sc->n_listed, true);
+  if (k == 0) {
+    atomicAdd(&sc->n_listed, (unsigned long long)n);
+    if (full) atomicAdd(&sc->n_rebuilt, (unsigned long long)n);
+  }
   const double xk = x[k], yk = y[k], zk = DIM == 3 ? z[k] : 0.0, hk = h[k];
   if (full) {
-    count_lanes(&sc->n_rebuilt, true);
     xr_new[k] = xk;
     xr_new[pad + k] = yk;
     xr_new[2 * pad + k] = zk;
@@ -606,19 +601,22 @@ __global__ void __launch_bounds__(256) k_remap(int n, int cap, const int* __rest
                                                int* __restrict__ idx_new, int* __restrict__ cnt_new,
                                                int* __restrict__ gcnt_new, DevScalars* sc) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n) return;
-  const int dirty = mark[k];
-  if (dirty) {
-    xr_new[k] = x[k];
-    xr_new[pad + k] = y[k];
-    xr_new[2 * pad + k] = z[k];
-    hm_new[k] = h[k];
-    md_new[k] = 0.f;
+  bool rebuild = false;
+  if (k < n) {
+    const int dirty = mark[k];
+    if (dirty) {
+      xr_new[k] = x[k];
+      xr_new[pad + k] = y[k];
+      xr_new[2 * pad + k] = z[k];
+      hm_new[k] = h[k];
+      md_new[k] = 0.f;
+    }
+    rebuild = dirty || cell_dirty[keys[k]] != 0u;
+    mark[k] = rebuild ? 1 : 0;
   }
-  const bool rebuild = dirty || cell_dirty[keys[k]] != 0u;
-  mark[k] = rebuild ? 1 : 0;
-  count_lanes(&sc->n_rebuilt, rebuild);
-  if (rebuild) return;
+  const int nr = __syncthreads_count(rebuild);
+  if (threadIdx.x == 0 && nr) atomicAdd(&sc->n_rebuilt, (unsigned long long)nr);
+  if (k >= n || rebuild) return;
   const int o = perm[k];
   int c = cnt_old[o];
   c = c < cap ? c : cap;
