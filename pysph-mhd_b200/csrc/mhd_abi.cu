@@ -110,6 +110,12 @@ int fill_params(Ctx* c, const MhdParams* p) {
   P.alpha_max = p->alpha_max;
   P.tf = p->tf;
   P.norm = kernel_norm(p->kernel, p->dim);
+  P.Rf = (float)P.R;
+  P.normf = (float)P.norm;
+  P.avf = (float)P.av;
+  P.acf = (float)P.ac;
+  P.arf = (float)P.ar;
+  P.inv_mu0f = (float)P.inv_mu0;
   P.fp32 = p->precision == MHD_PRECISION_FP32 ? 1 : 0;
   return MHD_OK;
 }

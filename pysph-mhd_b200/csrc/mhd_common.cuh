@@ -73,6 +73,9 @@ struct DevParams {
   double hfact, gamma, gamma1, mu0, inv_mu0, av, ac, ar, clean_speed, clean_damp, clean_active;
   double c_cour, c_force, alpha_min, alpha_max, tf;
   double norm;  // kernel normalisation sigma_d
+  // FP32 copies for the FP32 pair loops (kernel-parameter operands, no
+  // conversion in the kernel)
+  float Rf, normf, avf, acf, arf, inv_mu0f;
 };
 
 // Device-resident scalars of one context (status, pass counters, events).

@@ -62,6 +62,13 @@ struct Acc<float> {
   __device__ __forceinline__ double get() const { return (double)s - (double)c; }
 };
 
+// A kernel parameter in the pair precision: the FP32 copy or the FP64 value.
+template <class T>
+__device__ __forceinline__ T prm_t(float f, double d) {
+  if constexpr (sizeof(T) == 4) return f;
+  else return d;
+}
+
 // FP32: the MUFU approximations (about 2 ulp); FP64: IEEE division and sqrt.
 __device__ __forceinline__ float fast_rcp(float x) { return __fdividef(1.0f, x); }
 __device__ __forceinline__ double fast_rcp(double x) { return 1.0 / x; }
@@ -135,7 +142,7 @@ constexpr int kForceShapeCount = 4;
 
 template <int K, int DIM, class T, int SHAPE>
 __global__ void __launch_bounds__(kForceShapes[SHAPE][0], kForceShapes[SHAPE][1])
-    k_force_pass(int n, DevParams P, NbrList L, ForceRecords<T> R, ForceOut<T> o, DevScalars* sc, int count) {
+    k_force_pass(int n, DevParams P, NbrList L, ForceRecords<T> R, ForceOut<T> o) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const Grid& G = grid_of(R.grids, R.inst, i);
@@ -144,8 +151,8 @@ __global__ void __launch_bounds__(kForceShapes[SHAPE][0], kForceShapes[SHAPE][1]
   const double xi = pi.x, yi = pi.y, zi = DIM == 3 ? pi.z : 0.0, hi = pi.w;
   const double rhi2 = rh2_exact(P.R, hi);
   const T h1i = i3.w;
-  const T faci = (T)P.norm * (DIM == 2 ? h1i * h1i : h1i * h1i * h1i);
-  const T norm = (T)P.norm;
+  const T norm = prm_t<T>(P.normf, P.norm);
+  const T faci = norm * (DIM == 2 ? h1i * h1i : h1i * h1i * h1i);
   const T rhoi = i0.y, irhoi = i0.z, omegai = i0.w;
   const T PI = i1.x, AI = i1.y, vwi = i1.z, p_i = i1.w;
   const T ui = i2.x, vi = i2.y, wi = i2.z, epi = i2.w;
@@ -153,7 +160,8 @@ __global__ void __launch_bounds__(kForceShapes[SHAPE][0], kForceShapes[SHAPE][1]
   const T bxi = i4.x, byi = i4.y, bzi = i4.z, psichi = i4.w;
   const T brxi = i5.x, bryi = i5.y, brzi = i5.z, bro2i = i5.w;
   const T rhoi2inv = irhoi * irhoi;
-  const T av = (T)P.av, ac = (T)P.ac, ar = (T)P.ar, inv_mu0 = (T)P.inv_mu0;
+  const T av = prm_t<T>(P.avf, P.av), ac = prm_t<T>(P.acf, P.ac), ar = prm_t<T>(P.arf, P.ar),
+          inv_mu0 = prm_t<T>(P.inv_mu0f, P.inv_mu0);
   const T two = (T)2, half = (T)0.5, zero = (T)0;
 
   // Cullen-Dehnen moments (src/equations.py:329-354)
@@ -162,7 +170,6 @@ __global__ void __launch_bounds__(kForceShapes[SHAPE][0], kForceShapes[SHAPE][1]
   T axx = 0, axy = 0, axz = 0, ayx = 0, ayy = 0, ayz = 0, azx = 0, azy = 0, azz = 0;
   Acc<T> fx, fy, fz, fe, fdiv, bxr, byr, bzr, dbs, dbd;
   T dtc = 0;
-  unsigned npair = 0, ncand = 0;
 
   const int cnt = L.cnt[i];
   const int* __restrict__ row = L.idx + (size_t)(i >> 5) * L.cap * 32 + (i & 31);
@@ -172,15 +179,13 @@ __global__ void __launch_bounds__(kForceShapes[SHAPE][0], kForceShapes[SHAPE][1]
     pif = R.posf[i];
     cif = R.cellc[i];
   }
-  const float Rf = (float)P.R;
+  const float Rf = P.Rf;
   for (int k = 0; k < cnt; k++) {
     const int j = row[k * 32];
-    ncand++;
     if (j == i) {
       // the self pair: every sum term carries a zero kernel gradient or a
       // zero displacement; only the signal speed max(vw_i - 2 dot, 0) = vw_i
       // enters dt_cfl
-      npair++;
       dtc = fmax(dtc, vwi);
       continue;
     }
@@ -208,7 +213,6 @@ __global__ void __launch_bounds__(kForceShapes[SHAPE][0], kForceShapes[SHAPE][1]
       r = sqrt(r2d);
       inv_r0 = 0;
     }
-    npair++;
     const V4<T> j0 = ld4(R.r[0] + j), j1 = ld4(R.r[1] + j), j2 = ld4(R.r[2] + j), j3 = ld4(R.r[3] + j);
     const V4<T> j4 = ld4(R.r[4] + j), j5 = ld4(R.r[5] + j);
     const T mj = j0.x, rhoj = j0.y, irhoj = j0.z, omegaj = j0.w;
@@ -423,14 +427,6 @@ __global__ void __launch_bounds__(kForceShapes[SHAPE][0], kForceShapes[SHAPE][1]
   o.apsi[i] = apsi;
   o.divBsymm[i] = rhoi_d * dbsv;
   o.divBdiff[i] = dbdv;
-  if (count) {
-    const unsigned mask = __activemask();
-    const unsigned sp = __reduce_add_sync(mask, npair), sc_ = __reduce_add_sync(mask, ncand);
-    if ((int)(threadIdx.x & 31) == __ffs(mask) - 1) {
-      atomicAdd(&sc->n_pairs, (unsigned long long)sp);
-      atomicAdd(&sc->n_candidates, (unsigned long long)sc_);
-    }
-  }
   (void)rhoi;
 }
 
@@ -477,12 +473,11 @@ static void force_launch_t(Ctx* c, const ForceOut<T>& o, int n, cudaStream_t st)
   const int s = c->force_shape >= 0 ? c->force_shape : (sizeof(T) == 4 ? 2 : 0);
   const int bs = kForceShapes[s][0];
   const int grid = (n + bs - 1) / bs;
-  const int cnt = c->timing ? 1 : 0;  // pair counters only while timing
   switch (s) {
-    case 1: k_force_pass<K, DIM, T, 1><<<grid, bs, 0, st>>>(n, c->P, c->lists(), records<T>(c), o, c->d_sc, cnt); break;
-    case 2: k_force_pass<K, DIM, T, 2><<<grid, bs, 0, st>>>(n, c->P, c->lists(), records<T>(c), o, c->d_sc, cnt); break;
-    case 3: k_force_pass<K, DIM, T, 3><<<grid, bs, 0, st>>>(n, c->P, c->lists(), records<T>(c), o, c->d_sc, cnt); break;
-    default: k_force_pass<K, DIM, T, 0><<<grid, bs, 0, st>>>(n, c->P, c->lists(), records<T>(c), o, c->d_sc, cnt);
+    case 1: k_force_pass<K, DIM, T, 1><<<grid, bs, 0, st>>>(n, c->P, c->lists(), records<T>(c), o); break;
+    case 2: k_force_pass<K, DIM, T, 2><<<grid, bs, 0, st>>>(n, c->P, c->lists(), records<T>(c), o); break;
+    case 3: k_force_pass<K, DIM, T, 3><<<grid, bs, 0, st>>>(n, c->P, c->lists(), records<T>(c), o); break;
+    default: k_force_pass<K, DIM, T, 0><<<grid, bs, 0, st>>>(n, c->P, c->lists(), records<T>(c), o);
   }
 }
 
@@ -517,6 +512,7 @@ static void force_launch(Ctx* c, MhdState* s, int n, cudaStream_t st) {
 
 void launch_force_pass(Ctx* c, MhdState* s, int n, cudaStream_t st) {
   if (n <= 0) return;
+  if (c->timing) launch_pair_stats(c, s, n, st);  // outside the timed scope
   TimedScope ts(c, MHD_TIMING_FORCE, st);
   const int d3 = c->P.dim == 3;
   switch (c->P.kernel) {

@@ -197,6 +197,9 @@ void launch_plan_grids(Ctx* c, cudaStream_t st);
 void launch_build_lists(Ctx* c, const MhdState* s, int n, cudaStream_t st, const MhdState* src);
 void launch_pack_positions(Ctx* c, const MhdState* s, int n, cudaStream_t st);
 void launch_neighbour_counts(Ctx* c, const MhdState* s, int n, int* out, cudaStream_t st);
+// adds the exact-rule neighbour pairs and the list entries of the current
+// lists to DevScalars::n_pairs / n_candidates (the force pass's pair counts)
+void launch_pair_stats(Ctx* c, const MhdState* s, int n, cudaStream_t st);
 // density pass `pass` (0-based) reading h_in, writing h_out
 void launch_density_pass(Ctx* c, MhdState* s, int n, int pass, const double* h_in, double* h_out, cudaStream_t st);
 void launch_finish_density(Ctx* c, MhdState* s, int n, int passes, cudaStream_t st);

@@ -654,6 +654,54 @@ __global__ void __launch_bounds__(128) k_neighbour_counts(int n, DevParams P, co
   out[i] = nb;
 }
 
+// Pairs under the exact rule and list entries, summed over the particles
+// (one atomic pair per block).
+template <int DIM>
+__global__ void __launch_bounds__(256) k_pair_stats(int n, DevParams P, const Grid* __restrict__ grids,
+                                                    const int* __restrict__ inst, NbrList L,
+                                                    const double* __restrict__ x, const double* __restrict__ y,
+                                                    const double* __restrict__ z, const double* __restrict__ h,
+                                                    DevScalars* sc) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned nb = 0, cnt = 0;
+  if (i < n) {
+    const Grid& G = grid_of(grids, inst, i);
+    const double xi = x[i], yi = y[i], zi = DIM == 3 ? z[i] : 0.0;
+    const double rhi2 = rh2_exact(P.R, h[i]);
+    cnt = (unsigned)L.cnt[i];
+    const int* __restrict__ row = L.idx + (size_t)(i >> 5) * L.cap * 32 + (i & 31);
+    for (unsigned k = 0; k < cnt; k++) {
+      const int j = row[(size_t)k * 32];
+      const double dx = min_image(xi - x[j], G.L[0], G.half[0], G.periodic[0]);
+      const double dy = min_image(yi - y[j], G.L[1], G.half[1], G.periodic[1]);
+      const double dz = DIM == 3 ? min_image(zi - z[j], G.L[2], G.half[2], G.periodic[2]) : 0.0;
+      const double r2 = r2_exact(dx, dy, dz);
+      nb += (r2 < rhi2 || r2 < rh2_exact(P.R, h[j])) ? 1u : 0u;
+    }
+  }
+  __shared__ unsigned long long acc[2];
+  if (threadIdx.x == 0) acc[0] = acc[1] = 0ULL;
+  __syncthreads();
+  atomicAdd(&acc[0], (unsigned long long)nb);
+  atomicAdd(&acc[1], (unsigned long long)cnt);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    atomicAdd(&sc->n_pairs, acc[0]);
+    atomicAdd(&sc->n_candidates, acc[1]);
+  }
+}
+
+void launch_pair_stats(Ctx* c, const MhdState* s, int n, cudaStream_t st) {
+  if (n <= 0) return;
+  if (c->P.dim == 3)
+    k_pair_stats<3><<<(n + 255) / 256, 256, 0, st>>>(n, c->P, c->d_grids, c->inst, c->lists(), s->x, s->y, s->z,
+                                                     s->h, c->d_sc);
+  else
+    k_pair_stats<2><<<(n + 255) / 256, 256, 0, st>>>(n, c->P, c->d_grids, c->inst, c->lists(), s->x, s->y, s->z,
+                                                     s->h, c->d_sc);
+  c->launches++;
+}
+
 void launch_neighbour_counts(Ctx* c, const MhdState* s, int n, int* out, cudaStream_t st) {
   if (n <= 0) return;
   if (c->P.dim == 3)
