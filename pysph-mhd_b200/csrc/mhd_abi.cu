@@ -618,6 +618,10 @@ int mhd_ctx_create(const MhdParams* params, int64_t n_max, void** out) {
   Ctx* c = new Ctx();
   c->device = dev;
   c->n_max = n_max;
+  {
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && sms > 0) c->num_sms = sms;
+  }
   int rc = fill_params(c, params);
   if (rc != MHD_OK) {
     g_err = c->err;
@@ -643,7 +647,8 @@ int mhd_ctx_create(const MhdParams* params, int64_t n_max, void** out) {
     const double rr = radius_scale_of(params->kernel) * params->hfact * (1.0 + c->list_margin);
     const double vol = params->dim == 3 ? 4.0 / 3.0 * M_PI * rr * rr * rr : M_PI * rr * rr;
     const int cap = ((int)(1.5 * vol) + 16 + 7) & ~7;
-    ok = ok && dev_alloc(c, &c->posf, c->n_pad) == MHD_OK && dev_alloc(c, &c->cellc, c->n_pad) == MHD_OK;
+    ok = ok && dev_alloc(c, &c->posf, c->n_pad) == MHD_OK && dev_alloc(c, &c->posm, c->n_pad) == MHD_OK &&
+         dev_alloc(c, &c->cellc, c->n_pad) == MHD_OK;
     ok = ok && dev_alloc(c, &c->nbr_hlim, c->n_pad) == MHD_OK && dev_alloc(c, &c->big_idx, c->n_pad) == MHD_OK &&
          dev_alloc(c, &c->new_of_old, c->n_pad) == MHD_OK && dev_alloc(c, &c->nbr_mark, c->n_pad) == MHD_OK;
     for (Ctx::ListSlot& S : c->slots)
@@ -696,6 +701,7 @@ int mhd_ctx_destroy(void* ctx) {
   cudaFree(c->rec_pos);
   for (void* p : c->rec) cudaFree(p);
   cudaFree(c->posf);
+  cudaFree(c->posm);
   cudaFree(c->cellc);
   for (Ctx::ListSlot& S : c->slots) {
     cudaFree(S.idx);

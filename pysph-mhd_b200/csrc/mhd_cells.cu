@@ -365,14 +365,16 @@ __global__ void __launch_bounds__(256) k_cell_starts(int n, int ncells, const ui
 
 // ------------------------------------------------------- packed positions
 // FP32 position relative to the particle's cell origin (|error| <= 2^-24
-// cell widths) plus h, and the cell coordinates packed into one int: the
+// cell widths) plus h (posf) or plus m (posm, the density pass's record),
+// and the cell coordinates packed into one int: the
 // FP32 geometry of a pair is (pos_i - pos_j) + (cell_i - cell_j) * cell width.
 template <int DIM>
 __global__ void __launch_bounds__(256) k_pack_positions(int n, const Grid* __restrict__ grids,
                                                         const int* __restrict__ inst, const double* __restrict__ x,
                                                         const double* __restrict__ y, const double* __restrict__ z,
-                                                        const double* __restrict__ h, float4* __restrict__ posf,
-                                                        int* __restrict__ cellc) {
+                                                        const double* __restrict__ h,
+                                                        const double* __restrict__ m, float4* __restrict__ posf,
+                                                        float4* __restrict__ posm, int* __restrict__ cellc) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const Grid& g = grid_of(grids, inst, i);
@@ -383,17 +385,18 @@ __global__ void __launch_bounds__(256) k_pack_positions(int n, const Grid* __res
   const float ry = (float)(y[i] - (g.lo[1] + cy * g.cs[1]));
   const float rz = DIM == 3 ? (float)(z[i] - (g.lo[2] + cz * g.cs[2])) : 0.f;
   posf[i] = make_float4(rx, ry, rz, (float)h[i]);
+  posm[i] = make_float4(rx, ry, rz, (float)m[i]);
   cellc[i] = pack_cell<DIM>(cx, cy, cz);
 }
 
 void launch_pack_positions(Ctx* c, const MhdState* s, int n, cudaStream_t st) {
   if (n <= 0) return;
   if (c->P.dim == 3)
-    k_pack_positions<3><<<(n + 255) / 256, 256, 0, st>>>(n, c->d_grids, c->inst, s->x, s->y, s->z, s->h, c->posf,
-                                                         c->cellc);
+    k_pack_positions<3><<<(n + 255) / 256, 256, 0, st>>>(n, c->d_grids, c->inst, s->x, s->y, s->z, s->h, s->m,
+                                                         c->posf, c->posm, c->cellc);
   else
-    k_pack_positions<2><<<(n + 255) / 256, 256, 0, st>>>(n, c->d_grids, c->inst, s->x, s->y, s->z, s->h, c->posf,
-                                                         c->cellc);
+    k_pack_positions<2><<<(n + 255) / 256, 256, 0, st>>>(n, c->d_grids, c->inst, s->x, s->y, s->z, s->h, s->m,
+                                                         c->posf, c->posm, c->cellc);
   c->launches++;
 }
 

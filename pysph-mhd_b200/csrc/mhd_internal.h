@@ -94,7 +94,9 @@ struct Ctx {
   // packed FP32 positions relative to the cell origin, and packed cell
   // coordinates, of the sorted particles (written after every sort)
   float4* posf = nullptr;
+  float4* posm = nullptr;  // {x, y, z relative to the cell, m}: the FP32 density pass
   int* cellc = nullptr;
+  int num_sms = 148;       // multiprocessors of the context's device
   int stencil = 2;       // cells are >= list cut-off / stencil wide
   int force_shape = -1;  // launch-shape variant of the force pass (kForceShapes); -1 = per-precision default
   double list_cut = 0;   // R * h_max * (1 + list_margin) of the current grid

@@ -42,32 +42,23 @@ struct SumT<float> {
 };
 
 // ------------------------------------------------------------ density pass
+// One particle of a density pass; returns whether it is still unconverged.
 template <int K, int DIM, class T>
-__global__ void __launch_bounds__(128) k_density_pass(int n, int pass, DevParams P, NbrList L,
-                                                      const double* __restrict__ x, const double* __restrict__ y,
-                                                      const double* __restrict__ z, const double* __restrict__ m,
-                                                      const double* __restrict__ h_in, double* __restrict__ h_out,
-                                                      const double* __restrict__ h0, double* __restrict__ rho_sum,
-                                                      double* __restrict__ omega, double* __restrict__ converged,
-                                                      const Grid* __restrict__ grids, const int* __restrict__ inst,
-                                                      const float4* __restrict__ posf,
-                                                      const int* __restrict__ cellc, DevScalars* sc) {
-  // Stop when the iterated group already stopped after pass `pass` (1-based
-  // count), or when the neighbour lists no longer cover the current h.
-  if (sc->relist) return;
-  if (pass > 0) {
-    const bool stop = !P.iterate || pass >= P.max_iter || (pass >= P.min_iter && sc->n_unconverged[pass - 1] == 0);
-    if (stop) return;
-  }
-  if (blockIdx.x == 0 && threadIdx.x == 0) atomicMax(&sc->passes_done, pass + 1);
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+__device__ __forceinline__ bool density_particle(int i, const DevParams& P, const NbrList& L,
+                                                 const double* __restrict__ x, const double* __restrict__ y,
+                                                 const double* __restrict__ z, const double* __restrict__ m,
+                                                 const double* __restrict__ h_in, double* __restrict__ h_out,
+                                                 const double* __restrict__ h0, double* __restrict__ rho_sum,
+                                                 double* __restrict__ omega, double* __restrict__ converged,
+                                                 const Grid* __restrict__ grids, const int* __restrict__ inst,
+                                                 const float4* __restrict__ posm, const int* __restrict__ cellc,
+                                                 DevScalars* sc) {
   const double hi = h_in[i];
   if (converged[i] == 1.0) {
     // Already finalised: its h is frozen; a re-summation would only refresh
     // the unconsumed rho_sum diagnostic (src/equations.py:117).
     h_out[i] = hi;
-    return;
+    return false;
   }
   const Grid& G = grid_of(grids, inst, i);
   const double xi = x[i], yi = y[i], zi = DIM == 3 ? z[i] : 0.0;
@@ -79,23 +70,26 @@ __global__ void __launch_bounds__(128) k_density_pass(int n, int pass, DevParams
   SumT<T> rs, ds;
   const int cnt = L.cnt[i];
   const int* __restrict__ row = L.idx + (size_t)(i >> 5) * L.cap * 32 + (i & 31);
-  // FP32 form: geometry from the packed positions; FP64: exact geometry.
+  // FP32 form: geometry and mass from the packed {x, y, z, m} records;
+  // FP64: exact geometry.
   float4 pif = make_float4(0.f, 0.f, 0.f, 0.f);
   int cif = 0;
   float rhi2f = 0.f;
   if constexpr (sizeof(T) == 4) {
-    pif = posf[i];
+    pif = posm[i];
     cif = cellc[i];
     const float rh = (float)P.R * (float)hi;
     rhi2f = rh * rh;
   }
   for (int k = 0; k < cnt; k++) {
     const int j = row[k * 32];
-    T r;
+    T r, mj;
     bool nb;
     if constexpr (sizeof(T) == 4) {
       float dx, dy, dz;
-      rel_dx<DIM>(G, pif, cif, __ldg(posf + j), __ldg(cellc + j), dx, dy, dz);
+      const float4 pj = __ldg(posm + j);
+      mj = pj.w;
+      rel_dx<DIM>(G, pif, cif, pj, __ldg(cellc + j), dx, dy, dz);
       const float r2 = dx * dx + dy * dy + dz * dz;
       nb = r2 < rhi2f;
       if (!compact && !nb) {
@@ -118,7 +112,7 @@ __global__ void __launch_bounds__(128) k_density_pass(int n, int pass, DevParams
       const T q = r * h1;
       T w, dw;
       w_dw<K>(q, DIM, w, dw);
-      const T mj = (T)m[j];
+      if constexpr (sizeof(T) == 8) mj = m[j];
       rs.add(mj * (w * fac));
       ds.add(mj * (fgh * (dw * q + w * (T)DIM)));
     }
@@ -141,7 +135,6 @@ __global__ void __launch_bounds__(128) k_density_pass(int n, int pass, DevParams
   if (!finalize) {
     hout = hnew;
     converged[i] = 0.0;
-    atomicAdd(&sc->n_unconverged[pass], 1);
   } else {
     hout = P.hfact * pow(mi / rsum, 1.0 / (double)DIM);
     converged[i] = 1.0;
@@ -151,6 +144,36 @@ __global__ void __launch_bounds__(128) k_density_pass(int n, int pass, DevParams
   // The lists hold every j within R * max(h_i, h_j) of the h they were built
   // with, enlarged by the list margin; a larger h needs new lists.
   if (!(hout <= L.hlim[i])) atomicExch(&sc->relist, 1);
+  return !finalize;
+}
+
+// A density pass over all particles (a pass after the group stopped
+// returns at once).
+template <int K, int DIM, class T>
+__global__ void __launch_bounds__(128) k_density_pass(int n, int pass, DevParams P, NbrList L,
+                                                      const double* __restrict__ x, const double* __restrict__ y,
+                                                      const double* __restrict__ z, const double* __restrict__ m,
+                                                      const double* __restrict__ h_in, double* __restrict__ h_out,
+                                                      const double* __restrict__ h0, double* __restrict__ rho_sum,
+                                                      double* __restrict__ omega, double* __restrict__ converged,
+                                                      const Grid* __restrict__ grids, const int* __restrict__ inst,
+                                                      const float4* __restrict__ posm,
+                                                      const int* __restrict__ cellc, DevScalars* sc) {
+  // Stop when the iterated group already stopped after pass `pass` (1-based
+  // count), or when the neighbour lists no longer cover the current h.
+  if (sc->relist) return;
+  if (pass > 0) {
+    const bool stop = !P.iterate || pass >= P.max_iter || (pass >= P.min_iter && sc->n_unconverged[pass - 1] == 0);
+    if (stop) return;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicMax(&sc->passes_done, pass + 1);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const bool unconv = density_particle<K, DIM, T>(i, P, L, x, y, z, m, h_in, h_out, h0, rho_sum, omega, converged,
+                                                  grids, inst, posm, cellc, sc);
+  const unsigned act = __activemask();
+  const unsigned b = __ballot_sync(act, unconv);
+  if (b && (int)(threadIdx.x & 31) == __ffs(act) - 1) atomicAdd(&sc->n_unconverged[pass], __popc(b));
 }
 
 // ------------------------------------------------------- neighbour lists
@@ -797,15 +820,16 @@ void launch_build_lists(Ctx* c, const MhdState* s, int n, cudaStream_t st, const
 // ------------------------------------------------------------- dispatch
 template <int K, int DIM>
 static void density_launch(Ctx* c, MhdState* s, int n, int pass, const double* h_in, double* h_out, cudaStream_t st) {
+  const int grid = (n + 127) / 128;
   if (c->P.fp32) {
-    k_density_pass<K, DIM, float><<<(n + 127) / 128, 128, 0, st>>>(n, pass, c->P, c->lists(), s->x, s->y, s->z, s->m,
-                                                                   h_in, h_out, s->h0, s->rho_sum, s->omega,
-                                                                   s->converged, c->d_grids, c->inst, c->posf, c->cellc, c->d_sc);
+    k_density_pass<K, DIM, float><<<grid, 128, 0, st>>>(n, pass, c->P, c->lists(), s->x, s->y, s->z, s->m, h_in, h_out,
+                                                        s->h0, s->rho_sum, s->omega, s->converged, c->d_grids, c->inst,
+                                                        c->posm, c->cellc, c->d_sc);
     return;
   }
-  k_density_pass<K, DIM, double><<<(n + 127) / 128, 128, 0, st>>>(n, pass, c->P, c->lists(), s->x, s->y, s->z, s->m,
-                                                                  h_in, h_out, s->h0, s->rho_sum, s->omega,
-                                                                  s->converged, c->d_grids, c->inst, c->posf, c->cellc, c->d_sc);
+  k_density_pass<K, DIM, double><<<grid, 128, 0, st>>>(n, pass, c->P, c->lists(), s->x, s->y, s->z, s->m, h_in, h_out,
+                                                       s->h0, s->rho_sum, s->omega, s->converged, c->d_grids, c->inst,
+                                                       c->posm, c->cellc, c->d_sc);
 }
 
 #define MHD_DISPATCH(FN, ...)                                                   \
