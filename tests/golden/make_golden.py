@@ -24,7 +24,10 @@ Cases (all tiny, pure-Python loops):
 * ``shock2d`` -- 2-D Brio-Wu tube, 16x24 left / 6x8 right lattice, frozen
   ``itype=3`` ends, quintic, hfact 1.0, gamma 2, 3 steps;
 * ``blast3d`` -- 3-D MHD blast on an 8^3 cubic lattice, cubic kernel,
-  hfact 1.2, gamma 5/3, 3 steps.
+  hfact 1.2, gamma 5/3, 3 steps;
+* ``ref_ics`` -- the initial particles the reference's sine, wave, rotor,
+  vortex, current-loop and jet generators build from its own TOML files at a
+  small nx (no stepping).
 """
 
 from __future__ import annotations
@@ -275,7 +278,42 @@ def case_lattice(ref, out):
     out["n_sets"] = np.array(len(setups))
 
 
+IC_FIELDS = "x y z u v w rho h m e Bx By Bz alpha1".split()
+# the reference's remaining case generators at small nx: (config, module, class, nx)
+IC_CASES = [
+    ("mhdsine", "mhdsine", "MHDSine", 12),
+    ("mhdwave", "mhdwave", "MHDWave", 16),
+    ("mhdrotor", "mhdrotor", "MHDRotor", 16),
+    ("mhdvortex", "mhdvortex", "MHDVortex", 12),
+    ("jadvect", "jadvect", "CurrentLoopAdvection", 12),
+    ("1jet", "jet", "JMXJets", 6),
+    ("3jet", "jet", "JMXJets", 5),
+    ("12jet", "jet", "JMXJets", 4),
+]
+
+
+def case_ref_ics(ref, out):
+    """Initial particles of the reference's other case generators
+    (src/cases/{mhdsine,mhdwave,mhdrotor,mhdvortex,jadvect,jet}.py), built by
+    the reference's own classes from its own TOML files at a small nx."""
+    import importlib
+
+    cfgmod = ref["config"]
+    for name, module, cls_name, nx in IC_CASES:
+        mod = importlib.import_module(f"src.cases.{module}")
+        cls = getattr(mod, cls_name)
+        sim = cfgmod.load_config(os.path.join(REF, "configs", f"{name}.toml"), {name: cls.config_type})
+        sim = replace(sim, case=replace(sim.case, nx=nx))
+        app = cls(sim)
+        pa = app.create_mhd_particles()[0]
+        for k in IC_FIELDS:
+            out[f"{name}/{k}"] = np.array(pa.properties[k], copy=True)
+        out[f"{name}/nx"] = np.array(nx)
+        print(f"  {name}: {pa.get_number_of_particles()} particles", flush=True)
+
+
 CASES = {
+    "ref_ics": case_ref_ics,
     "lattice": case_lattice,
     "ot2d": case_ot2d,
     "shock2d": case_shock2d,

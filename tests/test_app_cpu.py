@@ -48,14 +48,36 @@ def test_benchmark_configs_load_and_build_cases():
 
 @pytest.mark.skipif(not os.path.isdir(REFERENCE_CONFIGS), reason="reference checkout not present")
 def test_reference_toml_files_load_unchanged():
-    from src.config import SimulationConfig, load_config
+    from src.config import load_config
+    from src.run import CASES
 
+    types = {n: a.config_type for n, a in CASES.items()}
     for path in sorted(glob.glob(os.path.join(REFERENCE_CONFIGS, "*.toml"))):
-        if "jet" in os.path.basename(path):
-            continue  # the jet case has its own schema (out of scope)
-        name = os.path.basename(path)[:-5]
-        cfg = load_config(path, {name: SimulationConfig})
+        cfg = load_config(path, types)
         assert cfg.numerics.dim is None and cfg.execution.precision is None
+
+
+IC_FIELDS = "x y z u v w rho h m e Bx By Bz alpha1".split()
+
+
+@pytest.mark.parametrize("name", ["mhdsine", "mhdwave", "mhdrotor", "mhdvortex", "jadvect", "1jet", "3jet", "12jet"])
+def test_case_generators_match_reference_fixtures(name):
+    # the fixtures hold what the reference's own generators build from its
+    # own TOML files at a small nx (tests/golden/make_golden.py, ref_ics)
+    from dataclasses import replace
+
+    from src.config import load_config
+    from src.run import CASES
+
+    d = np.load(os.path.join(GOLDEN, "ref_ics.npz"))
+    cfg = load_config(os.path.join(PKG, "configs", f"{name}.toml"), {k: v.config_type for k, v in CASES.items()})
+    cfg = replace(cfg, case=replace(cfg.case, nx=int(d[f"{name}/nx"])))
+    got = CASES[name](cfg).create_mhd_particles()
+    for k in IC_FIELDS:
+        ref = d[f"{name}/{k}"]
+        assert got[k].shape == ref.shape, f"{name} {k}"
+        scale = max(float(np.abs(ref).max()), 1e-300)
+        np.testing.assert_allclose(got[k], ref, rtol=1e-13, atol=1e-13 * scale, err_msg=f"{name} {k}")
 
 
 def test_scheme_groups_compile_to_kernel_parameters():
