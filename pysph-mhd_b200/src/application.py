@@ -31,6 +31,7 @@ class Domain:
 
 class MHDApplication:
     config_type = SimulationConfig
+    detailed_output = False  # dumps hold every property (restart files)
 
     def __init__(self, config):
         self.config = config
@@ -83,6 +84,7 @@ class MHDApplication:
 
     def configure_scheme(self):
         self.scheme.configure_solver(dt=1.0, tf=self.tf, adaptive_timestep=self.adaptive_timestep, pfreq=self.pfreq,
+                                     detailed_output=self.detailed_output,
                                      max_steps=self.config.solver.max_steps,
                                      output_directory=self.config.execution.directory, fname=self.fname)
 
@@ -124,6 +126,23 @@ class MHDApplication:
         if self.engine is None:
             self.setup(device)
         self.solve()
+        torch.cuda.synchronize()
+        return self.particles[0]
+
+    def restart(self, path, device="cuda"):
+        """Continue a run from a dump written with ``detailed_output`` (every
+        property: the state, the integrator copies and the last rates): the
+        steps after it equal those of the uninterrupted run."""
+        from .solver import load_output
+
+        arrays, solver_data = load_output(path)
+        missing = [k for k in ("x0", "au", "dt_adapt", "Bevolxpred") if k not in arrays]
+        if missing:
+            raise ValueError(f"{path} is not a detailed dump (lacks {missing}); write it with detailed_output")
+        self.create_mhd_particles = lambda: arrays
+        self.setup(device)
+        self.solver.restore(solver_data)
+        self.solver.solve()
         torch.cuda.synchronize()
         return self.particles[0]
 

@@ -3,8 +3,16 @@
 The loop is the reference's: skip the start-up RHS when the application has
 already warmed it, ``dt = _get_timestep()``, step while ``tf - t`` exceeds the
 tolerance and ``count < max_steps``, dump every ``pfreq`` steps.  The step and
-the timestep reduction run on the device (``src.engine.Engine``); the dump is
-an ``.npz`` of ``OUTPUT_PROPERTIES`` ordered by ``gid``.
+the timestep reduction run on the device (``src.engine.Engine``).
+
+A dump is an ``.npz`` ordered by ``gid`` in PySPH's version-2 layout: a
+pickled ``particles`` dict ({name: {"name", "arrays", "constants",
+"output_property_arrays"}}) and a ``solver_data`` dict (t, dt, count), as
+PySPH's ``dump``/``load`` write and read them (restated from PySPH's
+documented format, not checked against PySPH, which is not installed), plus
+the same arrays and t, dt, count as plain top-level keys.  It holds
+``OUTPUT_PROPERTIES``, or every property with ``detailed_output``: such a
+dump restarts the run exactly (``MHDApplication.restart``).
 """
 
 from __future__ import annotations
@@ -23,7 +31,8 @@ EPSILON = 2.220446049250313e-16
 
 class MHDSolver:
     def __init__(self, dim=3, integrator=None, kernel="cubic", dt=1.0, tf=1.0, adaptive_timestep=True, pfreq=1,
-                 max_steps=None, output_directory=None, fname="mhd", **kw):
+                 max_steps=None, output_directory=None, fname="mhd", detailed_output=False, **kw):
+        self.detailed_output = detailed_output
         self.dim = dim
         self.integrator = integrator
         self.kernel = kernel
@@ -54,10 +63,24 @@ class MHDSolver:
             return None
         os.makedirs(self.output_directory, exist_ok=True)
         pa = self.particles[0]
-        arrays = pa.pull(*OUTPUT_PROPERTIES, order="gid")
+        names = tuple(pa.properties) if self.detailed_output else OUTPUT_PROPERTIES
+        arrays = pa.pull(*names, order="gid")
         path = os.path.join(self.output_directory, f"{self.fname}_{self.count:06d}.npz")
-        np.savez(path, t=self.t, dt=self.dt, count=self.count, **arrays)
+        solver_data = {"t": self.t, "dt": self.dt, "count": self.count}
+        particles = {pa.name: {"name": pa.name, "arrays": arrays, "constants": {},
+                               "output_property_arrays": list(OUTPUT_PROPERTIES)}}
+        blob = {"version": np.array(2), "particles": np.array(particles, dtype=object),
+                "solver_data": np.array(solver_data, dtype=object)}
+        np.savez(path, t=self.t, dt=self.dt, count=self.count, **blob, **arrays)
         return path
+
+    def restore(self, solver_data):
+        """Continue from a dump's clock: the state already holds the rates of
+        the last right-hand side."""
+        self.t = float(solver_data["t"])
+        self.count = int(solver_data["count"])
+        self.dt = float(solver_data["dt"])
+        self.initial_acceleration_is_current = True
 
     def solve(self, show_progress=False):
         self._epsilon = EPSILON * self.tf
@@ -81,3 +104,14 @@ class MHDSolver:
             if self.count % self.pfreq == 0:
                 self.dump_output()
         self.dump_output()
+
+
+def load_output(path):
+    """Arrays (by property name, in gid order) and solver data of a dump."""
+    with np.load(path, allow_pickle=True) as d:
+        if "particles" in d.files:
+            particles = d["particles"].item()
+            pa = next(iter(particles.values()))
+            return dict(pa["arrays"]), dict(d["solver_data"].item())
+        skip = {"t", "dt", "count"}
+        return {k: d[k] for k in d.files if k not in skip}, {k: d[k].item() for k in skip}

@@ -109,3 +109,33 @@ def test_config_rejects_unknown_keys_and_bad_types(tmp_path):
         p.write_text(text)
         with pytest.raises(ValueError):
             load_config(p, {"orstang2d": SimulationConfig})
+
+
+def test_dump_layout_and_load_round_trip(tmp_path):
+    # PySPH's version-2 npz layout (pickled particles / solver_data dicts)
+    # plus plain top-level arrays; a detailed dump holds every property
+    from src.particle_array import ParticleArray
+    from src.particles import OUTPUT_PROPERTIES
+    from src.solver import MHDSolver, load_output
+
+    rng = np.random.default_rng(3)
+    n = 50
+    arrays = {k: rng.random(n) for k in ("x", "y", "z", "u", "rho", "h", "m", "e", "Bx", "au", "x0")}
+    arrays["gid"] = rng.permutation(n).astype(np.float64)
+    pa = ParticleArray("fluid", arrays, device="cpu")
+    for detailed in (False, True):
+        s = MHDSolver(output_directory=str(tmp_path / str(detailed)), fname="t", detailed_output=detailed)
+        s.particles = [pa]
+        s.t, s.dt, s.count = 0.25, 1e-3, 7
+        path = s.dump_output()
+        with np.load(path, allow_pickle=True) as d:
+            assert int(d["version"]) == 2
+            parts = d["particles"].item()
+            assert list(parts) == ["fluid"] and parts["fluid"]["output_property_arrays"] == list(OUTPUT_PROPERTIES)
+            assert d["solver_data"].item() == {"t": 0.25, "dt": 1e-3, "count": 7}
+        got, sd = load_output(path)
+        assert sd == {"t": 0.25, "dt": 1e-3, "count": 7}
+        order = np.argsort(arrays["gid"])
+        np.testing.assert_array_equal(got["x"], arrays["x"][order])
+        assert ("au" in got) == detailed and ("x0" in got) == detailed
+        assert set(OUTPUT_PROPERTIES) <= set(got)
