@@ -292,11 +292,17 @@ def _timed(args, prec, dev, barrier, dist, world):
             "passes": passes, "lists_rebuilt": rebuilt.value / max(listed.value, 1)}
 
 
-def _batched(args, dev):
+def _batched(args, dev, rank=0, world=1):
     """The batched form: 64 independent 2-D Orszag-Tang instances (N ~ U{32..256},
     B0 x U[0.8, 1.2], seed 0) advanced 100 steps as one captured graph after
-    the autotuner, against the plain FP64 path run instance by instance."""
+    the autotuner, against the plain FP64 path run instance by instance.
+    With N ranks the instances are shared out by particle count
+    (src.parallel.shard_instances); each rank runs its share in FP32, the
+    value is all particle-steps over the slowest rank's time, and the ranks'
+    per-instance checksums are gathered."""
     import torch
+
+    from src.parallel import checksum, gather_instances, max_over_ranks, shard_instances
 
     from src.batch import BatchEngine
     from src.cases.orstang import orszag_tang_batch
@@ -308,10 +314,13 @@ def _batched(args, dev):
     cfg = load_config(os.path.join(PKG, "configs", "orstang2d.toml"), {k: v.config_type for k, v in CASES.items()})
     inst, prm, sizes, scales = orszag_tang_batch(cfg, n_inst=args.batch_instances, seed=0)
     total = int(sum(len(a["x"]) for a in inst))
+    n_all = len(inst)
+    share = shard_instances([len(a["x"]) for a in inst], world)[rank]
+    inst = [inst[k] for k in share]
     steps = args.batch_steps
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     out, final = {}, {}
-    for prec in ("fp32", "fp64"):
+    for prec in ("fp32", "fp64") if world == 1 else ("fp32",):
         eng = BatchEngine(params_from_dict(prm, prec), inst)
         eng.warmup()
         eng.begin(eng.initial_dt())
@@ -327,12 +336,20 @@ def _batched(args, dev):
         eng.advance(steps, finish=True, snapshot=snap)
         ev1.record()
         ev1.synchronize()
-        ms = ev0.elapsed_time(ev1)
+        ms = max_over_ranks(ev0.elapsed_time(ev1), dev)
         out[prec] = {"value": total * steps / (ms * 1e-3), "ms": ms, "gpu_launches": eng.launches() - l0,
                      "graph_launches": 1, "replays": eng.replays - r0, "tune_s": tune_s,
                      "tuned": {"stencil": tuned["stencil"], "force_shape": tuned["force_shape"]}}
         final[prec] = eng.pa.pull("rho", "u", "v", "Bx", "By", "gid", order="gid")
+        if world > 1:
+            sums = gather_instances({k: checksum(eng.pull_instance(i, "rho", "u", "v", "Bx", "By"))
+                                     for i, k in enumerate(share)}, n_all)
         eng.close()
+    if world > 1:
+        return {"workload": f"{n_all} x 2-D Orszag-Tang (seed 0), {total} particles, {steps} steps, instances "
+                            f"shared out over {world} ranks by particle count",
+                "particles": total, "steps": steps, "fp32": out["fp32"], "ranks": world,
+                "instance_checksums_sum": float(sum(sums))}
     # plain FP64 path, one instance at a time (K steps each, summed device time)
     k_loop = args.batch_loop_steps
     loop_ms = 0.0
@@ -618,7 +635,7 @@ def run_b200(args, rank, world):
     achieved_tf = flops / (force_ms * 1e-3) / 1e12
 
     e2e = run_e2e(args, dev)
-    batched = _batched(args, dev) if (rank == 0 and not dist and args.batch_instances > 0) else None
+    batched = _batched(args, dev, rank, world) if args.batch_instances > 0 else None
     derivative = _derivative(args, dev) if (rank == 0 and not dist and args.derivative_steps > 0) else None
 
     cpu = None
