@@ -451,6 +451,8 @@ __global__ void __launch_bounds__(128) k_build_lists_big(DevParams P, const Grid
 
 // Order the scattered entries of every list by index (the scatter pass
 // appends them in whatever order its atomics resolve) and cap the counts.
+constexpr int kSortLocal = 48;  // appended entries sorted in a private copy
+
 __global__ void __launch_bounds__(128) k_sort_appended(int n, int cap, int* __restrict__ idx, int* __restrict__ cnt,
                                                        const int* __restrict__ gcnt) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -461,8 +463,26 @@ __global__ void __launch_bounds__(128) k_sort_appended(int n, int cap, int* __re
     cnt[i] = cap;
   }
   const int g = gcnt[i];
-  if (c - g < 2) return;
+  const int m = c - g;
+  if (m < 2) return;
   int* __restrict__ row = idx + (size_t)(i >> 5) * cap * 32 + (i & 31);
+  if (m <= kSortLocal) {
+    // sort a private copy (thread-local memory, L1-resident) instead of
+    // shifting the strided list entries in place
+    int v[kSortLocal];
+    for (int a = 0; a < m; a++) v[a] = row[(size_t)(g + a) * 32];
+    for (int a = 1; a < m; a++) {
+      const int t = v[a];
+      int b = a - 1;
+      while (b >= 0 && v[b] > t) {
+        v[b + 1] = v[b];
+        b--;
+      }
+      v[b + 1] = t;
+    }
+    for (int a = 0; a < m; a++) row[(size_t)(g + a) * 32] = v[a];
+    return;
+  }
   for (int a = g + 1; a < c; a++) {
     const int v = row[a * 32];
     int b = a - 1;
