@@ -147,8 +147,8 @@ __device__ __forceinline__ bool density_particle(int i, const DevParams& P, cons
   return !finalize;
 }
 
-// A density pass over all particles (a pass after the group stopped
-// returns at once).
+// A density pass over all particles, grid-stride (a pass after the group
+// stopped returns at once).
 template <int K, int DIM, class T>
 __global__ void __launch_bounds__(128) k_density_pass(int n, int pass, DevParams P, NbrList L,
                                                       const double* __restrict__ x, const double* __restrict__ y,
@@ -167,13 +167,14 @@ __global__ void __launch_bounds__(128) k_density_pass(int n, int pass, DevParams
     if (stop) return;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) atomicMax(&sc->passes_done, pass + 1);
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const bool unconv = density_particle<K, DIM, T>(i, P, L, x, y, z, m, h_in, h_out, h0, rho_sum, omega, converged,
-                                                  grids, inst, posm, cellc, sc);
-  const unsigned act = __activemask();
-  const unsigned b = __ballot_sync(act, unconv);
-  if (b && (int)(threadIdx.x & 31) == __ffs(act) - 1) atomicAdd(&sc->n_unconverged[pass], __popc(b));
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const bool unconv = density_particle<K, DIM, T>(i, P, L, x, y, z, m, h_in, h_out, h0, rho_sum, omega,
+                                                    converged, grids, inst, posm, cellc, sc);
+    const unsigned act = __activemask();
+    const unsigned b = __ballot_sync(act, unconv);
+    if (b && (int)(threadIdx.x & 31) == __ffs(act) - 1) atomicAdd(&sc->n_unconverged[pass], __popc(b));
+  }
 }
 
 // ------------------------------------------------------- neighbour lists
@@ -840,7 +841,11 @@ void launch_build_lists(Ctx* c, const MhdState* s, int n, cudaStream_t st, const
 // ------------------------------------------------------------- dispatch
 template <int K, int DIM>
 static void density_launch(Ctx* c, MhdState* s, int n, int pass, const double* h_in, double* h_out, cudaStream_t st) {
-  const int grid = (n + 127) / 128;
+  // Passes 0 and 1 cover the particles with one thread each; later passes,
+  // which most groups skip (and which then return at once), use about one
+  // wave of blocks, so a skipped pass costs little in a captured run.
+  const int full = (n + 127) / 128;
+  const int grid = pass < 2 ? full : std::min(full, c->num_sms * 8);
   if (c->P.fp32) {
     k_density_pass<K, DIM, float><<<grid, 128, 0, st>>>(n, pass, c->P, c->lists(), s->x, s->y, s->z, s->m, h_in, h_out,
                                                         s->h0, s->rho_sum, s->omega, s->converged, c->d_grids, c->inst,
