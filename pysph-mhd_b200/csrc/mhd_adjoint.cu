@@ -73,6 +73,33 @@ __device__ inline void all_pairs(int n, const DevParams& P, int i, const double*
   }
 }
 
+// all_pairs over the candidates jlo .. jhi - 1 only (a slice of them).
+template <int DIM, class F>
+__device__ inline void pairs_in_range(int n, const DevParams& P, int i, const double* x, const double* y,
+                                      const double* z, const double* h, int jlo, int jhi, F&& f) {
+  __shared__ double4 shr[kTile];
+  const bool active = i < n;
+  const double xi = active ? x[i] : 0.0, yi = active ? y[i] : 0.0, zi = active && DIM == 3 ? z[i] : 0.0;
+  const double rhi2 = active ? rh2_exact(P.R, h[i]) : 0.0;
+  for (int base = jlo; base < jhi; base += kTile) {
+    const int j = base + threadIdx.x;
+    if (j < jhi) shr[threadIdx.x] = make_double4(x[j], y[j], DIM == 3 ? z[j] : 0.0, h[j]);
+    __syncthreads();
+    if (active) {
+      const int m = jhi - base < kTile ? jhi - base : kTile;
+      for (int t = 0; t < m; t++) {
+        const double4 q = shr[t];
+        const double dx = min_image(xi - q.x, P.L[0], P.half[0], P.periodic[0]);
+        const double dy = min_image(yi - q.y, P.L[1], P.half[1], P.periodic[1]);
+        const double dz = DIM == 3 ? min_image(zi - q.z, P.L[2], P.half[2], P.periodic[2]) : 0.0;
+        const double r2 = r2_exact(dx, dy, dz);
+        if (r2 < rhi2 || r2 < rh2_exact(P.R, q.w)) f(base + t, dx, dy, dz);
+      }
+    }
+    __syncthreads();
+  }
+}
+
 template <int N>
 __device__ inline Dual<N> seeded(double v, int k) {
   Dual<N> r(v);
@@ -97,6 +124,7 @@ struct Args {
   double* g_amax;          // reverse: per-particle dL/d alpha_max (accumulating over steps)
   const double* s_final;   // reverse, last step: S_K (loss terms)
   double* dta_out;         // forward: dt_adapt of the step (adaptive step sizes)
+  double* slices;          // reverse: per-slice partial sums of the force pair pass
 };
 
 #define TP(k, i) a.tape_w[(size_t)(k) * a.n + (i)]
@@ -158,6 +186,32 @@ __device__ inline Side<D> side_at(const double* t, int n, int i, int base) {
   auto g = [&](int k, int s) {
     D r(t[(size_t)k * n + i]);
     if (base >= 0) r.d[base + s] = 1.0;
+    return r;
+  };
+  Side<D> s;
+  s.h = g(T_HN, 0);
+  s.rho = g(T_RHO, 1);
+  s.p = g(T_P, 2);
+  s.omega = g(T_OM, 3);
+  s.cs = g(T_CS, 4);
+  for (int c = 0; c < 3; c++) {
+    s.b[c] = g(T_B + c, 5 + c);
+    s.v[c] = g(T_VP + c, 8 + c);
+  }
+  s.e = g(T_EP, 11);
+  s.alpha = g(T_A1, 12);
+  s.psi = g(T_PSIP, 13);
+  return s;
+}
+
+// Side of particle i with only the directions lo .. lo + N - 1 of the
+// kSideDirs side inputs seeded (local direction s - lo).
+template <int N>
+__device__ inline Side<Dual<N>> side_window(const double* t, int n, int i, int lo) {
+  using D = Dual<N>;
+  auto g = [&](int k, int s) {
+    D r(t[(size_t)k * n + i]);
+    if (s >= lo && s < lo + N) r.d[s - lo] = 1.0;
     return r;
   };
   Side<D> s;
@@ -465,56 +519,86 @@ __device__ inline void add_side(const Args& a, int i, const double* g, double si
 
 // Force pair terms reversed, gather form: particle k collects the terms of
 // the pairs (k, j) through its i side and x_k, and of the pairs (j, k)
-// through its j side and x_k.
+// through its j side and x_k.  The kSideDirs + 3 input directions are
+// evaluated a window of kForceWindow at a time, so the dual sums a thread
+// holds stay small (the same derivatives as one pass over all directions).
+// The candidates are split into kPairSlices slices (grid y), so that a
+// small particle count still fills the GPU; each slice writes its partial
+// sums and k_r_force_pair_sum adds them in slice order (deterministic).
+constexpr int kForceWindow = 3;
+constexpr int kPairSlices = 8;
+constexpr int kForceDirs = kSideDirs + 3;
+
 template <int K, int DIM>
 __global__ void __launch_bounds__(kTile) k_r_force_pair(Args a) {
-  using D = Dual<kSideDirs + 3>;
+  constexpr int NW = kForceWindow, ND = kForceDirs;
+  using D = Dual<NW>;
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int n = a.n;
   const double* X = a.tape + (size_t)T_X * n;
   const double* HN = a.tape + (size_t)T_HN * n;
   const int kk = k < n ? k : 0;
-  const Side<D> Kseed = side_at<D>(a.tape, n, kk, 0);
-  const Side<D> Kval = side_at<D>(a.tape, n, kk, -1);
+  const int chunk = (n + kPairSlices * kTile - 1) / (kPairSlices * kTile) * kTile;
+  const int jlo = blockIdx.y * chunk, jhi = jlo + chunk < n ? jlo + chunk : n;
   double gs[kSideDirs] = {}, gx[3] = {};
-  all_pairs<DIM>(n, a.P, k, X, X + n, X + 2 * n, HN, [&](int j, double dx, double dy, double dz) {
+  pairs_in_range<DIM>(n, a.P, k, X, X + n, X + 2 * n, HN, jlo, jhi, [&](int j, double dx, double dy, double dz) {
     const Side<D> Jval = side_at<D>(a.tape, n, j, -1);
-    // (k, j): k is the i side
-    {
-      const D xij[3] = {seeded<kSideDirs + 3>(dx, kSideDirs), seeded<kSideDirs + 3>(dy, kSideDirs + 1),
-                        seeded<kSideDirs + 3>(dz, kSideDirs + 2)};
-      FSums<D> S;
-      S.zero();
-      f_force_pair<K, DIM>(a.P, Kseed, Jval, D(a.m[j]), xij, S);
-      D* sp[kFSumDirs];
-      fsum_ptrs(S, sp);
-      for (int d = 0; d < kSideDirs + 3; d++) {
-        double s = 0.0;
-        for (int q = 0; q < kFSumDirs; q++) s += W(M_F + q, k) * sp[q]->d[d];
-        if (d < kSideDirs) gs[d] += s;
-        else gx[d - kSideDirs] += s;
+    for (int lo = 0; lo < ND; lo += NW) {
+      const Side<D> Kseed = side_window<NW>(a.tape, n, kk, lo);
+      // the displacement directions kSideDirs .. kSideDirs + 2 in this window
+      auto xs = [&](double v, int c) {
+        const int l = kSideDirs + c - lo;
+        return seeded<NW>(v, l >= 0 && l < NW ? l : -1);
+      };
+      // (k, j): k is the i side
+      {
+        const D xij[3] = {xs(dx, 0), xs(dy, 1), xs(dz, 2)};
+        FSums<D> S;
+        S.zero();
+        f_force_pair<K, DIM>(a.P, Kseed, Jval, D(a.m[j]), xij, S);
+        D* sp[kFSumDirs];
+        fsum_ptrs(S, sp);
+        for (int d = 0; d < NW && lo + d < ND; d++) {
+          double v = 0.0;
+          for (int q = 0; q < kFSumDirs; q++) v += W(M_F + q, k) * sp[q]->d[d];
+          if (lo + d < kSideDirs) gs[lo + d] += v;
+          else gx[lo + d - kSideDirs] += v;
+        }
       }
-    }
-    // (j, k): k is the j side, x_j - x_k = -(dx, dy, dz)
-    {
-      const D xji[3] = {seeded<kSideDirs + 3>(-dx, kSideDirs), seeded<kSideDirs + 3>(-dy, kSideDirs + 1),
-                        seeded<kSideDirs + 3>(-dz, kSideDirs + 2)};
-      FSums<D> S;
-      S.zero();
-      f_force_pair<K, DIM>(a.P, Jval, Kseed, D(a.m[k]), xji, S);
-      D* sp[kFSumDirs];
-      fsum_ptrs(S, sp);
-      for (int d = 0; d < kSideDirs + 3; d++) {
-        double s = 0.0;
-        for (int q = 0; q < kFSumDirs; q++) s += W(M_F + q, j) * sp[q]->d[d];
-        if (d < kSideDirs) gs[d] += s;
-        else gx[d - kSideDirs] -= s;
+      // (j, k): k is the j side, x_j - x_k = -(dx, dy, dz)
+      {
+        const D xji[3] = {xs(-dx, 0), xs(-dy, 1), xs(-dz, 2)};
+        FSums<D> S;
+        S.zero();
+        f_force_pair<K, DIM>(a.P, Jval, Kseed, D(a.m[k]), xji, S);
+        D* sp[kFSumDirs];
+        fsum_ptrs(S, sp);
+        for (int d = 0; d < NW && lo + d < ND; d++) {
+          double v = 0.0;
+          for (int q = 0; q < kFSumDirs; q++) v += W(M_F + q, j) * sp[q]->d[d];
+          if (lo + d < kSideDirs) gs[lo + d] += v;
+          else gx[lo + d - kSideDirs] -= v;
+        }
       }
     }
   });
-  (void)Kval;
   if (k >= n) return;
-  add_side(a, k, gs, 1.0, gx);
+  double* part = a.slices + (size_t)blockIdx.y * ND * n;
+  for (int d = 0; d < kSideDirs; d++) part[(size_t)d * n + k] = gs[d];
+  for (int c = 0; c < 3; c++) part[(size_t)(kSideDirs + c) * n + k] = gx[c];
+}
+
+__global__ void __launch_bounds__(256) k_r_force_pair_sum(Args a) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = a.n;
+  if (k >= n) return;
+  double g[kForceDirs];
+  for (int d = 0; d < kForceDirs; d++) {
+    double v = 0.0;
+    for (int s = 0; s < kPairSlices; s++) v += a.slices[((size_t)s * kForceDirs + d) * n + k];
+    g[d] = v;
+  }
+  add_side(a, k, g, 1.0, g + kSideDirs);
 }
 
 // Cullen-Dehnen post reversed: the sum adjoints mu_CD and the lambdas of
@@ -706,7 +790,8 @@ static void reverse_step(const Args& a, cudaStream_t st) {
   const int nb = (a.n + kTile - 1) / kTile, np = (a.n + 255) / 256, n64 = (a.n + 63) / 64;
   k_r_correct<<<np, 256, 0, st>>>(a);
   k_r_force_post<DIM><<<n64, 64, 0, st>>>(a);
-  k_r_force_pair<K, DIM><<<nb, kTile, 0, st>>>(a);
+  k_r_force_pair<K, DIM><<<dim3(nb, kPairSlices), kTile, 0, st>>>(a);
+  k_r_force_pair_sum<<<np, 256, 0, st>>>(a);
   k_r_cd_post<<<n64, 64, 0, st>>>(a);
   k_r_cd_pair<K, DIM><<<nb, kTile, 0, st>>>(a);
   k_r_prologue<DIM><<<np, 256, 0, st>>>(a);
@@ -758,7 +843,7 @@ const char* const kAdjointFields[NS] = {"x",  "y",  "z",  "u",  "v",  "w",      
 // Workspace of the adjoint: two states, `every` tapes, the reverse
 // workspace, two lambdas, the per-particle alpha_max derivative, partials.
 struct AdjLayout {
-  size_t state[2], tape, w, lam[2], g_amax, dta, part, total;
+  size_t state[2], tape, w, lam[2], g_amax, dta, part, slices, total;
 };
 
 AdjLayout layout(int64_t n, int every) {
@@ -778,6 +863,7 @@ AdjLayout layout(int64_t n, int every) {
   L.g_amax = take(n);
   L.dta = take(n);
   L.part = take(n / 256 + 64);
+  L.slices = take((size_t)kPairSlices * kForceDirs * n);
   L.total = off;
   return L;
 }
@@ -907,6 +993,7 @@ int mhd_adjoint_backward(void* ctx, const MhdState* s, int64_t n, int32_t steps,
   Args a = base_args(c, s, n, c->P.alpha_max);
   a.w = buf + L.w;
   a.g_amax = buf + L.g_amax;
+  a.slices = buf + L.slices;
   double* lam_next = buf + L.lam[0];
   double* lam = buf + L.lam[1];
   const int nseg = (steps + every - 1) / every;
@@ -926,7 +1013,7 @@ int mhd_adjoint_backward(void* ctx, const MhdState* s, int64_t n, int32_t steps,
         c->launches++;
       }
       MHD_A_DISPATCH(reverse_step, r, st);
-      c->launches += 9;
+      c->launches += 10;
       double* tmp = lam_next;
       lam_next = lam;
       lam = tmp;
