@@ -13,7 +13,7 @@ imports, so the reference's own equation, integrator, scheme, warm-up
 runs unchanged, in pure-Python loops, on tiny particle sets.
 
 What the shim itself restates (PySPH semantics; unpinned, since PySPH's
-source is not available) -- each item is a decision recorded in DESIGN.md:
+source is not available) -- each item is a decision of this restatement:
 
 * kernels: cubic spline (Monaghan M4, R=2), quintic spline (Morris, R=3),
   Wendland C2/C4/C6 (R=2), Gaussian and super-Gaussian (R=3), each with its
