@@ -48,10 +48,14 @@ __host__ __device__ inline Dual<N> operator*(const Dual<N>& a, const Dual<N>& b)
   for (int k = 0; k < N; k++) r.d[k] = a.d[k] * b.v + a.v * b.d[k];
   return r;
 }
+// The value is the IEEE quotient; the derivative parts are scaled by one
+// reciprocal (an FP64 division costs many instructions, N of them dominated
+// the dual arithmetic).
 template <int N>
 __host__ __device__ inline Dual<N> operator/(const Dual<N>& a, const Dual<N>& b) {
   Dual<N> r(a.v / b.v);
-  for (int k = 0; k < N; k++) r.d[k] = (a.d[k] - r.v * b.d[k]) / b.v;
+  const double inv = 1.0 / b.v;
+  for (int k = 0; k < N; k++) r.d[k] = (a.d[k] - r.v * b.d[k]) * inv;
   return r;
 }
 template <int N>
@@ -71,7 +75,12 @@ __host__ __device__ inline Dual<N> operator*(const Dual<N>& a, double b) {
 template <int N>
 __host__ __device__ inline Dual<N> operator*(double a, const Dual<N>& b) { return b * a; }
 template <int N>
-__host__ __device__ inline Dual<N> operator/(const Dual<N>& a, double b) { return a / Dual<N>(b); }
+__host__ __device__ inline Dual<N> operator/(const Dual<N>& a, double b) {
+  Dual<N> r(a.v / b);
+  const double inv = 1.0 / b;
+  for (int k = 0; k < N; k++) r.d[k] = a.d[k] * inv;
+  return r;
+}
 template <int N>
 __host__ __device__ inline Dual<N> operator/(double a, const Dual<N>& b) { return Dual<N>(a) / b; }
 template <int N, class T>
