@@ -525,7 +525,7 @@ __device__ inline void add_side(const Args& a, int i, const double* g, double si
 // The candidates are split into kPairSlices slices (grid y), so that a
 // small particle count still fills the GPU; each slice writes its partial
 // sums and k_r_force_pair_sum adds them in slice order (deterministic).
-constexpr int kForceWindow = 3;
+constexpr int kForceWindow = 6;
 constexpr int kPairSlices = 8;
 constexpr int kForceDirs = kSideDirs + 3;
 
