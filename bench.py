@@ -365,9 +365,22 @@ def _batched(args, dev, rank=0, world=1):
         loop_ms += ev0.elapsed_time(ev1)
         eng.close()
     loop = total * k_loop / (loop_ms * 1e-3)
-    a, b = final["fp32"], final["fp64"]
+    # control: the FP64 batch again with every x moved by 1e-10 of its
+    # instance's spacing -- the spread that rounding of any kind reaches on
+    # these unjittered lattices (their Cullen-Dehnen limiter starts as
+    # roundoff over roundoff)
+    rng = np.random.default_rng(1)
+    moved = [dict(a_, x=a_["x"] + 1e-10 * rng.uniform(-1.0, 1.0, len(a_["x"])) / np.sqrt(len(a_["x"])))
+             for a_ in inst]
+    eng = BatchEngine(params_from_dict(prm, "fp64"), moved)
+    eng.warmup()
+    eng.begin(eng.initial_dt())
+    eng.advance(steps, finish=True, capture=False)
+    final["fp64_moved"] = eng.pa.pull("rho", "u", "v", "Bx", "By", "gid", order="gid")
+    eng.close()
 
-    def rel(keys):
+    def rel(keys, a_name="fp32", b_name="fp64"):
+        a, b = final[a_name], final[b_name]
         num = sum(float(np.sum((a[k] - b[k]) ** 2)) for k in keys)
         den = sum(float(np.sum(b[k] ** 2)) for k in keys)
         return math.sqrt(num / den)
@@ -379,7 +392,9 @@ def _batched(args, dev, rank=0, world=1):
             "fp64_instance_loop": {"value": loop, "steps_per_instance": k_loop, "ms": loop_ms},
             "speedup_fp32_vs_fp64_loop": out["fp32"]["value"] / loop,
             "speedup_fp64_vs_fp64_loop": out["fp64"]["value"] / loop,
-            "fp32_vs_fp64_rel_l2": {"rho": rel(["rho"]), "v": rel(["u", "v"]), "B": rel(["Bx", "By"])}}
+            "fp32_vs_fp64_rel_l2": {"rho": rel(["rho"]), "v": rel(["u", "v"]), "B": rel(["Bx", "By"])},
+            "fp64_moved_1e-10dx_vs_fp64_rel_l2": {"rho": rel(["rho"], "fp64_moved"), "v": rel(["u", "v"], "fp64_moved"),
+                                                  "B": rel(["Bx", "By"], "fp64_moved")}}
 
 
 def _accuracy(args, dev, steps):
