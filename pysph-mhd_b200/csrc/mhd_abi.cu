@@ -741,6 +741,7 @@ int mhd_ctx_set_params(void* ctx, const MhdParams* params) {
   Ctx* c = (Ctx*)ctx;
   if (!c) return MHD_ERR_INVALID;
   c->generation++;
+  c->layout_gen++;  // the kernel radius may change: no list is carried over
   return fill_params(c, params);
 }
 
