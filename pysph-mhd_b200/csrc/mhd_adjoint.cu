@@ -125,6 +125,7 @@ struct Args {
   const double* s_final;   // reverse, last step: S_K (loss terms)
   double* dta_out;         // forward: dt_adapt of the step (adaptive step sizes)
   double* slices;          // reverse: per-slice partial sums of the force pair pass
+  int dual_pairs;          // reverse: force pair VJPs from dual Jacobians (check path) instead of by hand
 };
 
 #define TP(k, i) a.tape_w[(size_t)(k) * a.n + (i)]
@@ -529,7 +530,7 @@ constexpr int kForceWindow = 6;
 constexpr int kPairSlices = 8;
 constexpr int kForceDirs = kSideDirs + 3;
 
-template <int K, int DIM>
+template <int K, int DIM, bool DUAL>
 __global__ void __launch_bounds__(kTile) k_r_force_pair(Args a) {
   constexpr int NW = kForceWindow, ND = kForceDirs;
   using D = Dual<NW>;
@@ -541,6 +542,26 @@ __global__ void __launch_bounds__(kTile) k_r_force_pair(Args a) {
   const int chunk = (n + kPairSlices * kTile - 1) / (kPairSlices * kTile) * kTile;
   const int jlo = blockIdx.y * chunk, jhi = jlo + chunk < n ? jlo + chunk : n;
   double gs[kSideDirs] = {}, gx[3] = {};
+  if constexpr (!DUAL) {
+    // hand-written VJP (vjp_force_pair)
+    const Side<double> Kv = side_values(a.tape, n, kk);
+    pairs_in_range<DIM>(n, a.P, k, X, X + n, X + 2 * n, HN, jlo, jhi, [&](int j, double dx, double dy, double dz) {
+      const Side<double> Jv = side_values(a.tape, n, j);
+      double w[kFSumDirs], gI[kSideDirs], gJ[kSideDirs], gxx[3];
+      // (k, j): k is the i side
+      for (int q = 0; q < kFSumDirs; q++) w[q] = W(M_F + q, k);
+      const double xkj[3] = {dx, dy, dz};
+      vjp_force_pair<K, DIM>(a.P, Kv, Jv, a.m[j], xkj, w, gI, gJ, gxx);
+      for (int d = 0; d < kSideDirs; d++) gs[d] += gI[d];
+      for (int c = 0; c < 3; c++) gx[c] += gxx[c];
+      // (j, k): k is the j side, x_j - x_k = -(dx, dy, dz)
+      for (int q = 0; q < kFSumDirs; q++) w[q] = W(M_F + q, j);
+      const double xjk[3] = {-dx, -dy, -dz};
+      vjp_force_pair<K, DIM>(a.P, Jv, Kv, a.m[k], xjk, w, gI, gJ, gxx);
+      for (int d = 0; d < kSideDirs; d++) gs[d] += gJ[d];
+      for (int c = 0; c < 3; c++) gx[c] -= gxx[c];
+    });
+  } else {
   pairs_in_range<DIM>(n, a.P, k, X, X + n, X + 2 * n, HN, jlo, jhi, [&](int j, double dx, double dy, double dz) {
     const Side<D> Jval = side_at<D>(a.tape, n, j, -1);
     for (int lo = 0; lo < ND; lo += NW) {
@@ -582,6 +603,7 @@ __global__ void __launch_bounds__(kTile) k_r_force_pair(Args a) {
       }
     }
   });
+  }
   if (k >= n) return;
   double* part = a.slices + (size_t)blockIdx.y * ND * n;
   for (int d = 0; d < kSideDirs; d++) part[(size_t)d * n + k] = gs[d];
@@ -790,7 +812,10 @@ static void reverse_step(const Args& a, cudaStream_t st) {
   const int nb = (a.n + kTile - 1) / kTile, np = (a.n + 255) / 256, n64 = (a.n + 63) / 64;
   k_r_correct<<<np, 256, 0, st>>>(a);
   k_r_force_post<DIM><<<n64, 64, 0, st>>>(a);
-  k_r_force_pair<K, DIM><<<dim3(nb, kPairSlices), kTile, 0, st>>>(a);
+  if (a.dual_pairs)
+    k_r_force_pair<K, DIM, true><<<dim3(nb, kPairSlices), kTile, 0, st>>>(a);
+  else
+    k_r_force_pair<K, DIM, false><<<dim3(nb, kPairSlices), kTile, 0, st>>>(a);
   k_r_force_pair_sum<<<np, 256, 0, st>>>(a);
   k_r_cd_post<<<n64, 64, 0, st>>>(a);
   k_r_cd_pair<K, DIM><<<nb, kTile, 0, st>>>(a);
@@ -994,6 +1019,10 @@ int mhd_adjoint_backward(void* ctx, const MhdState* s, int64_t n, int32_t steps,
   a.w = buf + L.w;
   a.g_amax = buf + L.g_amax;
   a.slices = buf + L.slices;
+  {
+    const char* e = getenv("MHD_ADJOINT_DUAL");
+    a.dual_pairs = e && atoi(e) != 0;
+  }
   double* lam_next = buf + L.lam[0];
   double* lam = buf + L.lam[1];
   const int nseg = (steps + every - 1) / every;

@@ -283,6 +283,300 @@ __device__ inline void f_force_pair(const DevParams& P, const Side<D>& I, const 
   }
 }
 
+// The vector-Jacobian product of f_force_pair, written out by hand: given
+// weights w on the 14 differentiated sums (fsum_ptrs order), the gradients
+// of sum_q w_q S_q with respect to the i side (gI), the j side (gJ) and
+// x_ij (gx), each in Side order (h rho p omega cs b3 v3 e alpha psi).  The
+// kernel gradients' own Jacobians come from a 4-direction dual evaluation
+// (x_ij and h).  Derivative conventions follow the dual numbers: sqrt and
+// |.| have zero derivative at 0, max(a, b) passes a's derivative when a >= b.
+template <int K, int DIM>
+__device__ inline void vjp_force_pair(const DevParams& P, const Side<double>& I, const Side<double>& J, double mj,
+                                      const double* x, const double* w, double* gI, double* gJ, double* gx) {
+  const double beta = 2.0, mu0 = P.mu0, ch = P.clean_speed;
+  const double wa6[3] = {w[0], w[1], w[2]}, wa8[3] = {w[3], w[4], w[5]};
+  const double wae6 = w[6], wae9 = w[7], wdiv = w[8];
+  const double wab[3] = {w[9], w[10], w[11]}, wdivbs = w[12], wdivbd = w[13];
+  for (int d = 0; d < kSideDirs; d++) gI[d] = gJ[d] = 0.0;
+  gx[0] = gx[1] = gx[2] = 0.0;
+  // ---- forward values
+  const double r = f_norm(x);
+  double dwi[3], dwj[3];
+  f_kern_grad<K, DIM>(P.norm, x, r, I.h, dwi);
+  f_kern_grad<K, DIM>(P.norm, x, r, J.h, dwj);
+  const double dv[3] = {I.v[0] - J.v[0], I.v[1] - J.v[1], I.v[2] - J.v[2]};
+  const double bi2 = I.b[0] * I.b[0] + I.b[1] * I.b[1] + I.b[2] * I.b[2];
+  const double bj2 = J.b[0] * J.b[0] + J.b[1] * J.b[1] + J.b[2] * J.b[2];
+  const double si = I.cs * I.cs + bi2 / (mu0 * I.rho), sj = J.cs * J.cs + bj2 / (mu0 * J.rho);
+  const double vwi = ::sqrt(si), vwj = ::sqrt(sj);
+  const double rhoij = 0.5 * (I.rho + J.rho);
+  const double pri = I.p / (I.rho * I.rho), prj = J.p / (J.rho * J.rho);
+  const bool near6 = r < kInteractionDistanceEpsilon;
+  double run6[3];
+  for (int a = 0; a < 3; a++) run6[a] = near6 ? 0.0 : x[a] / r;
+  const double dot = dv[0] * run6[0] + dv[1] * run6[1] + dv[2] * run6[2];
+  const double gi6 = I.omega * (run6[0] * dwi[0] + run6[1] * dwi[1] + run6[2] * dwi[2]);
+  const double gj6 = J.omega * (run6[0] * dwj[0] + run6[1] * dwj[1] + run6[2] * dwj[2]);
+  const double dp = I.p - J.p;
+  const double va = ::fabs(dp) / rhoij;
+  const double vsig2 = ::sqrt(va);
+  const bool av = dot < 0.0;
+  const double ti = I.alpha * vwi - beta * dot, tj = J.alpha * vwj - beta * dot;
+  const double vav_i = ti >= 0.0 ? ti : 0.0, vav_j = tj >= 0.0 ? tj : 0.0;
+  const double q_i = -0.5 / I.rho * vav_i * dot * P.av, q_j = -0.5 / J.rho * vav_j * dot * P.av;
+  const double de = I.e - J.e;
+  const double tc = 0.5 * mj / I.rho * gi6 + 0.5 * mj / J.rho * gj6;
+  const double udw = dv[0] * dwi[0] + dv[1] * dwi[1] + dv[2] * dwi[2];
+  const bool far8 = r > kPairDistanceEpsilon;
+  double run8[3];
+  for (int a = 0; a < 3; a++) run8[a] = far8 ? x[a] / r : 0.0;
+  const double gi = I.omega * (run8[0] * dwi[0] + run8[1] * dwi[1] + run8[2] * dwi[2]);
+  const double gj = J.omega * (run8[0] * dwj[0] + run8[1] * dwj[1] + run8[2] * dwj[2]);
+  const double bri[3] = {I.b[0] / I.rho, I.b[1] / I.rho, I.b[2] / I.rho};
+  const double brj[3] = {J.b[0] / J.rho, J.b[1] / J.rho, J.b[2] / J.rho};
+  const double bro2_i = (bri[0] * bri[0] + bri[1] * bri[1] + bri[2] * bri[2]) / mu0;
+  const double bro2_j = (brj[0] * brj[0] + brj[1] * brj[1] + brj[2] * brj[2]) / mu0;
+  const double gradp = mj * (0.5 * bro2_i * gi + 0.5 * bro2_j * gj);
+  const double si8 = bri[0] * run8[0] + bri[1] * run8[1] + bri[2] * run8[2];
+  const double sj8 = brj[0] * run8[0] + brj[1] * run8[1] + brj[2] * run8[2];
+  const double cm = -mj / mu0;
+  const double proj_bi = I.b[0] * run8[0] + I.b[1] * run8[1] + I.b[2] * run8[2];
+  const double proj_bj = J.b[0] * run8[0] + J.b[1] * run8[1] + J.b[2] * run8[2];
+  const double db[3] = {I.b[0] - J.b[0], I.b[1] - J.b[1], I.b[2] - J.b[2]};
+  const double proj_db = db[0] * run8[0] + db[1] * run8[1] + db[2] * run8[2];
+  const double delta_b2 = db[0] * db[0] + db[1] * db[1] + db[2] * db[2];
+  const double ri2 = 1.0 / (I.rho * I.rho), rj2 = 1.0 / (J.rho * J.rho);
+  const double pgi = mj * ri2 * gi, pgj = mj * rj2 * gj;
+  const double d_brho = -(pgi * proj_bi);
+  const double projv = dv[0] * run8[0] + dv[1] * run8[1] + dv[2] * run8[2];
+  const double dvt[3] = {dv[0] - projv * run8[0], dv[1] - projv * run8[1], dv[2] - projv * run8[2]};
+  const double vsig_b = f_norm(dvt);
+  const double d_diss = 0.5 * (pgi + pgj) * vsig_b * P.ar;
+  const double dpsi = pgi * I.psi * (ch * vwi) + pgj * J.psi * (ch * vwj);
+  // ---- reverse
+  double r_ = 0.0, dwi_[3] = {}, dwj_[3] = {}, dv_[3] = {}, run6_[3] = {}, run8_[3] = {};
+  double vwi_ = 0.0, vwj_ = 0.0, gi_ = 0.0, gj_ = 0.0, gi6_ = 0.0, gj6_ = 0.0, dot_ = 0.0;
+  double Ib_[3] = {}, Jb_[3] = {};
+  // G9
+  double proj_db_ = wdivbd * (-mj * gi);
+  gi_ += wdivbd * (-mj * proj_db);
+  double pgi_ = wdivbs * proj_bi, pgj_ = wdivbs * proj_bj;
+  double proj_bi_ = wdivbs * pgi, proj_bj_ = wdivbs * pgj;
+  double delta_b2_ = wae9 * (-0.5 * d_diss / mu0);
+  double d_diss_ = wae9 * (-0.5 * delta_b2 / mu0);
+  double d_brho_ = 0.0, dpsi_ = 0.0, db_[3] = {};
+  for (int a = 0; a < 3; a++) {
+    d_brho_ += wab[a] * dv[a];
+    dv_[a] += wab[a] * d_brho;
+    d_diss_ += wab[a] * db[a];
+    db_[a] += wab[a] * d_diss;
+    dpsi_ -= wab[a] * run8[a];
+    run8_[a] -= wab[a] * dpsi;
+  }
+  pgi_ += dpsi_ * I.psi * ch * vwi;
+  gI[13] += dpsi_ * pgi * ch * vwi;
+  vwi_ += dpsi_ * pgi * I.psi * ch;
+  pgj_ += dpsi_ * J.psi * ch * vwj;
+  gJ[13] += dpsi_ * pgj * ch * vwj;
+  vwj_ += dpsi_ * pgj * J.psi * ch;
+  pgi_ += d_diss_ * 0.5 * vsig_b * P.ar;
+  pgj_ += d_diss_ * 0.5 * vsig_b * P.ar;
+  const double vsig_b_ = d_diss_ * 0.5 * (pgi + pgj) * P.ar;
+  double dvt_[3];
+  for (int a = 0; a < 3; a++) dvt_[a] = vsig_b > 0.0 ? vsig_b_ * dvt[a] / vsig_b : 0.0;
+  double projv_ = 0.0;
+  for (int a = 0; a < 3; a++) {
+    dv_[a] += dvt_[a];
+    projv_ -= dvt_[a] * run8[a];
+    run8_[a] -= dvt_[a] * projv;
+  }
+  for (int a = 0; a < 3; a++) {
+    dv_[a] += projv_ * run8[a];
+    run8_[a] += projv_ * dv[a];
+  }
+  pgi_ -= d_brho_ * proj_bi;
+  proj_bi_ -= d_brho_ * pgi;
+  const double ri2_ = pgi_ * mj * gi, rj2_ = pgj_ * mj * gj;
+  gi_ += pgi_ * mj * ri2;
+  gj_ += pgj_ * mj * rj2;
+  gI[1] += ri2_ * (-2.0 * ri2 / I.rho);
+  gJ[1] += rj2_ * (-2.0 * rj2 / J.rho);
+  for (int a = 0; a < 3; a++) {
+    db_[a] += delta_b2_ * 2.0 * db[a] + proj_db_ * run8[a];
+    run8_[a] += proj_db_ * db[a] + proj_bi_ * I.b[a] + proj_bj_ * J.b[a];
+    Ib_[a] += db_[a] + proj_bi_ * run8[a];
+    Jb_[a] += -db_[a] + proj_bj_ * run8[a];
+  }
+  // G8
+  double gradp_ = 0.0, si8_ = 0.0, sj8_ = 0.0, bri_[3] = {}, brj_[3] = {};
+  for (int a = 0; a < 3; a++) {
+    const double pia = cm * bri[a] * si8, pja = cm * brj[a] * sj8;
+    run8_[a] -= wa8[a] * gradp;
+    gradp_ -= wa8[a] * run8[a];
+    const double pia_ = -wa8[a] * gi, pja_ = -wa8[a] * gj;
+    gi_ -= wa8[a] * pia;
+    gj_ -= wa8[a] * pja;
+    bri_[a] += pia_ * cm * si8;
+    si8_ += pia_ * cm * bri[a];
+    brj_[a] += pja_ * cm * sj8;
+    sj8_ += pja_ * cm * brj[a];
+  }
+  for (int b = 0; b < 3; b++) {
+    bri_[b] += si8_ * run8[b];
+    run8_[b] += si8_ * bri[b] + sj8_ * brj[b];
+    brj_[b] += sj8_ * run8[b];
+  }
+  const double bro2_i_ = gradp_ * 0.5 * mj * gi, bro2_j_ = gradp_ * 0.5 * mj * gj;
+  gi_ += gradp_ * 0.5 * mj * bro2_i;
+  gj_ += gradp_ * 0.5 * mj * bro2_j;
+  for (int a = 0; a < 3; a++) {
+    bri_[a] += bro2_i_ * 2.0 * bri[a] / mu0;
+    brj_[a] += bro2_j_ * 2.0 * brj[a] / mu0;
+    Ib_[a] += bri_[a] / I.rho;
+    gI[1] -= bri_[a] * bri[a] / I.rho;
+    Jb_[a] += brj_[a] / J.rho;
+    gJ[1] -= brj_[a] * brj[a] / J.rho;
+  }
+  // gi, gj (run8 path)
+  gI[3] += gi_ * (run8[0] * dwi[0] + run8[1] * dwi[1] + run8[2] * dwi[2]);
+  gJ[3] += gj_ * (run8[0] * dwj[0] + run8[1] * dwj[1] + run8[2] * dwj[2]);
+  for (int a = 0; a < 3; a++) {
+    run8_[a] += gi_ * I.omega * dwi[a] + gj_ * J.omega * dwj[a];
+    dwi_[a] += gi_ * I.omega * run8[a];
+    dwj_[a] += gj_ * J.omega * run8[a];
+  }
+  if (far8)
+    for (int a = 0; a < 3; a++) {
+      gx[a] += run8_[a] / r;
+      r_ -= run8_[a] * x[a] / (r * r);
+    }
+  // G6: conduction, pressure, viscosity, divergence
+  {
+    const double T_ = wae6 * P.ac * vsig2 * de;
+    const double vsig2_ = wae6 * P.ac * de * tc;
+    gI[11] += wae6 * P.ac * vsig2 * tc;
+    gJ[11] -= wae6 * P.ac * vsig2 * tc;
+    gI[1] -= T_ * 0.5 * mj * gi6 / (I.rho * I.rho);
+    gi6_ += T_ * 0.5 * mj / I.rho;
+    gJ[1] -= T_ * 0.5 * mj * gj6 / (J.rho * J.rho);
+    gj6_ += T_ * 0.5 * mj / J.rho;
+    const double va_ = va > 0.0 ? vsig2_ * 0.5 / vsig2 : 0.0;
+    const double sgn = dp > 0.0 ? 1.0 : (dp < 0.0 ? -1.0 : 0.0);
+    gI[2] += va_ * sgn / rhoij;
+    gJ[2] -= va_ * sgn / rhoij;
+    const double rhoij_ = -va_ * va / rhoij;
+    gI[1] += 0.5 * rhoij_;
+    gJ[1] += 0.5 * rhoij_;
+  }
+  double pri_ = wae6 * mj * I.omega * udw;
+  gI[3] += wae6 * mj * pri * udw;
+  {
+    const double udw_ = wae6 * mj * pri * I.omega;
+    for (int a = 0; a < 3; a++) {
+      dv_[a] += udw_ * dwi[a];
+      dwi_[a] += udw_ * dv[a];
+    }
+  }
+  double prj_ = 0.0;
+  for (int a = 0; a < 3; a++) {
+    pri_ -= wa6[a] * mj * I.omega * dwi[a];
+    gI[3] -= wa6[a] * mj * pri * dwi[a];
+    dwi_[a] -= wa6[a] * mj * pri * I.omega;
+    prj_ -= wa6[a] * mj * J.omega * dwj[a];
+    gJ[3] -= wa6[a] * mj * prj * dwj[a];
+    dwj_[a] -= wa6[a] * mj * prj * J.omega;
+  }
+  if (av) {
+    double q_i_ = wae6 * mj * dot * gi6;
+    dot_ += wae6 * mj * q_i * gi6;
+    gi6_ += wae6 * mj * q_i * dot;
+    double q_j_ = 0.0;
+    for (int a = 0; a < 3; a++) {
+      q_i_ -= wa6[a] * mj * I.omega * dwi[a];
+      gI[3] -= wa6[a] * mj * q_i * dwi[a];
+      dwi_[a] -= wa6[a] * mj * q_i * I.omega;
+      q_j_ -= wa6[a] * mj * J.omega * dwj[a];
+      gJ[3] -= wa6[a] * mj * q_j * dwj[a];
+      dwj_[a] -= wa6[a] * mj * q_j * J.omega;
+    }
+    gI[1] += q_i_ * 0.5 / (I.rho * I.rho) * vav_i * dot * P.av;
+    gJ[1] += q_j_ * 0.5 / (J.rho * J.rho) * vav_j * dot * P.av;
+    const double vav_i_ = q_i_ * (-0.5 / I.rho * dot * P.av), vav_j_ = q_j_ * (-0.5 / J.rho * dot * P.av);
+    dot_ += q_i_ * (-0.5 / I.rho * vav_i * P.av) + q_j_ * (-0.5 / J.rho * vav_j * P.av);
+    if (ti >= 0.0) {
+      gI[12] += vav_i_ * vwi;
+      vwi_ += vav_i_ * I.alpha;
+      dot_ -= beta * vav_i_;
+    }
+    if (tj >= 0.0) {
+      gJ[12] += vav_j_ * vwj;
+      vwj_ += vav_j_ * J.alpha;
+      dot_ -= beta * vav_j_;
+    }
+  }
+  dot_ += wdiv * mj * gi6;
+  gi6_ += wdiv * mj * dot;
+  gI[3] += gi6_ * (run6[0] * dwi[0] + run6[1] * dwi[1] + run6[2] * dwi[2]);
+  gJ[3] += gj6_ * (run6[0] * dwj[0] + run6[1] * dwj[1] + run6[2] * dwj[2]);
+  for (int a = 0; a < 3; a++) {
+    run6_[a] += gi6_ * I.omega * dwi[a] + gj6_ * J.omega * dwj[a] + dot_ * dv[a];
+    dwi_[a] += gi6_ * I.omega * run6[a];
+    dwj_[a] += gj6_ * J.omega * run6[a];
+    dv_[a] += dot_ * run6[a];
+  }
+  if (!near6)
+    for (int a = 0; a < 3; a++) {
+      gx[a] += run6_[a] / r;
+      r_ -= run6_[a] * x[a] / (r * r);
+    }
+  gI[2] += pri_ / (I.rho * I.rho);
+  gI[1] -= pri_ * 2.0 * I.p / (I.rho * I.rho * I.rho);
+  gJ[2] += prj_ / (J.rho * J.rho);
+  gJ[1] -= prj_ * 2.0 * J.p / (J.rho * J.rho * J.rho);
+  // wave speeds
+  {
+    const double si_ = si > 0.0 ? vwi_ * 0.5 / vwi : 0.0, sj_ = sj > 0.0 ? vwj_ * 0.5 / vwj : 0.0;
+    gI[4] += si_ * 2.0 * I.cs;
+    gJ[4] += sj_ * 2.0 * J.cs;
+    const double bi2_ = si_ / (mu0 * I.rho), bj2_ = sj_ / (mu0 * J.rho);
+    gI[1] -= si_ * bi2 / (mu0 * I.rho * I.rho);
+    gJ[1] -= sj_ * bj2 / (mu0 * J.rho * J.rho);
+    for (int a = 0; a < 3; a++) {
+      Ib_[a] += bi2_ * 2.0 * I.b[a];
+      Jb_[a] += bj2_ * 2.0 * J.b[a];
+    }
+  }
+  for (int a = 0; a < 3; a++) {
+    gI[5 + a] += Ib_[a];
+    gJ[5 + a] += Jb_[a];
+    gI[8 + a] += dv_[a];
+    gJ[8 + a] -= dv_[a];
+  }
+  // kernel gradients: Jacobians in x_ij and h from a dual evaluation
+  {
+    using D4 = Dual<4>;
+    D4 xd[3];
+    for (int a = 0; a < 3; a++) {
+      xd[a] = D4(x[a]);
+      xd[a].d[a] = 1.0;
+    }
+    const D4 rd = f_norm(xd);
+    D4 hi(I.h), hj(J.h);
+    hi.d[3] = 1.0;
+    hj.d[3] = 1.0;
+    D4 gdi[3], gdj[3];
+    f_kern_grad<K, DIM>(P.norm, xd, rd, hi, gdi);
+    f_kern_grad<K, DIM>(P.norm, xd, rd, hj, gdj);
+    for (int a = 0; a < 3; a++) {
+      for (int b = 0; b < 3; b++) gx[b] += dwi_[a] * gdi[a].d[b] + dwj_[a] * gdj[a].d[b];
+      gI[0] += dwi_[a] * gdi[a].d[3];
+      gJ[0] += dwj_[a] * gdj[a].d[3];
+    }
+  }
+  if (r > 0.0)
+    for (int a = 0; a < 3; a++) gx[a] += r_ * x[a] / r;
+}
+
 // Outputs of the force groups' post loops and G10.
 template <class D>
 struct FOut {

@@ -87,3 +87,35 @@ def test_autograd_function_gradient():
     assert abs(float(loss.detach()) - value) <= 1e-12 * abs(value)
     assert abs(float(a.grad) - grad[0]) <= 1e-9 * abs(grad[0])
     assert float(am.grad) == grad[1] == 0.0
+
+
+def test_hand_written_pair_vjp_equals_dual_jacobian(monkeypatch):
+    # the reverse force-pair pass by the hand-written VJP (default) and by
+    # contracting dual-number Jacobians (MHD_ADJOINT_DUAL=1): every lambda
+    # of the initial state agrees to roundoff
+    from src.derivative import AdjointEngine, TangentEngine, TangentState
+    from src.engine import params_from_dict
+
+    ic, prm = sc_.blast_3d(8, "cubic", seed=5, alpha=(0.1, 0.6))
+    params = params_from_dict(dict(prm, density="single"))
+    te = TangentEngine(params, TangentState(dict(ic), {"e": [0.01 * ic["e"], None]}), alpha_max_seed=[0.0, 1.0])
+    te.warmup()
+    ae = AdjointEngine(params, te.ts.n)
+    values = {f: te.ts[f][:, 0].contiguous() for f in ae.fields}
+    values["m"] = te.ts["m"][:, 0].contiguous()
+    values["itype"] = te.ts["itype"]
+    steps, every = 5, 2
+    _, used, cps = ae.forward(values, steps, [te.initial_dt()] + [-1.0] * (steps - 1), every)
+    out = {}
+    for mode in ("0", "1"):
+        monkeypatch.setenv("MHD_ADJOINT_DUAL", mode)
+        lam, dam = ae.backward(values, steps, used, every, cps)
+        out[mode] = (lam.clone(), dam)
+    ae.close()
+    te.close()
+    a, b = out["0"][0], out["1"][0]
+    assert float(torch.linalg.norm(b)) > 0.0
+    for f in range(a.shape[0]):
+        scale = max(float(torch.linalg.norm(b[f])), 1e-300)
+        assert float(torch.linalg.norm(a[f] - b[f])) <= 1e-11 * max(scale, 1e-12 * float(torch.linalg.norm(b))), f
+    assert abs(out["0"][1] - out["1"][1]) <= 1e-11 * max(abs(out["1"][1]), 1e-300)
