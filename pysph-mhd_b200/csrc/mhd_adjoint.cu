@@ -125,7 +125,7 @@ struct Args {
   const double* s_final;   // reverse, last step: S_K (loss terms)
   double* dta_out;         // forward: dt_adapt of the step (adaptive step sizes)
   double* slices;          // reverse: per-slice partial sums of the force pair pass
-  int dual_pairs;          // reverse: force pair VJPs from dual Jacobians (check path) instead of by hand
+  int dual_pairs;          // reverse: force and CD pair VJPs from dual Jacobians (check path) instead of by hand
 };
 
 #define TP(k, i) a.tape_w[(size_t)(k) * a.n + (i)]
@@ -649,7 +649,7 @@ __global__ void __launch_bounds__(64) k_r_cd_post(Args a) {
 }
 
 // Cullen-Dehnen pair terms reversed (gather form, as the force pairs).
-template <int K, int DIM>
+template <int K, int DIM, bool DUAL>
 __global__ void __launch_bounds__(kTile) k_r_cd_pair(Args a) {
   using D = Dual<10>;  // x_ij 3, h_i, dv 3, da 3
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -663,23 +663,35 @@ __global__ void __launch_bounds__(kTile) k_r_cd_pair(Args a) {
       // side 0: pair (k, j); side 1: pair (j, k)
       const int ii = side ? j : kk, jj = side ? kk : j;
       const double sgn = side ? -1.0 : 1.0;
-      const D xij[3] = {seeded<10>(sgn * dx, 0), seeded<10>(sgn * dy, 1), seeded<10>(sgn * dz, 2)};
-      const D hi = seeded<10>(HN[ii], side ? -1 : 3);
-      D dv[3], da[3];
+      const double xv[3] = {sgn * dx, sgn * dy, sgn * dz};
+      double dvv[3], dav[3];
       for (int c = 0; c < 3; c++) {
-        dv[c] = seeded<10>(TR(T_VP + c, ii) - TR(T_VP + c, jj), 4 + c);
-        da[c] = seeded<10>(TR(T_S + SA + c, ii) - TR(T_S + SA + c, jj), 7 + c);
+        dvv[c] = TR(T_VP + c, ii) - TR(T_VP + c, jj);
+        dav[c] = TR(T_S + SA + c, ii) - TR(T_S + SA + c, jj);
       }
-      D r[6], vv[9], aa[9];
-      for (int q = 0; q < 6; q++) r[q] = D(0.0);
-      for (int q = 0; q < 9; q++) vv[q] = aa[q] = D(0.0);
-      f_cd_pair<K, DIM>(a.P.norm, xij, hi, D(a.m[jj]), dv, da, r, vv, aa);
       double g[10] = {};
-      for (int d = 0; d < 10; d++) {
-        double s = 0.0;
-        for (int q = 0; q < 6; q++) s += W(M_CD + q, ii) * r[q].d[d];
-        for (int q = 0; q < 9; q++) s += W(M_CD + 6 + q, ii) * vv[q].d[d] + W(M_CD + 15 + q, ii) * aa[q].d[d];
-        g[d] = s;
+      if constexpr (DUAL) {
+        const D xij[3] = {seeded<10>(xv[0], 0), seeded<10>(xv[1], 1), seeded<10>(xv[2], 2)};
+        const D hi = seeded<10>(HN[ii], side ? -1 : 3);
+        D dv[3], da[3];
+        for (int c = 0; c < 3; c++) {
+          dv[c] = seeded<10>(dvv[c], 4 + c);
+          da[c] = seeded<10>(dav[c], 7 + c);
+        }
+        D r[6], vv[9], aa[9];
+        for (int q = 0; q < 6; q++) r[q] = D(0.0);
+        for (int q = 0; q < 9; q++) vv[q] = aa[q] = D(0.0);
+        f_cd_pair<K, DIM>(a.P.norm, xij, hi, D(a.m[jj]), dv, da, r, vv, aa);
+        for (int d = 0; d < 10; d++) {
+          double s = 0.0;
+          for (int q = 0; q < 6; q++) s += W(M_CD + q, ii) * r[q].d[d];
+          for (int q = 0; q < 9; q++) s += W(M_CD + 6 + q, ii) * vv[q].d[d] + W(M_CD + 15 + q, ii) * aa[q].d[d];
+          g[d] = s;
+        }
+      } else {
+        double w[24];
+        for (int q = 0; q < 24; q++) w[q] = W(M_CD + q, ii);
+        vjp_cd_pair<K, DIM>(a.P.norm, xv, HN[ii], a.m[jj], dvv, dav, w, g);
       }
       for (int c = 0; c < 3; c++) {
         gx[c] += sgn * g[c];
@@ -818,7 +830,10 @@ static void reverse_step(const Args& a, cudaStream_t st) {
     k_r_force_pair<K, DIM, false><<<dim3(nb, kPairSlices), kTile, 0, st>>>(a);
   k_r_force_pair_sum<<<np, 256, 0, st>>>(a);
   k_r_cd_post<<<n64, 64, 0, st>>>(a);
-  k_r_cd_pair<K, DIM><<<nb, kTile, 0, st>>>(a);
+  if (a.dual_pairs)
+    k_r_cd_pair<K, DIM, true><<<nb, kTile, 0, st>>>(a);
+  else
+    k_r_cd_pair<K, DIM, false><<<nb, kTile, 0, st>>>(a);
   k_r_prologue<DIM><<<np, 256, 0, st>>>(a);
   k_r_density_post<DIM><<<np, 256, 0, st>>>(a);
   k_r_density_pair<K, DIM><<<nb, kTile, 0, st>>>(a);

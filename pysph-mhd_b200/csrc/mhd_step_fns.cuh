@@ -156,6 +156,52 @@ __device__ inline D f_cd_post(const D* r, const D* vv, const D* aa, const D& ome
   return pmax(pmin(source / (cs * cs), alpha_max), D(alpha_min));
 }
 
+// The vector-Jacobian product of f_cd_pair, written out by hand: weights w
+// on its 24 sums (r 6, vv 9, aa 9) give g over (x_ij 3, h_i, dv 3, da 3);
+// the kernel gradient's Jacobian comes from a 4-direction dual evaluation.
+template <int K, int DIM>
+__device__ inline void vjp_cd_pair(double norm, const double* x, double hi, double mj, const double* dv,
+                                   const double* da, const double* w, double* g) {
+  const double r = f_norm(x);
+  double dwi[3];
+  f_kern_grad<K, DIM>(norm, x, r, hi, dwi);
+  const double run[3] = {mj * dwi[0], mj * dwi[1], mj * dwi[2]};
+  double run_[3] = {}, x_[3] = {};
+  // r[6] = -x_a run_b over (0,0) (0,1) (0,2) (1,1) (1,2) (2,2)
+  const int ra[6] = {0, 0, 0, 1, 1, 2}, rb[6] = {0, 1, 2, 1, 2, 2};
+  for (int q = 0; q < 6; q++) {
+    run_[rb[q]] -= w[q] * x[ra[q]];
+    x_[ra[q]] -= w[q] * run[rb[q]];
+  }
+  for (int a = 0; a < 3; a++) {
+    double dv_ = 0.0, da_ = 0.0;
+    for (int b = 0; b < 3; b++) {
+      dv_ += w[6 + 3 * a + b] * run[b];
+      da_ += w[15 + 3 * a + b] * run[b];
+      run_[b] += w[6 + 3 * a + b] * dv[a] + w[15 + 3 * a + b] * da[a];
+    }
+    g[4 + a] = dv_;
+    g[7 + a] = da_;
+  }
+  using D4 = Dual<4>;
+  D4 xd[3];
+  for (int a = 0; a < 3; a++) {
+    xd[a] = D4(x[a]);
+    xd[a].d[a] = 1.0;
+  }
+  D4 hd(hi);
+  hd.d[3] = 1.0;
+  D4 gd[3];
+  f_kern_grad<K, DIM>(norm, xd, f_norm(xd), hd, gd);
+  g[3] = 0.0;
+  for (int a = 0; a < 3; a++) g[a] = x_[a];
+  for (int b = 0; b < 3; b++) {
+    const double dwi_ = mj * run_[b];
+    for (int a = 0; a < 3; a++) g[a] += dwi_ * gd[b].d[a];
+    g[3] += dwi_ * gd[b].d[3];
+  }
+}
+
 // ------------------------------------------------- G6-G10 force groups
 // The per-particle inputs of the force pair loop.
 template <class D>

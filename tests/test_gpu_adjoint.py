@@ -90,9 +90,10 @@ def test_autograd_function_gradient():
 
 
 def test_hand_written_pair_vjp_equals_dual_jacobian(monkeypatch):
-    # the reverse force-pair pass by the hand-written VJP (default) and by
-    # contracting dual-number Jacobians (MHD_ADJOINT_DUAL=1): every lambda
-    # of the initial state agrees to roundoff
+    # the reverse force-pair and Cullen-Dehnen pair passes by the
+    # hand-written VJPs (default) and by contracting dual-number Jacobians
+    # (MHD_ADJOINT_DUAL=1): every lambda of the initial state agrees to
+    # roundoff
     from src.derivative import AdjointEngine, TangentEngine, TangentState
     from src.engine import params_from_dict
 
