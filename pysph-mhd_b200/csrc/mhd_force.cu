@@ -180,8 +180,13 @@ __global__ void __launch_bounds__(kForceShapes[SHAPE][0], kForceShapes[SHAPE][1]
     cif = R.cellc[i];
   }
   const float Rf = P.Rf;
+  // the list entry is fetched one pair ahead, and every record of a pair is
+  // requested before its neighbour test, so a pair waits on one memory
+  // round trip instead of three (entry, position, records)
+  int jn = cnt > 0 ? row[0] : i;
   for (int k = 0; k < cnt; k++) {
-    const int j = row[k * 32];
+    const int j = jn;
+    if (k + 1 < cnt) jn = row[(k + 1) * 32];
     if (j == i) {
       // the self pair: every sum term carries a zero kernel gradient or a
       // zero displacement; only the signal speed max(vw_i - 2 dot, 0) = vw_i
@@ -189,6 +194,8 @@ __global__ void __launch_bounds__(kForceShapes[SHAPE][0], kForceShapes[SHAPE][1]
       dtc = fmax(dtc, vwi);
       continue;
     }
+    const V4<T> j0 = ld4(R.r[0] + j), j1 = ld4(R.r[1] + j), j2 = ld4(R.r[2] + j), j3 = ld4(R.r[3] + j);
+    const V4<T> j4 = ld4(R.r[4] + j), j5 = ld4(R.r[5] + j);
     T dx, dy, dz, r, inv_r0;
     if constexpr (sizeof(T) == 4) {
       // FP32 geometry from the packed positions; FP32 neighbour test
@@ -213,8 +220,6 @@ __global__ void __launch_bounds__(kForceShapes[SHAPE][0], kForceShapes[SHAPE][1]
       r = sqrt(r2d);
       inv_r0 = 0;
     }
-    const V4<T> j0 = ld4(R.r[0] + j), j1 = ld4(R.r[1] + j), j2 = ld4(R.r[2] + j), j3 = ld4(R.r[3] + j);
-    const V4<T> j4 = ld4(R.r[4] + j), j5 = ld4(R.r[5] + j);
     const T mj = j0.x, rhoj = j0.y, irhoj = j0.z, omegaj = j0.w;
     const T h1j = j3.w;
     // DWI = ti * XIJ, DWJ = tj * XIJ (zero at r <= 1e-12)

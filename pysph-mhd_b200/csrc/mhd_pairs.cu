@@ -81,8 +81,12 @@ __device__ __forceinline__ bool density_particle(int i, const DevParams& P, cons
     const float rh = (float)P.R * (float)hi;
     rhi2f = rh * rh;
   }
+  // the list entry is fetched one pair ahead, so a pair waits on one memory
+  // round trip (its record) instead of two
+  int jn = cnt > 0 ? row[0] : i;
   for (int k = 0; k < cnt; k++) {
-    const int j = row[k * 32];
+    const int j = jn;
+    if (k + 1 < cnt) jn = row[(k + 1) * 32];
     T r, mj;
     bool nb;
     if constexpr (sizeof(T) == 4) {
@@ -98,6 +102,7 @@ __device__ __forceinline__ bool density_particle(int i, const DevParams& P, cons
       }
       r = r2 > 0.f ? r2 * rsqrtf(r2) : 0.f;
     } else {
+      mj = m[j];  // requested with the position, before the neighbour test
       const double dx = min_image(xi - x[j], G.L[0], G.half[0], G.periodic[0]);
       const double dy = min_image(yi - y[j], G.L[1], G.half[1], G.periodic[1]);
       const double dz = DIM == 3 ? min_image(zi - z[j], G.L[2], G.half[2], G.periodic[2]) : 0.0;
@@ -112,7 +117,6 @@ __device__ __forceinline__ bool density_particle(int i, const DevParams& P, cons
       const T q = r * h1;
       T w, dw;
       w_dw<K>(q, DIM, w, dw);
-      if constexpr (sizeof(T) == 8) mj = m[j];
       rs.add(mj * (w * fac));
       ds.add(mj * (fgh * (dw * q + w * (T)DIM)));
     }
