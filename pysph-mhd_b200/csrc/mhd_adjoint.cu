@@ -54,12 +54,15 @@ __device__ inline void all_pairs(int n, const DevParams& P, int i, const double*
   const bool active = i < n;
   const double xi = active ? x[i] : 0.0, yi = active ? y[i] : 0.0, zi = active && DIM == 3 ? z[i] : 0.0;
   const double rhi2 = active ? rh2_exact(P.R, h[i]) : 0.0;
+  const PairBox wb = warp_pair_box<DIM>(active, xi, yi, zi, active ? h[i] : 0.0);
   for (int base = 0; base < n; base += kTile) {
     const int j = base + threadIdx.x;
     if (j < n) sh[threadIdx.x] = make_double4(x[j], y[j], DIM == 3 ? z[j] : 0.0, h[j]);
     __syncthreads();
-    if (active) {
-      const int m = n - base < kTile ? n - base : kTile;
+    const int m = n - base < kTile ? n - base : kTile;
+    // every lane takes part in the tile box's warp reductions
+    const PairBox tb = tile_pair_box<DIM, kTile>(sh, m);
+    if (active && !pair_boxes_apart<DIM>(wb, tb, P.R, P.L, P.periodic)) {
       for (int t = 0; t < m; t++) {
         const double4 q = sh[t];
         const double dx = min_image(xi - q.x, P.L[0], P.half[0], P.periodic[0]);
@@ -81,12 +84,15 @@ __device__ inline void pairs_in_range(int n, const DevParams& P, int i, const do
   const bool active = i < n;
   const double xi = active ? x[i] : 0.0, yi = active ? y[i] : 0.0, zi = active && DIM == 3 ? z[i] : 0.0;
   const double rhi2 = active ? rh2_exact(P.R, h[i]) : 0.0;
+  const PairBox wb = warp_pair_box<DIM>(active, xi, yi, zi, active ? h[i] : 0.0);
   for (int base = jlo; base < jhi; base += kTile) {
     const int j = base + threadIdx.x;
     if (j < jhi) shr[threadIdx.x] = make_double4(x[j], y[j], DIM == 3 ? z[j] : 0.0, h[j]);
     __syncthreads();
-    if (active) {
-      const int m = jhi - base < kTile ? jhi - base : kTile;
+    const int m = jhi - base < kTile ? jhi - base : kTile;
+    // every lane takes part in the tile box's warp reductions
+    const PairBox tb = tile_pair_box<DIM, kTile>(shr, m);
+    if (active && !pair_boxes_apart<DIM>(wb, tb, P.R, P.L, P.periodic)) {
       for (int t = 0; t < m; t++) {
         const double4 q = shr[t];
         const double dx = min_image(xi - q.x, P.L[0], P.half[0], P.periodic[0]);

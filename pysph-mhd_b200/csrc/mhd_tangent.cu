@@ -83,12 +83,15 @@ __device__ inline void all_pairs(int n, const DevParams& P, int i, const MhdStat
   const double xi = active ? X[i].v : 0.0, yi = active ? Y[i].v : 0.0;
   const double zi = active && DIM == 3 ? Z[i].v : 0.0;
   const double rhi2 = active ? rh2_exact(P.R, H[i].v) : 0.0;
+  const PairBox wb = warp_pair_box<DIM>(active, xi, yi, zi, active ? H[i].v : 0.0);
   for (int base = 0; base < n; base += kTile) {
     const int j = base + threadIdx.x;
     if (j < n) sh[threadIdx.x] = make_double4(X[j].v, Y[j].v, DIM == 3 ? Z[j].v : 0.0, H[j].v);
     __syncthreads();
-    if (active) {
-      const int m = n - base < kTile ? n - base : kTile;
+    const int m = n - base < kTile ? n - base : kTile;
+    // every lane takes part in the tile box's warp reductions
+    const PairBox tb = tile_pair_box<DIM, kTile>(sh, m);
+    if (active && !pair_boxes_apart<DIM>(wb, tb, P.R, P.L, P.periodic)) {
       for (int t = 0; t < m; t++) {
         const double4 q = sh[t];
         const double dx = min_image(xi - q.x, P.L[0], P.half[0], P.periodic[0]);
