@@ -76,23 +76,30 @@ __device__ inline void all_pairs(int n, const DevParams& P, int i, const double*
   }
 }
 
-// all_pairs over the candidates jlo .. jhi - 1 only (a slice of them).
+// all_pairs over one slice of the candidate tiles: the tiles within reach
+// of the warp (in ascending order) are dealt round robin to `slices`
+// slices and this call visits those of slice `slice`, so the pairs of a
+// warp spread evenly over the slices wherever its neighbours lie in the
+// index order.  Which tiles are within reach is warp-uniform (the box
+// reductions give every lane the same values).
 template <int DIM, class F>
-__device__ inline void pairs_in_range(int n, const DevParams& P, int i, const double* x, const double* y,
-                                      const double* z, const double* h, int jlo, int jhi, F&& f) {
+__device__ inline void pairs_in_slice(int n, const DevParams& P, int i, const double* x, const double* y,
+                                      const double* z, const double* h, int slice, int slices, F&& f) {
   __shared__ double4 shr[kTile];
   const bool active = i < n;
   const double xi = active ? x[i] : 0.0, yi = active ? y[i] : 0.0, zi = active && DIM == 3 ? z[i] : 0.0;
   const double rhi2 = active ? rh2_exact(P.R, h[i]) : 0.0;
   const PairBox wb = warp_pair_box<DIM>(active, xi, yi, zi, active ? h[i] : 0.0);
-  for (int base = jlo; base < jhi; base += kTile) {
+  int near = 0;  // tiles within reach of the warp so far
+  for (int base = 0; base < n; base += kTile) {
     const int j = base + threadIdx.x;
-    if (j < jhi) shr[threadIdx.x] = make_double4(x[j], y[j], DIM == 3 ? z[j] : 0.0, h[j]);
+    if (j < n) shr[threadIdx.x] = make_double4(x[j], y[j], DIM == 3 ? z[j] : 0.0, h[j]);
     __syncthreads();
-    const int m = jhi - base < kTile ? jhi - base : kTile;
+    const int m = n - base < kTile ? n - base : kTile;
     // every lane takes part in the tile box's warp reductions
     const PairBox tb = tile_pair_box<DIM, kTile>(shr, m);
-    if (active && !pair_boxes_apart<DIM>(wb, tb, P.R, P.L, P.periodic)) {
+    const bool mine = !pair_boxes_apart<DIM>(wb, tb, P.R, P.L, P.periodic) && near++ % slices == slice;
+    if (active && mine) {
       for (int t = 0; t < m; t++) {
         const double4 q = shr[t];
         const double dx = min_image(xi - q.x, P.L[0], P.half[0], P.periodic[0]);
@@ -529,9 +536,10 @@ __device__ inline void add_side(const Args& a, int i, const double* g, double si
 // through its j side and x_k.  The kSideDirs + 3 input directions are
 // evaluated a window of kForceWindow at a time, so the dual sums a thread
 // holds stay small (the same derivatives as one pass over all directions).
-// The candidates are split into kPairSlices slices (grid y), so that a
-// small particle count still fills the GPU; each slice writes its partial
-// sums and k_r_force_pair_sum adds them in slice order (deterministic).
+// The candidate tiles within reach of a warp are dealt to kPairSlices
+// slices (grid y, pairs_in_slice), so that a small particle count still
+// fills the GPU; each slice writes its partial sums and k_r_force_pair_sum
+// adds them in slice order (deterministic).
 constexpr int kForceWindow = 6;
 constexpr int kPairSlices = 8;
 constexpr int kForceDirs = kSideDirs + 3;
@@ -545,13 +553,11 @@ __global__ void __launch_bounds__(kTile) k_r_force_pair(Args a) {
   const double* X = a.tape + (size_t)T_X * n;
   const double* HN = a.tape + (size_t)T_HN * n;
   const int kk = k < n ? k : 0;
-  const int chunk = (n + kPairSlices * kTile - 1) / (kPairSlices * kTile) * kTile;
-  const int jlo = blockIdx.y * chunk, jhi = jlo + chunk < n ? jlo + chunk : n;
   double gs[kSideDirs] = {}, gx[3] = {};
   if constexpr (!DUAL) {
     // hand-written VJP (vjp_force_pair)
     const Side<double> Kv = side_values(a.tape, n, kk);
-    pairs_in_range<DIM>(n, a.P, k, X, X + n, X + 2 * n, HN, jlo, jhi, [&](int j, double dx, double dy, double dz) {
+    pairs_in_slice<DIM>(n, a.P, k, X, X + n, X + 2 * n, HN, blockIdx.y, kPairSlices, [&](int j, double dx, double dy, double dz) {
       const Side<double> Jv = side_values(a.tape, n, j);
       double w[kFSumDirs], gI[kSideDirs], gJ[kSideDirs], gxx[3];
       // (k, j): k is the i side
@@ -568,7 +574,7 @@ __global__ void __launch_bounds__(kTile) k_r_force_pair(Args a) {
       for (int c = 0; c < 3; c++) gx[c] -= gxx[c];
     });
   } else {
-  pairs_in_range<DIM>(n, a.P, k, X, X + n, X + 2 * n, HN, jlo, jhi, [&](int j, double dx, double dy, double dz) {
+  pairs_in_slice<DIM>(n, a.P, k, X, X + n, X + 2 * n, HN, blockIdx.y, kPairSlices, [&](int j, double dx, double dy, double dz) {
     const Side<D> Jval = side_at<D>(a.tape, n, j, -1);
     for (int lo = 0; lo < ND; lo += NW) {
       const Side<D> Kseed = side_window<NW>(a.tape, n, kk, lo);
