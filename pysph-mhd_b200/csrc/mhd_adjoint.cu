@@ -346,8 +346,13 @@ __global__ void __launch_bounds__(kTile) k_f_cd(Args a) {
   TP(T_ALOC, i) = f_cd_post(r, vv, aa, TP(T_OM, i), TP(T_RHO, i), hi, TP(T_CS, i), a.amax, a.P.alpha_min);
 }
 
+// Force pair sums over one slice of the candidate tiles (grid y, as the
+// reverse force pairs): partial sums of the 14 sums and the dt_cfl max.
+constexpr int kFwdSlices = 8;
+constexpr int kFwdSums = kFSumDirs + 1;
+
 template <int K, int DIM>
-__global__ void __launch_bounds__(kTile) k_f_force(Args a) {
+__global__ void __launch_bounds__(kTile) k_f_force_pair(Args a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int n = a.n;
   const double* X = a.tape_w + (size_t)T_X * n;
@@ -355,13 +360,36 @@ __global__ void __launch_bounds__(kTile) k_f_force(Args a) {
   const Side<double> I = side_values(a.tape_w, n, i < n ? i : 0);
   FSums<double> S;
   S.zero();
-  all_pairs<DIM>(n, a.P, i, X, X + n, X + 2 * n, HN, [&](int j, double dx, double dy, double dz) {
+  pairs_in_slice<DIM>(n, a.P, i, X, X + n, X + 2 * n, HN, blockIdx.y, kFwdSlices,
+                      [&](int j, double dx, double dy, double dz) {
     const double xij[3] = {dx, dy, dz};
     f_force_pair<K, DIM>(a.P, I, side_values(a.tape_w, n, j), a.m[j], xij, S);
   });
   if (i >= n) return;
   double* sp[kFSumDirs];
   fsum_ptrs(S, sp);
+  double* part = a.slices + (size_t)blockIdx.y * kFwdSums * n;
+  for (int k = 0; k < kFSumDirs; k++) part[(size_t)k * n + i] = *sp[k];
+  part[(size_t)kFSumDirs * n + i] = S.dtcfl;
+}
+
+// The slices' sums added in slice order, then the force post-loop, stage2
+// and the next state.
+template <int DIM>
+__global__ void __launch_bounds__(kTile) k_f_force(Args a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = a.n;
+  if (i >= n) return;
+  const Side<double> I = side_values(a.tape_w, n, i);
+  FSums<double> S;
+  S.zero();
+  double* sp[kFSumDirs];
+  fsum_ptrs(S, sp);
+  for (int sl = 0; sl < kFwdSlices; sl++) {
+    const double* part = a.slices + (size_t)sl * kFwdSums * n;
+    for (int k = 0; k < kFSumDirs; k++) *sp[k] += part[(size_t)k * n + i];
+    S.dtcfl = fmax(S.dtcfl, part[(size_t)kFSumDirs * n + i]);
+  }
   for (int k = 0; k < kFSumDirs; k++) TP(T_FS + k, i) = *sp[k];
   TP(T_DTCFL, i) = S.dtcfl;
   FOut<double> o;
@@ -828,7 +856,8 @@ static void forward_step(const Args& a, cudaStream_t st) {
   k_f_density<K, DIM><<<nb, kTile, 0, st>>>(a);
   k_f_prologue<DIM><<<np, 256, 0, st>>>(a);
   k_f_cd<K, DIM><<<nb, kTile, 0, st>>>(a);
-  k_f_force<K, DIM><<<nb, kTile, 0, st>>>(a);
+  k_f_force_pair<K, DIM><<<dim3(nb, kFwdSlices), kTile, 0, st>>>(a);
+  k_f_force<DIM><<<nb, kTile, 0, st>>>(a);
 }
 
 template <int K, int DIM>
@@ -915,6 +944,7 @@ AdjLayout layout(int64_t n, int every) {
   L.g_amax = take(n);
   L.dta = take(n);
   L.part = take(n / 256 + 64);
+  static_assert(kFwdSlices * kFwdSums <= kPairSlices * kForceDirs, "forward slices share the reverse buffer");
   L.slices = take((size_t)kPairSlices * kForceDirs * n);
   L.total = off;
   return L;
@@ -967,8 +997,9 @@ double* run_segment(Ctx* c, Args a, const AdjLayout& L, const double* s0, int k0
     a.tape_w = buf + L.tape + (size_t)(t - k0) * NT * a.n;
     a.dt = dts[t];
     a.dta_out = buf + L.dta;
+    a.slices = buf + L.slices;
     MHD_A_DISPATCH(forward_step, a, st);
-    c->launches += 5;
+    c->launches += 6;
     time += dts[t];
     if (t + 1 < steps && dts[t + 1] < 0.0) {
       k_min<<<1, 256, 0, st>>>(a.n, buf + L.dta, buf + L.part);
