@@ -2,8 +2,10 @@
 
 Same hooks and order: ``initialize`` reads the config, ``create_particles``
 wraps the case's arrays in a CUDA ``ParticleArray``, ``create_domain`` the
-periodic box (``periodic_mode`` ``minimum_image``; ``None`` gives an open
-domain), ``configure_scheme`` builds the solver, and ``solve`` runs the
+periodic box (``periodic_mode`` ``minimum_image``, or ``ghost``, which gives
+the same pairs and displacements as the minimum image in a box wider than
+twice the kernel reach; ``None`` gives an open domain), ``configure_scheme``
+builds the solver, and ``solve`` runs the
 warm-up (src/application.py:110-132), the initial timestep (:134-147) and the
 time loop.  ``run()`` does all of it.
 """
