@@ -45,39 +45,11 @@ enum { L_X = 0, L_VH = 3, L_VP = 6, L_EH = 9, L_EP = 10, L_HP = 11, L_A1 = 12, L
        L_PSIP = 20, L_HN = 21, L_OM = 22, L_RHO = 23, L_P = 24, L_CS = 25, L_B = 26, M_D = 29, M_CD = 31, M_F = 58,
        L_RATES = 72, NL = 81 };  // L_RATES: au 3, ae, ah, ab 3, apsi
 
-// All j (ascending) with r2 < (R h_i)^2 or r2 < (R h_j)^2 for the positions
-// x, y, z and smoothing lengths h, self included; f(j, x_i - x_j min image).
-template <int DIM, class F>
-__device__ inline void all_pairs(int n, const DevParams& P, int i, const double* x, const double* y, const double* z,
-                                 const double* h, F&& f) {
-  __shared__ double4 sh[kTile];
-  const bool active = i < n;
-  const double xi = active ? x[i] : 0.0, yi = active ? y[i] : 0.0, zi = active && DIM == 3 ? z[i] : 0.0;
-  const double rhi2 = active ? rh2_exact(P.R, h[i]) : 0.0;
-  const PairBox wb = warp_pair_box<DIM>(active, xi, yi, zi, active ? h[i] : 0.0);
-  for (int base = 0; base < n; base += kTile) {
-    const int j = base + threadIdx.x;
-    if (j < n) sh[threadIdx.x] = make_double4(x[j], y[j], DIM == 3 ? z[j] : 0.0, h[j]);
-    __syncthreads();
-    const int m = n - base < kTile ? n - base : kTile;
-    // every lane takes part in the tile box's warp reductions
-    const PairBox tb = tile_pair_box<DIM, kTile>(sh, m);
-    if (active && !pair_boxes_apart<DIM>(wb, tb, P.R, P.L, P.periodic)) {
-      for (int t = 0; t < m; t++) {
-        const double4 q = sh[t];
-        const double dx = min_image(xi - q.x, P.L[0], P.half[0], P.periodic[0]);
-        const double dy = min_image(yi - q.y, P.L[1], P.half[1], P.periodic[1]);
-        const double dz = DIM == 3 ? min_image(zi - q.z, P.L[2], P.half[2], P.periodic[2]) : 0.0;
-        const double r2 = r2_exact(dx, dy, dz);
-        if (r2 < rhi2 || r2 < rh2_exact(P.R, q.w)) f(base + t, dx, dy, dz);
-      }
-    }
-    __syncthreads();
-  }
-}
-
-// all_pairs over one slice of the candidate tiles: the tiles within reach
-// of the warp (in ascending order) are dealt round robin to `slices`
+// The pair search of every pass: all j (ascending) with r2 < (R h_i)^2 or
+// r2 < (R h_j)^2 for the positions x, y, z and smoothing lengths h, self
+// included, f(j, x_i - x_j min image), over one slice of the candidates.
+// The candidates are staged a block-wide tile at a time; the tiles within
+// reach of the warp (in ascending order) are dealt round robin to `slices`
 // slices and this call visits those of slice `slice`, so the pairs of a
 // warp spread evenly over the slices wherever its neighbours lie in the
 // index order.  Which tiles are within reach is warp-uniform (the box
@@ -148,6 +120,21 @@ struct Args {
 #define LN(k, i) a.lam_next[(size_t)(k) * a.n + (i)]
 #define LS(k, i) a.lam[(size_t)(k) * a.n + (i)]
 #define W(k, i) a.w[(size_t)(k) * a.n + (i)]
+
+// Pair passes split over kPairSlices slices of candidate tiles (grid y,
+// pairs_in_slice): each writes `width` partial sums per particle and slice,
+// value q of slice s at slices[(s * width + q) * n + i], and a per-particle
+// kernel adds the slices in slice order (deterministic).
+constexpr int kPairSlices = 8;
+constexpr int kSliceWidth = 24;  // the widest partial record (the 24 CD moments)
+__device__ inline double& slice_part(const Args& a, int width, int q, int i) {
+  return a.slices[((size_t)blockIdx.y * width + q) * a.n + i];
+}
+__device__ inline double slices_sum(const Args& a, int width, int q, int i) {
+  double v = 0.0;
+  for (int s = 0; s < kPairSlices; s++) v += a.slices[((size_t)s * width + q) * a.n + i];
+  return v;
+}
 
 template <class D>
 __device__ inline StepState<D> state_at(const double* s, int n, int i, int seed_base) {
@@ -286,18 +273,30 @@ __global__ void __launch_bounds__(256) k_f_predict(Args a) {
 }
 
 template <int K, int DIM>
-__global__ void __launch_bounds__(kTile) k_f_density(Args a) {
+__global__ void __launch_bounds__(kTile) k_f_density_pair(Args a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int n = a.n;
   const double* X = a.tape_w + (size_t)T_X * n;
   const double* HP = a.tape_w + (size_t)T_HP * n;
   double rho = 0.0, dwdh = 0.0;
   const double hi = i < n ? HP[i] : 1.0;
-  all_pairs<DIM>(n, a.P, i, X, X + n, X + 2 * n, HP, [&](int j, double dx, double dy, double dz) {
+  pairs_in_slice<DIM>(n, a.P, i, X, X + n, X + 2 * n, HP, blockIdx.y, kPairSlices,
+                      [&](int j, double dx, double dy, double dz) {
     const double xij[3] = {dx, dy, dz};
     f_density_pair<K, DIM>(a.P.norm, xij, hi, a.m[j], rho, dwdh);
   });
   if (i >= n) return;
+  slice_part(a, 2, 0, i) = rho;
+  slice_part(a, 2, 1, i) = dwdh;
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(256) k_f_density(Args a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = a.n;
+  if (i >= n) return;
+  const double hi = TP(T_HP, i);
+  const double rho = slices_sum(a, 2, 0, i), dwdh = slices_sum(a, 2, 1, i);
   double om, hn;
   f_density_post<DIM>(a.P.hfact, hi, a.m[i], rho, dwdh, om, hn);
   TP(T_RS, i) = rho;
@@ -320,7 +319,7 @@ __global__ void __launch_bounds__(256) k_f_prologue(Args a) {
 }
 
 template <int K, int DIM>
-__global__ void __launch_bounds__(kTile) k_f_cd(Args a) {
+__global__ void __launch_bounds__(kTile) k_f_cd_pair(Args a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int n = a.n;
   const double* X = a.tape_w + (size_t)T_X * n;
@@ -328,7 +327,8 @@ __global__ void __launch_bounds__(kTile) k_f_cd(Args a) {
   double r[6] = {}, vv[9] = {}, aa[9] = {};
   const int ii = i < n ? i : 0;
   const double hi = HN[ii];
-  all_pairs<DIM>(n, a.P, i, X, X + n, X + 2 * n, HN, [&](int j, double dx, double dy, double dz) {
+  pairs_in_slice<DIM>(n, a.P, i, X, X + n, X + 2 * n, HN, blockIdx.y, kPairSlices,
+                      [&](int j, double dx, double dy, double dz) {
     const double xij[3] = {dx, dy, dz};
     double dv[3], da[3];
     for (int c = 0; c < 3; c++) {
@@ -338,6 +338,24 @@ __global__ void __launch_bounds__(kTile) k_f_cd(Args a) {
     f_cd_pair<K, DIM>(a.P.norm, xij, hi, a.m[j], dv, da, r, vv, aa);
   });
   if (i >= n) return;
+  for (int k = 0; k < 6; k++) slice_part(a, 24, k, i) = r[k];
+  for (int k = 0; k < 9; k++) {
+    slice_part(a, 24, 6 + k, i) = vv[k];
+    slice_part(a, 24, 15 + k, i) = aa[k];
+  }
+}
+
+__global__ void __launch_bounds__(256) k_f_cd(Args a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = a.n;
+  if (i >= n) return;
+  const double hi = TP(T_HN, i);
+  double r[6], vv[9], aa[9];
+  for (int k = 0; k < 6; k++) r[k] = slices_sum(a, 24, k, i);
+  for (int k = 0; k < 9; k++) {
+    vv[k] = slices_sum(a, 24, 6 + k, i);
+    aa[k] = slices_sum(a, 24, 15 + k, i);
+  }
   for (int k = 0; k < 6; k++) TP(T_CD + k, i) = r[k];
   for (int k = 0; k < 9; k++) {
     TP(T_CD + 6 + k, i) = vv[k];
@@ -348,7 +366,6 @@ __global__ void __launch_bounds__(kTile) k_f_cd(Args a) {
 
 // Force pair sums over one slice of the candidate tiles (grid y, as the
 // reverse force pairs): partial sums of the 14 sums and the dt_cfl max.
-constexpr int kFwdSlices = 8;
 constexpr int kFwdSums = kFSumDirs + 1;
 
 template <int K, int DIM>
@@ -360,7 +377,7 @@ __global__ void __launch_bounds__(kTile) k_f_force_pair(Args a) {
   const Side<double> I = side_values(a.tape_w, n, i < n ? i : 0);
   FSums<double> S;
   S.zero();
-  pairs_in_slice<DIM>(n, a.P, i, X, X + n, X + 2 * n, HN, blockIdx.y, kFwdSlices,
+  pairs_in_slice<DIM>(n, a.P, i, X, X + n, X + 2 * n, HN, blockIdx.y, kPairSlices,
                       [&](int j, double dx, double dy, double dz) {
     const double xij[3] = {dx, dy, dz};
     f_force_pair<K, DIM>(a.P, I, side_values(a.tape_w, n, j), a.m[j], xij, S);
@@ -385,7 +402,7 @@ __global__ void __launch_bounds__(kTile) k_f_force(Args a) {
   S.zero();
   double* sp[kFSumDirs];
   fsum_ptrs(S, sp);
-  for (int sl = 0; sl < kFwdSlices; sl++) {
+  for (int sl = 0; sl < kPairSlices; sl++) {
     const double* part = a.slices + (size_t)sl * kFwdSums * n;
     for (int k = 0; k < kFSumDirs; k++) *sp[k] += part[(size_t)k * n + i];
     S.dtcfl = fmax(S.dtcfl, part[(size_t)kFSumDirs * n + i]);
@@ -569,7 +586,6 @@ __device__ inline void add_side(const Args& a, int i, const double* g, double si
 // fills the GPU; each slice writes its partial sums and k_r_force_pair_sum
 // adds them in slice order (deterministic).
 constexpr int kForceWindow = 6;
-constexpr int kPairSlices = 8;
 constexpr int kForceDirs = kSideDirs + 3;
 
 template <int K, int DIM, bool DUAL>
@@ -698,7 +714,8 @@ __global__ void __launch_bounds__(kTile) k_r_cd_pair(Args a) {
   const double* HN = a.tape + (size_t)T_HN * n;
   const int kk = k < n ? k : 0;
   double gx[3] = {}, gh = 0.0, gv[3] = {}, ga[3] = {};
-  all_pairs<DIM>(n, a.P, k, X, X + n, X + 2 * n, HN, [&](int j, double dx, double dy, double dz) {
+  pairs_in_slice<DIM>(n, a.P, k, X, X + n, X + 2 * n, HN, blockIdx.y, kPairSlices,
+                      [&](int j, double dx, double dy, double dz) {
     for (int side = 0; side < 2; side++) {
       // side 0: pair (k, j); side 1: pair (j, k)
       const int ii = side ? j : kk, jj = side ? kk : j;
@@ -743,11 +760,22 @@ __global__ void __launch_bounds__(kTile) k_r_cd_pair(Args a) {
   });
   if (k >= n) return;
   for (int c = 0; c < 3; c++) {
-    W(L_X + c, k) += gx[c];
-    W(L_VP + c, k) += gv[c];
-    LS(SA + c, k) += ga[c];
+    slice_part(a, 10, c, k) = gx[c];
+    slice_part(a, 10, 3 + c, k) = gv[c];
+    slice_part(a, 10, 6 + c, k) = ga[c];
   }
-  W(L_HN, k) += gh;
+  slice_part(a, 10, 9, k) = gh;
+}
+
+__global__ void __launch_bounds__(256) k_r_cd_sum(Args a) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= a.n) return;
+  for (int c = 0; c < 3; c++) {
+    W(L_X + c, k) += slices_sum(a, 10, c, k);
+    W(L_VP + c, k) += slices_sum(a, 10, 3 + c, k);
+    LS(SA + c, k) += slices_sum(a, 10, 6 + c, k);
+  }
+  W(L_HN, k) += slices_sum(a, 10, 9, k);
 }
 
 // EOS and magnetic-state reconstruction reversed.
@@ -795,7 +823,8 @@ __global__ void __launch_bounds__(kTile) k_r_density_pair(Args a) {
   const double* HP = a.tape + (size_t)T_HP * n;
   const int kk = k < n ? k : 0;
   double gx[3] = {}, gh = 0.0;
-  all_pairs<DIM>(n, a.P, k, X, X + n, X + 2 * n, HP, [&](int j, double dx, double dy, double dz) {
+  pairs_in_slice<DIM>(n, a.P, k, X, X + n, X + 2 * n, HP, blockIdx.y, kPairSlices,
+                      [&](int j, double dx, double dy, double dz) {
     for (int side = 0; side < 2; side++) {
       const int ii = side ? j : kk, jj = side ? kk : j;
       const double sgn = side ? -1.0 : 1.0;
@@ -808,8 +837,15 @@ __global__ void __launch_bounds__(kTile) k_r_density_pair(Args a) {
     }
   });
   if (k >= n) return;
-  for (int c = 0; c < 3; c++) W(L_X + c, k) += gx[c];
-  W(L_HP, k) += gh;
+  for (int c = 0; c < 3; c++) slice_part(a, 4, c, k) = gx[c];
+  slice_part(a, 4, 3, k) = gh;
+}
+
+__global__ void __launch_bounds__(256) k_r_density_sum(Args a) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= a.n) return;
+  for (int c = 0; c < 3; c++) W(L_X + c, k) += slices_sum(a, 4, c, k);
+  W(L_HP, k) += slices_sum(a, 4, 3, k);
 }
 
 // initialize + stage1 + wrap reversed: lambda(S_n).
@@ -853,10 +889,12 @@ template <int K, int DIM>
 static void forward_step(const Args& a, cudaStream_t st) {
   const int nb = (a.n + kTile - 1) / kTile, np = (a.n + 255) / 256;
   k_f_predict<<<np, 256, 0, st>>>(a);
-  k_f_density<K, DIM><<<nb, kTile, 0, st>>>(a);
+  k_f_density_pair<K, DIM><<<dim3(nb, kPairSlices), kTile, 0, st>>>(a);
+  k_f_density<DIM><<<np, 256, 0, st>>>(a);
   k_f_prologue<DIM><<<np, 256, 0, st>>>(a);
-  k_f_cd<K, DIM><<<nb, kTile, 0, st>>>(a);
-  k_f_force_pair<K, DIM><<<dim3(nb, kFwdSlices), kTile, 0, st>>>(a);
+  k_f_cd_pair<K, DIM><<<dim3(nb, kPairSlices), kTile, 0, st>>>(a);
+  k_f_cd<<<np, 256, 0, st>>>(a);
+  k_f_force_pair<K, DIM><<<dim3(nb, kPairSlices), kTile, 0, st>>>(a);
   k_f_force<DIM><<<nb, kTile, 0, st>>>(a);
 }
 
@@ -872,12 +910,14 @@ static void reverse_step(const Args& a, cudaStream_t st) {
   k_r_force_pair_sum<<<np, 256, 0, st>>>(a);
   k_r_cd_post<<<n64, 64, 0, st>>>(a);
   if (a.dual_pairs)
-    k_r_cd_pair<K, DIM, true><<<nb, kTile, 0, st>>>(a);
+    k_r_cd_pair<K, DIM, true><<<dim3(nb, kPairSlices), kTile, 0, st>>>(a);
   else
-    k_r_cd_pair<K, DIM, false><<<nb, kTile, 0, st>>>(a);
+    k_r_cd_pair<K, DIM, false><<<dim3(nb, kPairSlices), kTile, 0, st>>>(a);
+  k_r_cd_sum<<<np, 256, 0, st>>>(a);
   k_r_prologue<DIM><<<np, 256, 0, st>>>(a);
   k_r_density_post<DIM><<<np, 256, 0, st>>>(a);
-  k_r_density_pair<K, DIM><<<nb, kTile, 0, st>>>(a);
+  k_r_density_pair<K, DIM><<<dim3(nb, kPairSlices), kTile, 0, st>>>(a);
+  k_r_density_sum<<<np, 256, 0, st>>>(a);
   k_r_predict<<<n64, 64, 0, st>>>(a);
 }
 
@@ -944,8 +984,8 @@ AdjLayout layout(int64_t n, int every) {
   L.g_amax = take(n);
   L.dta = take(n);
   L.part = take(n / 256 + 64);
-  static_assert(kFwdSlices * kFwdSums <= kPairSlices * kForceDirs, "forward slices share the reverse buffer");
-  L.slices = take((size_t)kPairSlices * kForceDirs * n);
+  static_assert(kFwdSums <= kSliceWidth && kForceDirs <= kSliceWidth, "slice records fit the buffer");
+  L.slices = take((size_t)kPairSlices * kSliceWidth * n);
   L.total = off;
   return L;
 }
@@ -999,7 +1039,7 @@ double* run_segment(Ctx* c, Args a, const AdjLayout& L, const double* s0, int k0
     a.dta_out = buf + L.dta;
     a.slices = buf + L.slices;
     MHD_A_DISPATCH(forward_step, a, st);
-    c->launches += 6;
+    c->launches += 8;
     time += dts[t];
     if (t + 1 < steps && dts[t + 1] < 0.0) {
       k_min<<<1, 256, 0, st>>>(a.n, buf + L.dta, buf + L.part);
@@ -1100,7 +1140,7 @@ int mhd_adjoint_backward(void* ctx, const MhdState* s, int64_t n, int32_t steps,
         c->launches++;
       }
       MHD_A_DISPATCH(reverse_step, r, st);
-      c->launches += 10;
+      c->launches += 12;
       double* tmp = lam_next;
       lam_next = lam;
       lam = tmp;
