@@ -15,6 +15,8 @@
 // order throughout.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <climits>
 #include <string>
 
 #include "mhd_common.cuh"
@@ -72,9 +74,25 @@ __device__ inline D pmin(const D& a, const D& b) { return b < a ? b : a; }
 
 // ------------------------------------------------------- all-pairs search
 // Calls f(j) for every j (ascending) with r2 < (R h_i)^2 or r2 < (R h_j)^2
-// on the minimum-image FP64 values, self included.  The block (kTile
-// threads) stages kTile positions at a time in shared memory; every thread
-// of the block must call it.
+// on the minimum-image FP64 values, self included, within one slice of the
+// candidates.  The block (kTile threads) stages kTile positions at a time
+// in shared memory; every thread of the block must call it.  The tiles
+// within reach of a warp (bounding boxes) are dealt round robin to the
+// kTSlices slices (grid y), so that each slice has a share of every warp's
+// pairs; each pair kernel writes its partial sums per slice and a
+// per-particle kernel adds them in slice order (deterministic).
+constexpr int kTSlices = 8;
+constexpr int kTWidth = 24;  // partial records per particle and slice (the 24 CD moments at most)
+
+__device__ inline TD& t_part(TD* part, int n, int q, int i) {
+  return part[((size_t)blockIdx.y * kTWidth + q) * n + i];
+}
+__device__ inline TD t_slices_sum(const TD* part, int n, int q, int i) {
+  TD v(0.0);
+  for (int sl = 0; sl < kTSlices; sl++) v = v + part[((size_t)sl * kTWidth + q) * n + i];
+  return v;
+}
+
 template <int DIM, class F>
 __device__ inline void all_pairs(int n, const DevParams& P, int i, const MhdState& s, F&& f) {
   __shared__ double4 sh[kTile];
@@ -84,6 +102,7 @@ __device__ inline void all_pairs(int n, const DevParams& P, int i, const MhdStat
   const double zi = active && DIM == 3 ? Z[i].v : 0.0;
   const double rhi2 = active ? rh2_exact(P.R, H[i].v) : 0.0;
   const PairBox wb = warp_pair_box<DIM>(active, xi, yi, zi, active ? H[i].v : 0.0);
+  int near = 0;  // tiles within reach of the warp so far
   for (int base = 0; base < n; base += kTile) {
     const int j = base + threadIdx.x;
     if (j < n) sh[threadIdx.x] = make_double4(X[j].v, Y[j].v, DIM == 3 ? Z[j].v : 0.0, H[j].v);
@@ -91,7 +110,8 @@ __device__ inline void all_pairs(int n, const DevParams& P, int i, const MhdStat
     const int m = n - base < kTile ? n - base : kTile;
     // every lane takes part in the tile box's warp reductions
     const PairBox tb = tile_pair_box<DIM, kTile>(sh, m);
-    if (active && !pair_boxes_apart<DIM>(wb, tb, P.R, P.L, P.periodic)) {
+    const bool mine = !pair_boxes_apart<DIM>(wb, tb, P.R, P.L, P.periodic) && near++ % kTSlices == (int)blockIdx.y;
+    if (active && mine) {
       for (int t = 0; t < m; t++) {
         const double4 q = sh[t];
         const double dx = min_image(xi - q.x, P.L[0], P.half[0], P.periodic[0]);
@@ -238,7 +258,7 @@ __global__ void __launch_bounds__(256) k_t_sync(int n, MhdState s) {
 // h_i, Omega from the old h, then h = hfact (m / rho)^(1/dim).  The new h goes
 // to h_new (other threads still read h).
 template <int K, int DIM>
-__global__ void __launch_bounds__(kTile) k_t_density(int n, DevParams P, MhdState s, TD* __restrict__ h_new) {
+__global__ void __launch_bounds__(kTile) k_t_density_pair(int n, DevParams P, MhdState s, TD* __restrict__ part) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   TD rho(0.0), dwdh(0.0);
   const TD hi = i < n ? TF(h)[i] : TD(1.0);
@@ -250,6 +270,17 @@ __global__ void __launch_bounds__(kTile) k_t_density(int n, DevParams P, MhdStat
     dwdh += mj * t_kern_gradh<K, DIM>(P.norm, rij, hi);
   });
   if (i >= n) return;
+  t_part(part, n, 0, i) = rho;
+  t_part(part, n, 1, i) = dwdh;
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(256) k_t_density(int n, DevParams P, MhdState s, const TD* __restrict__ part,
+                                                   TD* __restrict__ h_new) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const TD hi = TF(h)[i];
+  const TD rho = t_slices_sum(part, n, 0, i), dwdh = t_slices_sum(part, n, 1, i);
   TF(rho_sum)[i] = rho;
   if (TF(converged)[i].v == 1.0) {
     // already finalised in this group evaluation (the warm-up's second and
@@ -291,7 +322,7 @@ __global__ void __launch_bounds__(256) k_t_prologue(int n, DevParams P, MhdState
 // src/equations.py:318-429 with the previous step's accelerations; the
 // alpha clip [alpha_min, alpha_max] with alpha_max a dual number.
 template <int K, int DIM>
-__global__ void __launch_bounds__(kTile) k_t_cd(int n, DevParams P, MhdState s, TD alpha_max) {
+__global__ void __launch_bounds__(kTile) k_t_cd_pair(int n, DevParams P, MhdState s, TD* __restrict__ part) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   TD r[6], vv[9], aa[9];
   for (int k = 0; k < 6; k++) r[k] = TD(0.0);
@@ -319,6 +350,24 @@ __global__ void __launch_bounds__(kTile) k_t_cd(int n, DevParams P, MhdState s, 
       }
   });
   if (!act) return;
+  for (int k = 0; k < 6; k++) t_part(part, n, k, i) = r[k];
+  for (int k = 0; k < 9; k++) {
+    t_part(part, n, 6 + k, i) = vv[k];
+    t_part(part, n, 15 + k, i) = aa[k];
+  }
+}
+
+__global__ void __launch_bounds__(256) k_t_cd(int n, DevParams P, MhdState s, const TD* __restrict__ part,
+                                              TD alpha_max) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const TD hi = TF(h)[i];
+  TD r[6], vv[9], aa[9];
+  for (int k = 0; k < 6; k++) r[k] = t_slices_sum(part, n, k, i);
+  for (int k = 0; k < 9; k++) {
+    vv[k] = t_slices_sum(part, n, 6 + k, i);
+    aa[k] = t_slices_sum(part, n, 15 + k, i);
+  }
   const TD rxx = r[0], rxy = r[1], rxz = r[2], ryy = r[3], ryz = r[4], rzz = r[5];
   const TD denom = rxx * ryy * rzz + 2.0 * rxy * rxz * ryz - rxx * ryz * ryz - ryy * rxz * rxz - rzz * rxy * rxy;
   const TD termnorm = TF(omega)[i] / TF(rho)[i];
@@ -363,24 +412,37 @@ __global__ void __launch_bounds__(kTile) k_t_cd(int n, DevParams P, MhdState s, 
 // 133-140, 143-195, 488-567) in one neighbour loop with the accumulations
 // of each group kept apart, then EnergyLimiter, DivBCorrection and
 // AdaptiveTimestep (src/equations.py:588-624, 570-585).
+// The i-side values of the force groups, shared by the pair and post-loop
+// kernels (a macro, so that both read as the one loop they split).
+#define T_FORCE_SIDE_I                                                                                        \
+  const double beta = 2.0, mu0 = P.mu0;                                                                       \
+  const TD hi = TF(h)[ii], rhoi = TF(rho)[ii], p_i = TF(p)[ii], omegai = TF(omega)[ii], csi = TF(cs)[ii];      \
+  const TD bi[3] = {TF(Bx)[ii], TF(By)[ii], TF(Bz)[ii]};                                                       \
+  const TD vi[3] = {TF(upred)[ii], TF(vpred)[ii], TF(wpred)[ii]};                                              \
+  const TD epi = TF(epred)[ii], alphai = TF(alpha1)[ii], psii = TF(psipred)[ii];                               \
+  const TD bi2 = bi[0] * bi[0] + bi[1] * bi[1] + bi[2] * bi[2];                                                \
+  const TD vwave_i = sqrt(csi * csi + bi2 / (mu0 * rhoi));                                                     \
+  const TD brhoi[3] = {bi[0] / rhoi, bi[1] / rhoi, bi[2] / rhoi};                                              \
+  const TD bro2_i = (brhoi[0] * brhoi[0] + brhoi[1] * brhoi[1] + brhoi[2] * brhoi[2]) / mu0;                   \
+  const TD rho_i2_inv = 1.0 / (rhoi * rhoi);                                                                   \
+  const TD ch_i = P.clean_speed * vwave_i;
+
+// Partial records of the force pair kernel: the 14 sums, dt_cfl and the
+// index of the pair that set it (so that the slices' maxima combine to the
+// first maximum in ascending j, as one loop over all pairs gives).
+enum { TF_A6 = 0, TF_A8 = 3, TF_AE6 = 6, TF_AE9 = 7, TF_DIV = 8, TF_AB = 9, TF_DIVBS = 12, TF_DIVBD = 13,
+       TF_DTCFL = 14, TF_JMAX = 15 };
+
 template <int K, int DIM>
-__global__ void __launch_bounds__(kTile) k_t_force(int n, DevParams P, MhdState s) {
+__global__ void __launch_bounds__(kTile) k_t_force_pair(int n, DevParams P, MhdState s, TD* __restrict__ part) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const bool act = i < n;
-  const double beta = 2.0, mu0 = P.mu0;
   TD a6[3] = {TD(0.0), TD(0.0), TD(0.0)}, a8[3] = {TD(0.0), TD(0.0), TD(0.0)};
   TD ae6(0.0), ae9(0.0), div(0.0), dtcfl(0.0), ab[3] = {TD(0.0), TD(0.0), TD(0.0)}, divbs(0.0), divbd(0.0);
+  int jmax = INT_MAX;
   const int ii = act ? i : 0;
-  const TD hi = TF(h)[ii], rhoi = TF(rho)[ii], p_i = TF(p)[ii], omegai = TF(omega)[ii], csi = TF(cs)[ii];
-  const TD bi[3] = {TF(Bx)[ii], TF(By)[ii], TF(Bz)[ii]};
-  const TD vi[3] = {TF(upred)[ii], TF(vpred)[ii], TF(wpred)[ii]};
-  const TD epi = TF(epred)[ii], alphai = TF(alpha1)[ii], psii = TF(psipred)[ii];
-  const TD bi2 = bi[0] * bi[0] + bi[1] * bi[1] + bi[2] * bi[2];
-  const TD vwave_i = sqrt(csi * csi + bi2 / (mu0 * rhoi));
-  const TD brhoi[3] = {bi[0] / rhoi, bi[1] / rhoi, bi[2] / rhoi};
-  const TD bro2_i = (brhoi[0] * brhoi[0] + brhoi[1] * brhoi[1] + brhoi[2] * brhoi[2]) / mu0;
-  const TD rho_i2_inv = 1.0 / (rhoi * rhoi);
-  const TD ch_i = P.clean_speed * vwave_i;
+  T_FORCE_SIDE_I
+  (void)alphai;
   all_pairs<DIM>(n, P, i, s, [&](int j) {
     TD xij[3], rij, dwi[3], dwj[3];
     pair_geometry<DIM>(P, s, i, j, xij, rij);
@@ -412,7 +474,10 @@ __global__ void __launch_bounds__(kTile) k_t_force(int n, DevParams P, MhdState 
       TD c = vwave_i - beta * dot;
       c = pmax(c, vwave_j - beta * dot);
       c = pmax(c, TD(0.0));
-      dtcfl = pmax(dtcfl, c);
+      if (c > dtcfl) {  // pmax(dtcfl, c), keeping the pair that set it
+        dtcfl = c;
+        jmax = j;
+      }
       if (dot < 0.0) {
         const TD vav_i = pmax(alphai * vwave_i - beta * dot, TD(0.0));
         const TD vav_j = pmax(TF(alpha1)[j] * vwave_j - beta * dot, TD(0.0));
@@ -480,6 +545,52 @@ __global__ void __launch_bounds__(kTile) k_t_force(int n, DevParams P, MhdState 
     }
   });
   if (!act) return;
+  for (int a = 0; a < 3; a++) {
+    t_part(part, n, TF_A6 + a, i) = a6[a];
+    t_part(part, n, TF_A8 + a, i) = a8[a];
+    t_part(part, n, TF_AB + a, i) = ab[a];
+  }
+  t_part(part, n, TF_AE6, i) = ae6;
+  t_part(part, n, TF_AE9, i) = ae9;
+  t_part(part, n, TF_DIV, i) = div;
+  t_part(part, n, TF_DIVBS, i) = divbs;
+  t_part(part, n, TF_DIVBD, i) = divbd;
+  t_part(part, n, TF_DTCFL, i) = dtcfl;
+  t_part(part, n, TF_JMAX, i) = TD((double)jmax);
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(256) k_t_force(int n, DevParams P, MhdState s, const TD* __restrict__ part) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int ii = i;
+  T_FORCE_SIDE_I
+  (void)beta;
+  (void)omegai;
+  (void)vi;
+  (void)alphai;
+  (void)bro2_i;
+  (void)rho_i2_inv;
+  TD a6[3], a8[3], ab[3];
+  for (int a = 0; a < 3; a++) {
+    a6[a] = t_slices_sum(part, n, TF_A6 + a, i);
+    a8[a] = t_slices_sum(part, n, TF_A8 + a, i);
+    ab[a] = t_slices_sum(part, n, TF_AB + a, i);
+  }
+  const TD ae6 = t_slices_sum(part, n, TF_AE6, i), ae9 = t_slices_sum(part, n, TF_AE9, i);
+  const TD div = t_slices_sum(part, n, TF_DIV, i);
+  const TD divbs = t_slices_sum(part, n, TF_DIVBS, i), divbd = t_slices_sum(part, n, TF_DIVBD, i);
+  // the largest slice maximum; on a tie the one set by the smaller j
+  TD dtcfl(0.0);
+  double jbest = (double)INT_MAX;
+  for (int sl = 0; sl < kTSlices; sl++) {
+    const TD v = part[((size_t)sl * kTWidth + TF_DTCFL) * n + i];
+    const double jv = part[((size_t)sl * kTWidth + TF_JMAX) * n + i].v;
+    if (v > dtcfl || (v.v == dtcfl.v && jv < jbest)) {
+      dtcfl = v;
+      jbest = jv;
+    }
+  }
   // G6 post (src/equations.py:278-280) and G7 (:133-140)
   const TD divv = -div / rhoi;
   TF(div)[i] = divv;
@@ -561,11 +672,16 @@ template <int K, int DIM>
 static void t_rhs_launch(Ctx* c, MhdState* s, int n, TD amax, cudaStream_t st) {
   const int nb = (n + kTile - 1) / kTile, np = (n + 255) / 256;
   TD* h_new = reinterpret_cast<TD*>(c->tan_work);
-  k_t_density<K, DIM><<<nb, kTile, 0, st>>>(n, c->P, *s, h_new);
+  TD* part = h_new + c->n_max + 1024;  // kTSlices * kTWidth records per particle
+  const dim3 sliced(nb, kTSlices);
+  k_t_density_pair<K, DIM><<<sliced, kTile, 0, st>>>(n, c->P, *s, part);
+  k_t_density<DIM><<<np, 256, 0, st>>>(n, c->P, *s, part, h_new);
   k_t_prologue<DIM><<<np, 256, 0, st>>>(n, c->P, *s, h_new);
-  k_t_cd<K, DIM><<<nb, kTile, 0, st>>>(n, c->P, *s, amax);
-  k_t_force<K, DIM><<<nb, kTile, 0, st>>>(n, c->P, *s);
-  c->launches += 4;
+  k_t_cd_pair<K, DIM><<<sliced, kTile, 0, st>>>(n, c->P, *s, part);
+  k_t_cd<<<np, 256, 0, st>>>(n, c->P, *s, part, amax);
+  k_t_force_pair<K, DIM><<<sliced, kTile, 0, st>>>(n, c->P, *s, part);
+  k_t_force<DIM><<<np, 256, 0, st>>>(n, c->P, *s, part);
+  c->launches += 7;
 }
 
 #define MHD_T_DISPATCH(...)                                                                                   \
@@ -621,7 +737,9 @@ int check_tangent(Ctx* c, const MhdState* s, int64_t n) {
   }
   if (!s->itype) T_FAIL(MHD_ERR_INVALID, "itype is null");
   if (!c->tan_work) {
-    T_CK(cudaMalloc(&c->tan_work, sizeof(TD) * (size_t)(c->n_max + 1024)));
+    // new h (n_max + 1024 records), then the pair kernels' partial sums
+    const size_t nt = (size_t)std::min<int64_t>(c->n_max, MHD_TANGENT_MAX_N);
+    T_CK(cudaMalloc(&c->tan_work, sizeof(TD) * ((size_t)c->n_max + 1024 + (size_t)kTSlices * kTWidth * nt)));
   }
   return MHD_OK;
 }
