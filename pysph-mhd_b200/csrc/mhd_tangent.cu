@@ -442,7 +442,6 @@ __global__ void __launch_bounds__(kTile) k_t_force_pair(int n, DevParams P, MhdS
   int jmax = INT_MAX;
   const int ii = act ? i : 0;
   T_FORCE_SIDE_I
-  (void)alphai;
   all_pairs<DIM>(n, P, i, s, [&](int j) {
     TD xij[3], rij, dwi[3], dwj[3];
     pair_geometry<DIM>(P, s, i, j, xij, rij);
