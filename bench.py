@@ -649,7 +649,7 @@ def run_b200(args, rank, world):
     flops = (FORCE_FLOPS_PER_PAIR * head["pairs"] + FORCE_FLOPS_PER_CANDIDATE * head["candidates"]) / args.steps
     achieved_tf = flops / (force_ms * 1e-3) / 1e12
 
-    e2e = run_e2e(args, dev)
+    e2e = run_e2e(args, dev, barrier, dist, world)
     batched = _batched(args, dev, rank, world) if args.batch_instances > 0 else None
     derivative = _derivative(args, dev) if (rank == 0 and not dist and args.derivative_steps > 0) else None
 
@@ -704,7 +704,7 @@ def run_b200(args, rank, world):
         tdist.destroy_process_group()
 
 
-def run_e2e(args, dev):
+def run_e2e(args, dev, barrier=lambda: None, dist=False, world=1):
     import torch
 
     from src.engine import Engine, params_from_dict
@@ -725,6 +725,7 @@ def run_e2e(args, dev):
     pfreq = 20
     h2d = sum(t.numel() * t.element_size() for t in host.values())
     d2h = 0
+    barrier()
     t0 = time.perf_counter()
     for k, t in host.items():
         eng.pa.properties[k].copy_(t, non_blocking=True)
@@ -740,9 +741,17 @@ def run_e2e(args, dev):
                 d2h += out[k].numel() * out[k].element_size()
             torch.cuda.synchronize()
     el = time.perf_counter() - t0
+    if dist:
+        # every rank's replica, timed as the slowest rank
+        import torch.distributed as tdist
+
+        t = torch.tensor([el], device=dev, dtype=torch.float64)
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        el = float(t.item())
+    barrier()
     eng.close()
-    return {"value": n * args.steps / el, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,
-            "d2h_bytes_per_step": d2h / args.steps,
+    return {"value": world * n * args.steps / el, "unit": UNIT, "h2d_bytes_per_step": world * h2d / args.steps,
+            "d2h_bytes_per_step": world * d2h / args.steps,
             "path": "ParticleArray push from pinned host + Engine.step (literal MHDStep stages, host dt per step) "
                     "+ OUTPUT_PROPERTIES pulled every 20 steps and at the end"}
 
