@@ -258,8 +258,8 @@ __device__ __forceinline__ PairBox tile_pair_box(const double4* sh, int m) {
 // reach carries a relative slack of 1e-6 and an absolute one of a few ulp
 // of the coordinates, far above the rounding of the test itself.
 template <int DIM>
-__device__ __forceinline__ bool pair_boxes_apart(const PairBox& w, const PairBox& t, double R, const double* L,
-                                                 const int* periodic) {
+__host__ __device__ __forceinline__ bool pair_boxes_apart(const PairBox& w, const PairBox& t, double R,
+                                                          const double* L, const int* periodic) {
   const double reach = R * fmax(w.h, t.h) * (1.0 + 1e-6);
   for (int a = 0; a < DIM; a++) {
     double g = fmax(t.lo[a] - w.hi[a], w.lo[a] - t.hi[a]);
