@@ -185,12 +185,17 @@ def oracle_rate(n_side, steps, warm_steps=0):
     return s.n * steps / el, el, s.n
 
 
+def blast_workload(n_side):
+    """The workload name both arms put in config.workload."""
+    return (f"3-D MHD blast {n_side}^3 = {n_side ** 3} particles, cubic kernel hfact 1.2, alpha [0.1, 1], "
+            f"periodic unit cube")
+
+
 def run_reference(args, rank):
     if rank != 0:
         return
     n_side = args.ref_n
     rate, el, n = oracle_rate(n_side, args.steps, args.warmup)
-    ic_n = args.n ** 3
     sample = (f"C oracle (reference equations restated, FP64, OpenMP {cpu_cores()} threads): 3-D blast at {n_side}^3 "
               f"= {n} particles (same physics and spacing law as the {args.n}^3 workload), {args.warmup} untimed + "
               f"{args.steps} timed PEC steps after the 3-RHS warm-up")
@@ -198,8 +203,7 @@ def run_reference(args, rank):
         "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"3-D MHD blast {args.n}^3 = {ic_n} particles, cubic kernel hfact 1.2, alpha [0.1, 1]",
-                   "sample_particles": n},
+        "config": {"workload": blast_workload(args.n), "form": "fp64 (the oracle)", "sample_particles": n},
         "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cpu_cores(), "kind": "port", "sample": sample},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -667,8 +671,7 @@ def run_b200(args, rank, world):
             "vs_baseline": None,
             "dtype": "f64" if args.precision == "fp64" else "f32 pair arithmetic, f64 h-iteration/epilogue/dt",
             "data": "synthetic",
-            "config": {"workload": f"3-D MHD blast {args.n}^3 = {n} particles, cubic kernel hfact 1.2, "
-                                   f"alpha [0.1, 1], periodic unit cube", "form": args.precision,
+            "config": {"workload": blast_workload(args.n), "form": args.precision,
                        "parallelism": "replicas" if world > 1 else "single", "l2_flush": "inputs (~0.6 GB) > L2",
                        "density_passes_per_rhs": head["passes"], "timed_run": "one captured graph of K fused steps",
                        "replays": head["replays"], "ms_per_step_uncaptured": head["ms_per_step_uncaptured"],
