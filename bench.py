@@ -165,7 +165,10 @@ def cpu_cores():
 
 def oracle_rate(n_side, steps, warm_steps=0):
     """Particle-steps/s of the C oracle (the reference restated, OpenMP over all
-    host threads) on the blast at n_side^3: warm-up untimed, then `steps`."""
+    host threads) on the blast at n_side^3: the 3-RHS warm-up and
+    `warm_steps` steps untimed, then `steps` timed.  Returns the rate, the
+    timed seconds, the particle count and the density passes of each timed
+    step."""
     import oracle
 
     oracle.build()
@@ -177,12 +180,13 @@ def oracle_rate(n_side, steps, warm_steps=0):
     for _ in range(warm_steps):
         o.step(s, dt)
         dt = o.min_dt(s)
+    passes = []
     t0 = time.perf_counter()
     for _ in range(steps):
-        o.step(s, dt)
+        passes.append(o.step(s, dt))
         dt = o.min_dt(s)
     el = time.perf_counter() - t0
-    return s.n * steps / el, el, s.n
+    return s.n * steps / el, el, s.n, passes
 
 
 def blast_workload(n_side):
@@ -191,20 +195,25 @@ def blast_workload(n_side):
             f"periodic unit cube")
 
 
+def oracle_sample(n_side, warm, steps, el, passes):
+    return (f"C oracle (reference equations restated, FP64, OpenMP {cpu_cores()} threads): 3-D blast at {n_side}^3 "
+            f"= {n_side ** 3} particles, the 3-RHS warm-up and {warm} steps untimed, then {steps} timed PEC steps "
+            f"({el:.1f} s; density passes per step {passes})")
+
+
 def run_reference(args, rank):
     if rank != 0:
         return
-    n_side = args.ref_n
-    rate, el, n = oracle_rate(n_side, args.steps, args.warmup)
-    sample = (f"C oracle (reference equations restated, FP64, OpenMP {cpu_cores()} threads): 3-D blast at {n_side}^3 "
-              f"= {n} particles (same physics and spacing law as the {args.n}^3 workload), {args.warmup} untimed + "
-              f"{args.steps} timed PEC steps after the 3-RHS warm-up")
+    n_side = args.ref_n or args.n
+    rate, el, n, passes = oracle_rate(n_side, args.steps, args.warmup)
     line = {
         "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": blast_workload(args.n), "form": "fp64 (the oracle)", "sample_particles": n},
-        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cpu_cores(), "kind": "port", "sample": sample},
+        "config": {"workload": blast_workload(args.n), "timed_workload": blast_workload(n_side),
+                   "form": "fp64 (the oracle)", "sample_particles": n},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cpu_cores(), "kind": "port",
+                         "sample": oracle_sample(n_side, args.warmup, args.steps, el, passes)},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -659,10 +668,13 @@ def run_b200(args, rank, world):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rate, el, ns = oracle_rate(args.ref_n, args.cpu_steps)
+        # the reference arm's measurement on a bounded sample of its steps:
+        # the same workload and the same untimed lead-in, fewer timed steps
+        n_side = args.ref_n or args.n
+        k = min(args.cpu_steps, args.steps)
+        rate, el, ns, passes = oracle_rate(n_side, k, args.warmup)
         cpu = {"value": rate, "unit": UNIT, "cores": cpu_cores(), "kind": "port",
-               "sample": f"C oracle (reference equations restated, FP64, OpenMP) on the blast at {args.ref_n}^3 = "
-                         f"{ns} particles, {args.cpu_steps} PEC steps after the warm-up, {el:.1f} s"}
+               "sample": oracle_sample(n_side, args.warmup, k, el, passes)}
 
     if rank == 0:
         line = {
@@ -766,8 +778,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=("b200", "reference"))
     ap.add_argument("--n", type=int, default=128, help="lattice side of the blast (n^3 particles)")
-    ap.add_argument("--ref-n", type=int, default=64, help="lattice side of the CPU sample")
-    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--ref-n", type=int, default=0, help="lattice side of the CPU runs (0: the workload's)")
+    ap.add_argument("--cpu-steps", type=int, default=5, help="timed oracle steps of the cpu_baseline sample")
     ap.add_argument("--precision", default="fp32", choices=("fp64", "fp32"),
                     help="form timed as the headline value (the FP64 path is timed beside it)")
     ap.add_argument("--accuracy-steps", type=int, default=100)

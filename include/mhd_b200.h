@@ -199,7 +199,7 @@ int mhd_force_pass(void* ctx, MhdState* s, int64_t n, void* stream);
    `dst`): PySPH's Integrator.compute_accelerations. */
 int mhd_rhs(void* ctx, const MhdState* src, MhdState* dst, int64_t n, MhdRhsStats* stats, void* stream);
 
-/* ---- timestep (src/solver.py:40,61; src/application.py:134-147) ----
+/* ---- timestep (src/solver.py:40,61; src/equations.py:570-585) ----
    dt = min_i dt_adapt_i, clipped so that t + dt <= tf.  Writes dt to the
    device scalar the corrector reads and to *dt_host (synchronising) when
    dt_host is non-null. */
@@ -213,9 +213,10 @@ int mhd_timestep(void* ctx, const MhdState* s, int64_t n, double t, double* dt_h
    NaN if some dt_adapt is non-positive or non-finite.  Scratch is a
    file-scope __device__ array (32 KiB) kept on every GPU that loads the
    library; n above MHD_NOALLOC_MAX_N is rejected with MHD_ERR_INVALID.  The
-   first call on a device looks up the array's device address and clears it
-   (make it before any stream capture); calls that overlap on the GPU race on
-   the shared array. */
+   first call on a device looks up the array's device address (make it before
+   any stream capture; the address is kept, so do not call again on a device
+   after cudaDeviceReset); calls that overlap on the GPU race on the shared
+   array. */
 #define MHD_NOALLOC_MAX_N 67108864
 int mhd_timestep_noalloc(const double* dt_adapt, int64_t n, double t, double tf, double* dt_out, void* stream);
 

@@ -8,8 +8,16 @@
 //     r0 = {m, rho, 1/rho, omega}        r1 = {p omega/rho^2, alpha1 v_wave, v_wave, p}
 //     r2 = {upred, vpred, wpred, epred}  r3 = {au', av', aw', 1/h}   (a' = previous RHS)
 //     r4 = {Bx, By, Bz, psi c_h}         r5 = {Bx/rho, By/rho, Bz/rho, |B/rho|^2/mu0}
-//   and an FP64 {x, y, z, h} record, so pair geometry and the neighbour
-//   test stay FP64 (bit-identical neighbour sets) in both precisions.
+//   and an FP64 {x, y, z, h} record.  The FP64 form takes pair geometry
+//   from that record and applies the exact FP64 neighbour rule of the
+//   oracle (r^2 < (R h_i)^2 or r^2 < (R h_j)^2), so its neighbour sets are
+//   bit-identical to the reference's.  The FP32 form takes geometry from the
+//   packed cell-relative FP32 positions and tests r^2 < (R max(h_i, h_j))^2
+//   in FP32: a pair within ~1e-7 (relative) of the cut-off may be admitted
+//   or rejected differently from the exact rule.  Every compact kernel
+//   vanishes there, so the sums change by nothing but FP32 rounding; for the
+//   Gaussian kernels (truncated at R = 3, W(R) ~ 1e-4 W(0)) such a pair
+//   changes a sum by at most one truncated-tail term.
 // k_force_pass: CullenDehnenAlphaDiagnostics, MHDAccelerations,
 //   MagneticStressAccelerations and MagneticStateRates as one loop over the
 //   compacted neighbour list (src/equations.py:318-354, 217-275, 149-195,

@@ -4,23 +4,28 @@
 // being captured, embedders whose allocator policy forbids the library from
 // taking device memory on its own, and real-time loops that must not hit the
 // driver's allocator.  For them mhd_timestep_noalloc computes
-// dt = min_i dt_adapt_i clipped so that t + dt <= tf (the adaptive rule of
-// src/application.py:134-147 and src/equations.py:570-585) with its scratch in
-// a file-scope __device__ array instead of a context's workspace.
+// dt = min_i dt_adapt_i clipped so that t + dt <= tf -- the adaptive rule of
+// AdaptiveTimestep (src/equations.py:570-585) and the solver's step choice
+// with its stop at tf (src/solver.py:40,61) -- with its scratch in a
+// file-scope __device__ array instead of a context's workspace.
 //
 // The array (g_dt_scratch) holds one partial minimum per block for up to
 // kNoAllocMaxBlocks blocks of kNoAllocTile elements, plus a completion
 // counter: n is limited to MHD_NOALLOC_MAX_N = 67,108,864.  Every GPU that
 // loads the library keeps the array (32 KiB + 8 B) until the process exits.
+// A __device__ array starts zeroed when the module loads, so the counter
+// needs no clearing before the first call; the last block of every call
+// returns it to zero.
 //
 // Host code must not pass the symbol itself to a kernel: on the host it is a
 // stand-in, not a device address.  The first call on each device looks up
-// the real address with cudaGetSymbolAddress (that device current) and
-// zeroes the counter; make that first call before any stream capture.  All
-// calls share the one array, which keeps the last call's partials; the
-// counter is returned to zero by every call.  Calls that overlap on the GPU
-// (concurrent streams on one device) race on the array and must be
-// serialised by the caller.
+// the real address with cudaGetSymbolAddress (that device current) and keeps
+// it for the life of the process; make that first call before any stream
+// capture.  After cudaDeviceReset on a device the kept address is stale and
+// the entry point must not be called on that device again.  All calls share
+// the one array, which keeps the last call's partials.  Calls that overlap
+// on the GPU (concurrent streams on one device) race on the array and must
+// be serialised by the caller.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -98,7 +103,8 @@ __global__ void __launch_bounds__(kNoAllocThreads) k_dt_noalloc(const double* __
   }
 }
 
-// Device address of g_dt_scratch for each device, looked up once.
+// Device address of g_dt_scratch for each device, looked up once (the
+// array is zero from module load; nothing is cleared here).
 static std::mutex g_setup_mutex;
 static unsigned long long* g_scratch_addr[256] = {};
 
@@ -114,11 +120,6 @@ static int scratch_for_current_device(unsigned long long** out) {
     const cudaError_t e = cudaGetSymbolAddress(&p, g_dt_scratch);
     if (e != cudaSuccess) {
       set_library_error(std::string("mhd_timestep_noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
-      return MHD_ERR_CUDA;
-    }
-    const cudaError_t z = cudaMemset(p, 0, sizeof(g_dt_scratch));
-    if (z != cudaSuccess) {
-      set_library_error(std::string("mhd_timestep_noalloc: clearing the scratch failed: ") + cudaGetErrorString(z));
       return MHD_ERR_CUDA;
     }
     g_scratch_addr[dev] = (unsigned long long*)p;

@@ -1,20 +1,15 @@
-// mhd_pairs.cu -- FP64 neighbour passes of the SPMHD right-hand side (sm_100a).
+// mhd_pairs.cu -- density pass and neighbour lists of the SPMHD right-hand
+// side (sm_100a).
 //
 // k_density_pass: one pass of DensityIteration (src/equations.py:14-94) --
 //   pair sums rho = sum m W(h_i), dwdh = sum m dW/dh(h_i), then the Newton
 //   update of h with the [0.8h, 1.2h] clip and the convergence test, one
 //   thread per particle of the cell-sorted order, h read from one buffer and
 //   written to another (Jacobi semantics of PySPH's post_loop).
-// k_force_prologue: DensityFromSmoothingLength, IdealGasEOS and
-//   MagneticStateReconstruction (src/equations.py:109-118, 97-106, 474-485)
-//   plus the per-particle factors the pair loop reuses.
-// k_force_pass: CullenDehnenAlphaDiagnostics, MHDAccelerations,
-//   MagneticStressAccelerations and MagneticStateRates as one neighbour loop
-//   (src/equations.py:318-354, 217-275, 149-195, 507-559) with the per-particle
-//   epilogue of their post_loops, SmoothingLengthRateFromForceDivergence,
-//   EnergyLimiter, DivBCorrection and AdaptiveTimestep
-//   (src/equations.py:357-429, 278-280, 133-140, 562-567, 588-624, 570-585).
-//   Gather formulation: each thread writes only its own particle, no atomics.
+// k_build_lists & co.: the compacted neighbour lists every pair pass reads
+//   (PySPH's NNPS, src/application.py:63-78), carried across sorts where
+//   they stay valid.
+// The fused force pass (groups G2-G10) is in mhd_force.cu.
 #include <cuda_runtime.h>
 
 #include "mhd_common.cuh"

@@ -2,10 +2,14 @@
 
 Class names, constructor arguments and module constants are those of the
 reference's ``src/equations.py``; a group list built from them (by
-``MHDScheme.get_equations``) is what ``src.acceleration`` recognises and runs
-as the fused sm_100a kernels.  The arithmetic of every class lives in
-``csrc/mhd_pairs.cu`` (pair loops, post-loops) and ``csrc/mhd_integrate.cu``;
-each class below names the kernel stage that executes it.
+``MHDScheme.get_equations``) is what ``src.scheme.compile_groups`` recognises
+and runs as the fused sm_100a kernels.  The arithmetic of every class lives
+in the CUDA sources: ``DensityIteration`` in ``csrc/mhd_pairs.cu``
+(``k_density_pass``); ``DensityFromSmoothingLength``, ``IdealGasEOS`` and
+``MagneticStateReconstruction`` in the force prologue and every other
+equation of groups G4-G10 in the force pass (``csrc/mhd_force.cu``); the
+integrator stages in ``csrc/mhd_integrate.cu``.  Each class below names the
+kernel stage that executes it.
 """
 
 DENSITY_TOLERANCE = 1.0e-4  # src/equations.py:6

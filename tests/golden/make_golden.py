@@ -3,7 +3,8 @@
 Test infrastructure.  Run in the development container only (it imports the
 read-only reference checkout, which does not exist on GPU machines):
 
-    python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py /path/to/reference [case ...]
+    MHD_REFERENCE_ROOT=/path/to/reference python tests/golden/make_golden.py
 
 The physics executed here is the reference's own code, imported unchanged:
 the 14 ``Equation`` classes of ``src/equations.py``, ``MHDStep`` of
@@ -322,7 +323,9 @@ CASES = {
 }
 
 if __name__ == "__main__":
-    REF = sys.argv[1] if len(sys.argv) > 1 and not sys.argv[1] in CASES else "/root/reference"
+    REF = sys.argv[1] if len(sys.argv) > 1 and sys.argv[1] not in CASES else os.environ.get("MHD_REFERENCE_ROOT")
+    if not REF or not os.path.isdir(REF):
+        sys.exit("usage: make_golden.py /path/to/reference [case ...]  (or set MHD_REFERENCE_ROOT)")
     only = [a for a in sys.argv[1:] if a in CASES]
     ref = _import_reference(REF)
     for name, fn in CASES.items():

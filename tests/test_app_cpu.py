@@ -14,7 +14,9 @@ import pytest
 from golden_io import GOLDEN
 
 PKG = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "pysph-mhd_b200")
-REFERENCE_CONFIGS = "/root/reference/configs"
+# the reference checkout, when present (development machines only): its
+# configs/*.toml must load unchanged
+REFERENCE_CONFIGS = os.path.join(os.environ.get("MHD_REFERENCE_ROOT", ""), "configs")
 
 
 def test_close_packed_lattice_matches_reference_function():
@@ -46,7 +48,8 @@ def test_benchmark_configs_load_and_build_cases():
     assert 294_000 < sizes["mhdshock2d"] < 296_000  # 4096 x 128 left + 8:1 right
 
 
-@pytest.mark.skipif(not os.path.isdir(REFERENCE_CONFIGS), reason="reference checkout not present")
+@pytest.mark.skipif(not os.environ.get("MHD_REFERENCE_ROOT") or not os.path.isdir(REFERENCE_CONFIGS),
+                    reason="MHD_REFERENCE_ROOT does not name a reference checkout")
 def test_reference_toml_files_load_unchanged():
     from src.config import load_config
     from src.run import CASES

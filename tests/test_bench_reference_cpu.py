@@ -2,8 +2,9 @@
 shape, on the same metric, unit and workload as the B200 arm.
 
 ``bench.py --impl reference`` times the oracle (the reference's equations
-restated in C, OpenMP) on a bounded sample of the blast; it needs no GPU,
-so its line can be checked here on a small sample.
+restated in C, OpenMP) on the blast workload itself (--ref-n 0, the
+default); it needs no GPU, so its line can be checked here on a small
+lattice passed with --ref-n, which the line names in timed_workload.
 """
 
 import json
@@ -28,6 +29,8 @@ def test_reference_arm_prints_one_contract_line():
     assert d["impl"] == "reference"
     assert d["metric"] == bench.METRIC and d["unit"] == bench.UNIT and d["higher_is_better"] is True
     assert d["config"]["workload"] == bench.blast_workload(128)
+    # a sample smaller than the workload is named as such
+    assert d["config"]["timed_workload"] == bench.blast_workload(12) and d["config"]["sample_particles"] == 12 ** 3
     assert d["steps"] == 2 and d["warmup"] == 3 and d["value"] > 0
     cpu = d["cpu_baseline"]
     assert cpu["kind"] == "port" and cpu["cores"] >= 1 and cpu["value"] == d["value"]

@@ -87,3 +87,56 @@ def test_noalloc_timestep_rejects_oversize_and_flags_invalid_steps():
     assert rc == -1 and b"MHD_NOALLOC_MAX_N" in lib.mhd_last_error(None)
     bad = torch.tensor([1e-3, 0.0, 2e-3], dtype=torch.float64, device="cuda")
     assert np.isnan(_without_allocation(lib, bad, 0.0, 1.0))
+
+
+_FRESH_PROCESS = r"""
+import ctypes, sys
+import torch
+sys.path[:0] = sys.argv[1:]
+from src import _abi
+lib = _abi.load()
+torch.cuda.set_device(0)
+gen = torch.Generator(device="cuda").manual_seed(11)
+side = torch.cuda.Stream()  # non-blocking with respect to the legacy default stream
+out = torch.full((2,), -1.0, dtype=torch.float64, device="cuda")
+with torch.cuda.stream(side):
+    a = torch.rand(3_000_017, dtype=torch.float64, device="cuda", generator=gen) + 1e-3
+    b = torch.rand(70_001, dtype=torch.float64, device="cuda", generator=gen) + 1e-3
+    st = ctypes.c_void_p(side.cuda_stream)
+    for k, v in enumerate((a, b)):
+        rc = lib.mhd_timestep_noalloc(ctypes.c_void_p(v.data_ptr()), v.numel(), 0.0, 1e30,
+                                      ctypes.c_void_p(out[k:].data_ptr()), st)
+        assert rc == 0, lib.mhd_last_error(None)
+side.synchronize()
+assert float(out[0]) == float(a.min()) and float(out[1]) == float(b.min()), (out.tolist(), float(a.min()), float(b.min()))
+print("FRESH_OK")
+"""
+
+
+def test_noalloc_first_calls_on_a_nonblocking_stream_in_a_fresh_process():
+    """The first two calls of a process, both on a stream that does not wait
+    for the legacy default stream: the scratch needs no set-up work ordered
+    before them."""
+    import os
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    res = subprocess.run([sys.executable, "-c", _FRESH_PROCESS, root, os.path.join(root, "pysph-mhd_b200")],
+                         capture_output=True, text=True, timeout=300)
+    assert res.returncode == 0 and "FRESH_OK" in res.stdout, res.stdout + res.stderr
+
+
+def test_noalloc_timestep_large_input_with_ragged_tail():
+    """About 10^7 values (610 blocks, the last one partly filled), twice in a
+    row, against torch's own minimum."""
+    from src import _abi
+
+    lib = _abi.load()
+    gen = torch.Generator(device="cuda").manual_seed(5)
+    n = 10_000_019
+    assert n % 16384 and n // 16384 < 4096
+    for _ in range(2):
+        a = torch.rand(n, dtype=torch.float64, device="cuda", generator=gen) + 1e-4
+        a[n - 3] = 1e-6  # the minimum in the ragged tail
+        assert _without_allocation(lib, a, 0.0, 1e30) == float(a.min()) == 1e-6
