@@ -88,6 +88,9 @@ def lib():
                                      ctypes.c_void_p, ctypes.c_double]
         _lib.oracle_rhs.argtypes = [ctypes.POINTER(OracleParams), ctypes.c_int64, ctypes.POINTER(ctypes.c_void_p),
                                     ctypes.c_void_p]
+        _lib.oracle_neighbour_counts.restype = ctypes.c_int
+        _lib.oracle_neighbour_counts.argtypes = [ctypes.POINTER(OracleParams), ctypes.c_int64,
+                                                 ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p]
         _lib.oracle_min_dt.restype = ctypes.c_double
         _lib.oracle_min_dt.argtypes = [ctypes.c_int64, ctypes.POINTER(ctypes.c_void_p)]
     return _lib
@@ -167,6 +170,13 @@ class Oracle:
 
     def min_dt(self, s: State):
         return lib().oracle_min_dt(s.n, s._ptrs)
+
+    def neighbour_counts(self, s: State) -> np.ndarray:
+        """Per-particle neighbour counts (exact rule, self included) from the
+        oracle's own cell search with the current h."""
+        out = np.zeros(s.n, dtype=np.int32)
+        lib().oracle_neighbour_counts(ctypes.byref(self.cp), s.n, s._ptrs, out.ctypes.data_as(ctypes.c_void_p))
+        return out
 
     # --- src/application.py:99-108 ---
     @staticmethod

@@ -870,6 +870,25 @@ int oracle_rhs(const OracleParams* pr, int64_t n, double** P, int32_t* itype) {
   return passes;
 }
 
+/* Neighbour count of every particle under the rule of the pair loops
+   (r_ij < R max(h_i, h_j), minimum image, self included) with the current
+   h: the oracle's own cell search, for checking the device's lists. */
+int oracle_neighbour_counts(const OracleParams* pr, int64_t n, double** P, int32_t* counts) {
+  set_threads(pr);
+  Kern K = {pr->kernel, pr->dim, kernel_norm(pr->kernel, pr->dim), radius_scale(pr->kernel)};
+  Grid g;
+  grid_build(&g, pr, n, P, K.R * max_h(n, A(h)));
+#pragma omp parallel
+  {
+    int64_t* nb = (int64_t*)malloc(sizeof(int64_t) * NBR_MAX * 8);
+#pragma omp for schedule(dynamic, 256)
+    for (int64_t i = 0; i < n; i++) counts[i] = (int32_t)neighbours(&g, pr, P, K.R, i, nb);
+    free(nb);
+  }
+  grid_free(&g);
+  return 0;
+}
+
 /* MHDStep.initialize (src/integrator.py:12-35) */
 static void stage_initialize(int64_t n, double** P) {
 #pragma omp parallel for schedule(static)

@@ -443,6 +443,63 @@ __global__ void __launch_bounds__(kForceShapes[SHAPE][0], kForceShapes[SHAPE][1]
   (void)rhoi;
 }
 
+// 2-D complement of the Cullen-Dehnen moments.  In a 2-D layout the force
+// pass takes the fallback branch of the limiter (the 3x3 determinant is
+// zero), which needs neither R_ab nor the off-diagonal A_ab, so it does not
+// sum R_xx, R_xy, R_yy, A_xy, A_yx, A_zx, A_zy (A_z* is non-zero when a field
+// component along z gives a z acceleration).  When the caller asks for the cd_*
+// diagnostics this pass sums them as CullenDehnenAlphaDiagnostics.loop does
+// (src/equations.py:318-354), in FP64 over the neighbour list, and writes
+// them over the force pass's zeros.
+template <int K>
+__global__ void __launch_bounds__(128) k_cd_complement_2d(int n, DevParams P, NbrList L, const Grid* __restrict__ grids,
+                                                          const int* __restrict__ inst, const double* __restrict__ x,
+                                                          const double* __restrict__ y, const double* __restrict__ h,
+                                                          const double* __restrict__ m, const double* __restrict__ aup,
+                                                          const double* __restrict__ avp,
+                                                          const double* __restrict__ awp, double* __restrict__ rxx,
+                                                          double* __restrict__ rxy, double* __restrict__ ryy,
+                                                          double* __restrict__ axy, double* __restrict__ ayx,
+                                                          double* __restrict__ azx, double* __restrict__ azy) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const Grid& G = grid_of(grids, inst, i);
+  const double xi = x[i], yi = y[i], hi = h[i];
+  const double h1 = 1.0 / hi, fac = P.norm * (h1 * h1), rhi2 = rh2_exact(P.R, hi);
+  const double aui = aup[i], avi = avp[i], awi = awp[i];
+  double sxx = 0.0, sxy = 0.0, syy = 0.0, sab = 0.0, sba = 0.0, szx = 0.0, szy = 0.0;
+  const int cnt = L.cnt[i];
+  const int* __restrict__ row = L.idx + (size_t)(i >> 5) * L.cap * 32 + (i & 31);
+  for (int k = 0; k < cnt; k++) {
+    const int j = row[k * 32];
+    const double dx = min_image(xi - x[j], G.L[0], G.half[0], G.periodic[0]);
+    const double dy = min_image(yi - y[j], G.L[1], G.half[1], G.periodic[1]);
+    const double r2 = r2_exact(dx, dy, 0.0);
+    if (!(r2 < rhi2)) continue;  // W(h_i) and its gradient vanish beyond R h_i
+    const double r = sqrt(r2);
+    if (!(r > kPairDistanceEpsilon)) continue;
+    double w, dw;
+    w_dw<K>(r * h1, 2, w, dw);
+    const double t = fac * dw * h1 / r;
+    const double runx = m[j] * (t * dx), runy = m[j] * (t * dy);
+    sxx += -dx * runx;
+    sxy += -dx * runy;
+    syy += -dy * runy;
+    sab += (aui - aup[j]) * runy;
+    sba += (avi - avp[j]) * runx;
+    const double daz = awi - awp[j];
+    szx += daz * runx;
+    szy += daz * runy;
+  }
+  if (rxx) rxx[i] = sxx;
+  if (rxy) rxy[i] = sxy;
+  if (ryy) ryy[i] = syy;
+  if (axy) axy[i] = sab;
+  if (ayx) ayx[i] = sba;
+  if (azx) azx[i] = szx;
+  if (azy) azy[i] = szy;
+}
+
 // ------------------------------------------------------------- dispatch
 template <class T>
 static ForceRecords<T> records(Ctx* c) {
@@ -523,21 +580,43 @@ static void force_launch(Ctx* c, MhdState* s, int n, cudaStream_t st) {
   }
 }
 
+template <int K>
+static void cd_complement_launch(Ctx* c, MhdState* s, int n, cudaStream_t st) {
+  k_cd_complement_2d<K><<<(n + 127) / 128, 128, 0, st>>>(n, c->P, c->lists(), c->d_grids, c->inst, s->x, s->y, s->h,
+                                                         s->m, c->au_prev, c->av_prev, c->aw_prev, s->cd_rxx,
+                                                         s->cd_rxy, s->cd_ryy, s->cd_axy, s->cd_ayx, s->cd_azx,
+                                                         s->cd_azy);
+}
+
 void launch_force_pass(Ctx* c, MhdState* s, int n, cudaStream_t st) {
   if (n <= 0) return;
   if (c->timing) launch_pair_stats(c, s, n, st);  // outside the timed scope
-  TimedScope ts(c, MHD_TIMING_FORCE, st);
-  const int d3 = c->P.dim == 3;
-  switch (c->P.kernel) {
-    case MHD_KERNEL_CUBIC: d3 ? force_launch<0, 3>(c, s, n, st) : force_launch<0, 2>(c, s, n, st); break;
-    case MHD_KERNEL_QUINTIC: d3 ? force_launch<1, 3>(c, s, n, st) : force_launch<1, 2>(c, s, n, st); break;
-    case MHD_KERNEL_WENDLAND_C2: d3 ? force_launch<2, 3>(c, s, n, st) : force_launch<2, 2>(c, s, n, st); break;
-    case MHD_KERNEL_WENDLAND_C4: d3 ? force_launch<3, 3>(c, s, n, st) : force_launch<3, 2>(c, s, n, st); break;
-    case MHD_KERNEL_WENDLAND_C6: d3 ? force_launch<4, 3>(c, s, n, st) : force_launch<4, 2>(c, s, n, st); break;
-    case MHD_KERNEL_GAUSSIAN: d3 ? force_launch<5, 3>(c, s, n, st) : force_launch<5, 2>(c, s, n, st); break;
-    default: d3 ? force_launch<6, 3>(c, s, n, st) : force_launch<6, 2>(c, s, n, st); break;
+  {
+    TimedScope ts(c, MHD_TIMING_FORCE, st);
+    const int d3 = c->P.dim == 3;
+    switch (c->P.kernel) {
+      case MHD_KERNEL_CUBIC: d3 ? force_launch<0, 3>(c, s, n, st) : force_launch<0, 2>(c, s, n, st); break;
+      case MHD_KERNEL_QUINTIC: d3 ? force_launch<1, 3>(c, s, n, st) : force_launch<1, 2>(c, s, n, st); break;
+      case MHD_KERNEL_WENDLAND_C2: d3 ? force_launch<2, 3>(c, s, n, st) : force_launch<2, 2>(c, s, n, st); break;
+      case MHD_KERNEL_WENDLAND_C4: d3 ? force_launch<3, 3>(c, s, n, st) : force_launch<3, 2>(c, s, n, st); break;
+      case MHD_KERNEL_WENDLAND_C6: d3 ? force_launch<4, 3>(c, s, n, st) : force_launch<4, 2>(c, s, n, st); break;
+      case MHD_KERNEL_GAUSSIAN: d3 ? force_launch<5, 3>(c, s, n, st) : force_launch<5, 2>(c, s, n, st); break;
+      default: d3 ? force_launch<6, 3>(c, s, n, st) : force_launch<6, 2>(c, s, n, st); break;
+    }
+    c->launches++;
   }
-  c->launches++;
+  if (c->P.dim == 2 && (s->cd_rxx || s->cd_rxy || s->cd_ryy || s->cd_axy || s->cd_ayx || s->cd_azx || s->cd_azy)) {
+    switch (c->P.kernel) {
+      case MHD_KERNEL_CUBIC: cd_complement_launch<0>(c, s, n, st); break;
+      case MHD_KERNEL_QUINTIC: cd_complement_launch<1>(c, s, n, st); break;
+      case MHD_KERNEL_WENDLAND_C2: cd_complement_launch<2>(c, s, n, st); break;
+      case MHD_KERNEL_WENDLAND_C4: cd_complement_launch<3>(c, s, n, st); break;
+      case MHD_KERNEL_WENDLAND_C6: cd_complement_launch<4>(c, s, n, st); break;
+      case MHD_KERNEL_GAUSSIAN: cd_complement_launch<5>(c, s, n, st); break;
+      default: cd_complement_launch<6>(c, s, n, st); break;
+    }
+    c->launches++;
+  }
 }
 
 }  // namespace mhd

@@ -176,6 +176,119 @@ __global__ void __launch_bounds__(128) k_density_pass(int n, int pass, DevParams
   }
 }
 
+// ----------------------------------------- density pass with diagnostics
+// The density-pass outputs that no later equation reads (src/equations.py:
+// 24-50, 80-86): rho_sum, arho (scaled by the new omega when a particle is
+// finalised), grhox/y/z and dwdh.  Written when the caller passes any of the
+// arrays.  As in the reference every particle is summed in every pass --
+// converged ones too, with their frozen h -- so after the group these hold
+// the last pass's sums; the post-loop (Newton update, convergence test) runs
+// for unconverged particles only and is the fast pass's, op for op, so h,
+// omega and converged do not depend on whether diagnostics are written.
+// Pair arithmetic is FP64 in both precision forms.
+struct DensityDiag {
+  double *arho, *grhox, *grhoy, *grhoz, *dwdh;
+  const double *upred, *vpred, *wpred;
+};
+
+template <int K, int DIM>
+__global__ void __launch_bounds__(128) k_density_pass_diag(int n, int pass, DevParams P, NbrList L,
+                                                           const double* __restrict__ x, const double* __restrict__ y,
+                                                           const double* __restrict__ z, const double* __restrict__ m,
+                                                           const double* __restrict__ h_in, double* __restrict__ h_out,
+                                                           const double* __restrict__ h0,
+                                                           double* __restrict__ rho_sum, double* __restrict__ omega,
+                                                           double* __restrict__ converged,
+                                                           const Grid* __restrict__ grids, const int* __restrict__ inst,
+                                                           DensityDiag D, DevScalars* sc) {
+  if (sc->relist) return;
+  if (pass > 0) {
+    const bool stop = !P.iterate || pass >= P.max_iter || (pass >= P.min_iter && sc->n_unconverged[pass - 1] == 0);
+    if (stop) return;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicMax(&sc->passes_done, pass + 1);
+  const int stride = gridDim.x * blockDim.x;
+  constexpr bool compact = K <= MHD_KERNEL_WENDLAND_C6;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const double hi = h_in[i];
+    const Grid& G = grid_of(grids, inst, i);
+    const double xi = x[i], yi = y[i], zi = DIM == 3 ? z[i] : 0.0;
+    const double h1 = 1.0 / hi;
+    const double fac = P.norm * (DIM == 2 ? h1 * h1 : h1 * h1 * h1);
+    const double fgh = -fac * h1;
+    const double rhi2 = rh2_exact(P.R, hi);
+    const double ui = D.upred[i], vi = D.vpred[i], wi = D.wpred[i];
+    double rsum = 0.0, dsum = 0.0, ar = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
+    const int cnt = L.cnt[i];
+    const int* __restrict__ row = L.idx + (size_t)(i >> 5) * L.cap * 32 + (i & 31);
+    for (int k = 0; k < cnt; k++) {
+      const int j = row[k * 32];
+      const double dx = min_image(xi - x[j], G.L[0], G.half[0], G.periodic[0]);
+      const double dy = min_image(yi - y[j], G.L[1], G.half[1], G.periodic[1]);
+      const double dz = DIM == 3 ? min_image(zi - z[j], G.L[2], G.half[2], G.periodic[2]) : 0.0;
+      const double r2 = r2_exact(dx, dy, dz);
+      bool nb = r2 < rhi2;
+      if (!compact && !nb) nb = r2 < rh2_exact(P.R, h_in[j]);
+      if (!nb) continue;
+      const double r = sqrt(r2);
+      const double mj = m[j];
+      const double q = r * h1;
+      double w, dw;
+      w_dw<K>(q, DIM, w, dw);
+      // DWI = fac dw h1 / r * XIJ (zero at r <= 1e-12), GHI = -fac h1 (dw q + d w)
+      const double t = r > kPairDistanceEpsilon ? fac * dw * h1 / r : 0.0;
+      const double dwx = t * dx, dwy = t * dy, dwz = t * dz;
+      const double vdw = (ui - D.upred[j]) * dwx + (vi - D.vpred[j]) * dwy + (wi - D.wpred[j]) * dwz;
+      rsum += mj * (w * fac);
+      ar += mj * vdw;
+      gx += mj * dwx;
+      gy += mj * dwy;
+      gz += mj * dwz;
+      dsum += mj * (fgh * (dw * q + w * (double)DIM));
+    }
+    bool unconv = false;
+    if (converged[i] != 1.0) {
+      // post_loop (src/equations.py:53-86), as in density_particle
+      const double mi = m[i];
+      const double rhoi = mi / pow_dim<DIM>(hi / P.hfact);
+      const double dhdrhoi = -hi / ((double)DIM * rhoi);
+      const double omegai = 1.0 - dhdrhoi * dsum;
+      const double om = 1.0 / omegai;
+      omega[i] = om;
+      const double func = rhoi - rsum;
+      const double dfdh1 = omegai > 0.0 ? dhdrhoi / omegai : dhdrhoi / fabs(omegai + kMachineEps);
+      double hnew = hi - func * dfdh1;
+      if (hnew > 1.2 * hi) hnew = 1.2 * hi;
+      else if (hnew < 0.8 * hi) hnew = 0.8 * hi;
+      const double diff = fabs(hnew - hi) / h0[i];
+      const bool finalize = ((diff < kDensityTolerance) && (omegai > 0.0) && (hi > 0.0)) || !P.iterate;
+      double hout;
+      if (!finalize) {
+        hout = hnew;
+        converged[i] = 0.0;
+        unconv = true;
+      } else {
+        ar *= om;
+        hout = P.hfact * pow(mi / rsum, 1.0 / (double)DIM);
+        converged[i] = 1.0;
+      }
+      h_out[i] = hout;
+      if (!(hout <= L.hlim[i])) atomicExch(&sc->relist, 1);
+    } else {
+      h_out[i] = hi;
+    }
+    rho_sum[i] = rsum;
+    if (D.arho) D.arho[i] = ar;
+    if (D.grhox) D.grhox[i] = gx;
+    if (D.grhoy) D.grhoy[i] = gy;
+    if (D.grhoz) D.grhoz[i] = gz;
+    if (D.dwdh) D.dwdh[i] = dsum;
+    const unsigned act = __activemask();
+    const unsigned b = __ballot_sync(act, unconv);
+    if (b && (int)(threadIdx.x & 31) == __ffs(act) - 1) atomicAdd(&sc->n_unconverged[pass], __popc(b));
+  }
+}
+
 // ------------------------------------------------------- neighbour lists
 // A list holds every j within the margin-enlarged symmetric radius
 // R * max(h_i, h_j) * (1 + margin) of the h it was built with.  The tests run
@@ -845,6 +958,13 @@ static void density_launch(Ctx* c, MhdState* s, int n, int pass, const double* h
   // wave of blocks, so a skipped pass costs little in a captured run.
   const int full = (n + 127) / 128;
   const int grid = pass < 2 ? full : std::min(full, c->num_sms * 8);
+  if (s->arho || s->grhox || s->grhoy || s->grhoz || s->dwdh) {
+    const DensityDiag D{s->arho, s->grhox, s->grhoy, s->grhoz, s->dwdh, s->upred, s->vpred, s->wpred};
+    k_density_pass_diag<K, DIM><<<grid, 128, 0, st>>>(n, pass, c->P, c->lists(), s->x, s->y, s->z, s->m, h_in, h_out,
+                                                      s->h0, s->rho_sum, s->omega, s->converged, c->d_grids, c->inst,
+                                                      D, c->d_sc);
+    return;
+  }
   if (c->P.fp32) {
     k_density_pass<K, DIM, float><<<grid, 128, 0, st>>>(n, pass, c->P, c->lists(), s->x, s->y, s->z, s->m, h_in, h_out,
                                                         s->h0, s->rho_sum, s->omega, s->converged, c->d_grids, c->inst,

@@ -70,9 +70,15 @@ class MHDApplication:
         raise NotImplementedError
 
     # --- reference hooks ---
+    # The reference evaluates every equation of its groups, diagnostics
+    # included (StrainDiagnostics' dvdx_*, the Cullen-Dehnen moments, the
+    # density pass's arho/grho/dwdh); so does this application unless a
+    # caller sets this to False before setup() (the state is the same).
+    diagnostics = True
+
     def create_particles(self, device="cuda"):
         arrays = self.create_mhd_particles()
-        pa = ParticleArray("fluid", arrays, device=device)
+        pa = ParticleArray("fluid", arrays, device=device, diagnostics=self.diagnostics)
         self.scheme.setup_properties(pa)
         return [pa]
 

@@ -5,6 +5,14 @@ Stands in for PySPH's ``ParticleArray`` + ``.gpu`` mirror for the hot path:
 copies, ``pa.push(name, array)`` uploads.  The neighbour sort permutes the
 particles (like PySPH's ``reorder_particles``), so every field the sort
 carries has a second buffer; ``gid`` tracks particle identity.
+
+Diagnostic outputs -- the Cullen-Dehnen moments ``cd_*``, ``xilimiter``,
+``divvdt``, the strain rates ``dvdx_*`` and the density pass's ``arho``,
+``grhox/y/z`` and ``dwdh`` -- are read by no equation.  With
+``diagnostics=True`` the array hands them to the kernels, which then write
+every one of them as the reference does (the density passes then also
+re-sum converged particles, so ``rho_sum`` is the last pass's sum); by
+default they are left out of the kernel state and not written.
 """
 
 from __future__ import annotations
@@ -18,10 +26,18 @@ from . import _abi
 from .particles import property_names
 
 
+DIAGNOSTIC_FIELDS = frozenset(
+    ("xilimiter", "divvdt", "arho", "grhox", "grhoy", "grhoz", "dwdh")
+    + tuple(f"cd_{k}" for k in "rxx rxy rxz ryy ryz rzz".split())
+    + tuple(f"cd_{q}{a}{b}" for q in "va" for a in "xyz" for b in "xyz")
+    + tuple(f"dvdx_{a}{b}" for a in "xyz" for b in "xyz"))
+
+
 class ParticleArray:
-    def __init__(self, name: str, arrays: dict, device="cuda"):
+    def __init__(self, name: str, arrays: dict, device="cuda", diagnostics: bool = False):
         _abi.load()
         self.name = name
+        self.diagnostics = bool(diagnostics)
         n = len(np.asarray(arrays["x"]))
         self.n = n
         self.device = torch.device(device)
@@ -78,6 +94,8 @@ class ParticleArray:
         S = _abi.state_type()
         s = S()
         for f in _abi.STATE_FIELDS:
+            if not self.diagnostics and f in DIAGNOSTIC_FIELDS:
+                continue
             src = self._spare if (spare and f in self._spare) else self._t
             t = src.get(f)
             if t is not None:

@@ -4,8 +4,8 @@ FP64 tolerances: the device sums neighbours in cell order with fused
 multiply-adds, the fixtures in ascending index order without them, so
 well-conditioned fields agree to rounding (relative 1e-9 after one
 right-hand side, 1e-8 after a few steps).  Fields where the reference is
-itself roundoff-sensitive are held to the reference's reordering spread
-(see ``compare.py``).
+itself roundoff-sensitive (named per fixture in ``SPREAD_FIELDS``) are held
+to the reference's reordering spread (see ``compare.py``).
 """
 
 import numpy as np
@@ -14,7 +14,7 @@ import pytest
 torch = pytest.importorskip("torch")
 
 import oracle  # noqa: E402
-from compare import assert_close, scales  # noqa: E402
+from compare import ROUNDOFF_SENSITIVE, assert_close, scales  # noqa: E402
 from golden_io import CASES, load, section  # noqa: E402
 
 pytestmark = pytest.mark.gpu
@@ -27,6 +27,14 @@ STEP_FIELDS = ("x", "y", "z", "u", "v", "w", "e", "h", "rho", "p", "cs", "Bx", "
 
 RTOL_RHS = 1e-9
 RTOL_STEP = 1e-8
+
+# Fields that may fall back to the reference's reordering spread, per
+# fixture.  The unjittered 2-D Orszag-Tang fixture starts with div v = curl v
+# = 0 on its stagnation lines, where the reference's own alpha_loc is 0/0 and
+# flips between 0 and 1 with the neighbour order; from the first step on
+# every evolved field carries those flips (u differs by ~2e-3 between two
+# orders of the same FP64 sums).  Every other fixture: the switch only.
+SPREAD_FIELDS = {"ot2d": ROUNDOFF_SENSITIVE | frozenset(STEP_FIELDS) | frozenset(WARM_FIELDS)}
 
 
 def _engine(case, precision="fp64"):
@@ -67,7 +75,8 @@ def test_warmup_and_initial_dt_match_reference_fixture(case):
     sc = scales(section(d, "ic"), warm["cs"])
     spread = _oracle_spread(d, p, [])[0]
     got = _by_gid(eng.pa, WARM_FIELDS)
-    assert_close(got, warm, WARM_FIELDS, RTOL_RHS, sc, spread, f"{case} warm-up")
+    assert_close(got, warm, WARM_FIELDS, RTOL_RHS, sc, spread, f"{case} warm-up",
+                 SPREAD_FIELDS.get(case, ROUNDOFF_SENSITIVE))
     assert eng.density_passes == list(d["density_passes"][:3])
     dt0 = eng.initial_dt()
     assert abs(dt0 - float(d["dt0"])) <= RTOL_RHS * float(d["dt0"])
@@ -86,7 +95,8 @@ def test_pec_steps_match_reference_fixture(case):
         eng.step(dt)
         ref = section(d, f"step{k}")
         got = _by_gid(eng.pa, STEP_FIELDS)
-        assert_close(got, ref, STEP_FIELDS, RTOL_STEP, sc, spread[k], f"{case} step {k}")
+        assert_close(got, ref, STEP_FIELDS, RTOL_STEP, sc, spread[k], f"{case} step {k}",
+                     SPREAD_FIELDS.get(case, ROUNDOFF_SENSITIVE))
         t += dt
         dt_dev = eng.timestep(t)
         if k < len(dts):
@@ -108,7 +118,7 @@ def test_fused_corrector_predictor_loop_matches_pec_steps(case):
     eng.advance(steps)
     ref = section(d, f"step{steps}")
     got = _by_gid(eng.pa, STEP_FIELDS)
-    assert_close(got, ref, STEP_FIELDS, RTOL_STEP, sc, spread, f"{case} fused")
+    assert_close(got, ref, STEP_FIELDS, RTOL_STEP, sc, spread, f"{case} fused", SPREAD_FIELDS.get(case, ROUNDOFF_SENSITIVE))
 
 
 def test_context_rejects_bad_parameters():
