@@ -636,18 +636,17 @@ int mhd_ctx_create(const MhdParams* params, int64_t n_max, void** out) {
             dev_alloc(c, &c->scan_sums, scan_sums_needed(N)) == MHD_OK && dev_alloc(c, &c->h_alt, N) == MHD_OK &&
             dev_alloc(c, &c->au_prev, N) == MHD_OK && dev_alloc(c, &c->av_prev, N) == MHD_OK &&
             dev_alloc(c, &c->aw_prev, N) == MHD_OK && dev_alloc(c, &c->d_sc, 1) == MHD_OK;
-  for (int k = 0; k < 7 && ok; k++) {
-    double* p = nullptr;
-    ok = dev_alloc(c, &p, 4 * ((N + 31) / 32 * 32)) == MHD_OK;
-    if (k == 0) c->rec_pos = p;
-    else c->rec[k - 1] = p;
-  }
   c->n_pad = (N + 31) / 32 * 32;
+  {
+    double* p = nullptr;
+    ok = ok && dev_alloc(c, &p, 32 * c->n_pad) == MHD_OK;  // 256 B per particle
+    c->frec = p;
+  }
   {
     const double rr = radius_scale_of(params->kernel) * params->hfact * (1.0 + c->list_margin);
     const double vol = params->dim == 3 ? 4.0 / 3.0 * M_PI * rr * rr * rr : M_PI * rr * rr;
     const int cap = ((int)(1.5 * vol) + 16 + 7) & ~7;
-    ok = ok && dev_alloc(c, &c->posf, c->n_pad) == MHD_OK && dev_alloc(c, &c->posm, c->n_pad) == MHD_OK &&
+    ok = ok && dev_alloc(c, &c->posf, c->n_pad) == MHD_OK && dev_alloc(c, &c->posq, c->n_pad) == MHD_OK &&
          dev_alloc(c, &c->cellc, c->n_pad) == MHD_OK;
     ok = ok && dev_alloc(c, &c->nbr_hlim, c->n_pad) == MHD_OK && dev_alloc(c, &c->big_idx, c->n_pad) == MHD_OK &&
          dev_alloc(c, &c->new_of_old, c->n_pad) == MHD_OK && dev_alloc(c, &c->nbr_mark, c->n_pad) == MHD_OK;
@@ -698,10 +697,9 @@ int mhd_ctx_destroy(void* ctx) {
   cudaFree(c->au_prev);
   cudaFree(c->av_prev);
   cudaFree(c->aw_prev);
-  cudaFree(c->rec_pos);
-  for (void* p : c->rec) cudaFree(p);
+  cudaFree(c->frec);
   cudaFree(c->posf);
-  cudaFree(c->posm);
+  cudaFree(c->posq);
   cudaFree(c->cellc);
   for (Ctx::ListSlot& S : c->slots) {
     cudaFree(S.idx);

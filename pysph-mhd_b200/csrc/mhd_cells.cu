@@ -364,28 +364,32 @@ __global__ void __launch_bounds__(256) k_cell_starts(int n, int ncells, const ui
 }
 
 // ------------------------------------------------------- packed positions
-// FP32 position relative to the particle's cell origin (|error| <= 2^-24
-// cell widths) plus h (posf) or plus m (posm, the density pass's record),
-// and the cell coordinates packed into one int: the
-// FP32 geometry of a pair is (pos_i - pos_j) + (cell_i - cell_j) * cell width.
+// posf: FP32 position relative to the particle's cell origin (|error| <=
+// 2^-24 cell widths) plus h, with the cell coordinates packed into one int
+// (cellc): the geometry of the list build, (pos_i - pos_j) + (cell_i -
+// cell_j) * cell width.  posq: the fixed-point position of the FP32 pair
+// passes (Grid::fx_lo; the pair displacement is one wrapped integer
+// difference per axis) plus m.
 template <int DIM>
 __global__ void __launch_bounds__(256) k_pack_positions(int n, const Grid* __restrict__ grids,
                                                         const int* __restrict__ inst, const double* __restrict__ x,
                                                         const double* __restrict__ y, const double* __restrict__ z,
                                                         const double* __restrict__ h,
                                                         const double* __restrict__ m, float4* __restrict__ posf,
-                                                        float4* __restrict__ posm, int* __restrict__ cellc) {
+                                                        uint4* __restrict__ posq, int* __restrict__ cellc) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const Grid& g = grid_of(grids, inst, i);
-  const int cx = cell_coord(g, 0, x[i]);
-  const int cy = cell_coord(g, 1, y[i]);
-  const int cz = DIM == 3 ? cell_coord(g, 2, z[i]) : 0;
-  const float rx = (float)(x[i] - (g.lo[0] + cx * g.cs[0]));
-  const float ry = (float)(y[i] - (g.lo[1] + cy * g.cs[1]));
-  const float rz = DIM == 3 ? (float)(z[i] - (g.lo[2] + cz * g.cs[2])) : 0.f;
+  const double xi = x[i], yi = y[i], zi = DIM == 3 ? z[i] : 0.0;
+  const int cx = cell_coord(g, 0, xi);
+  const int cy = cell_coord(g, 1, yi);
+  const int cz = DIM == 3 ? cell_coord(g, 2, zi) : 0;
+  const float rx = (float)(xi - (g.lo[0] + cx * g.cs[0]));
+  const float ry = (float)(yi - (g.lo[1] + cy * g.cs[1]));
+  const float rz = DIM == 3 ? (float)(zi - (g.lo[2] + cz * g.cs[2])) : 0.f;
   posf[i] = make_float4(rx, ry, rz, (float)h[i]);
-  posm[i] = make_float4(rx, ry, rz, (float)m[i]);
+  posq[i] = make_uint4(fixed_coord(g, 0, xi), fixed_coord(g, 1, yi), DIM == 3 ? fixed_coord(g, 2, zi) : 0u,
+                       __float_as_uint((float)m[i]));
   cellc[i] = pack_cell<DIM>(cx, cy, cz);
 }
 
@@ -393,10 +397,10 @@ void launch_pack_positions(Ctx* c, const MhdState* s, int n, cudaStream_t st) {
   if (n <= 0) return;
   if (c->P.dim == 3)
     k_pack_positions<3><<<(n + 255) / 256, 256, 0, st>>>(n, c->d_grids, c->inst, s->x, s->y, s->z, s->h, s->m,
-                                                         c->posf, c->posm, c->cellc);
+                                                         c->posf, c->posq, c->cellc);
   else
     k_pack_positions<2><<<(n + 255) / 256, 256, 0, st>>>(n, c->d_grids, c->inst, s->x, s->y, s->z, s->h, s->m,
-                                                         c->posf, c->posm, c->cellc);
+                                                         c->posf, c->posq, c->cellc);
   c->launches++;
 }
 

@@ -37,6 +37,15 @@ struct Grid {
   double cut;     // search reach of a normal particle: R (1 + margin) h_plan (>= the planned cutoff)
   float csf[3];   // cell widths in FP32 (packed-position geometry)
   float h_bigf;   // particles with FP32 h above this are "big": they search an extended stencil
+  // Fixed-point frame of the FP32 pair passes: a coordinate is stored as
+  // u = (x - fx_lo) * fx_scale modulo 2^32 (uint32), so x_i - x_j is the
+  // wrapped 32-bit difference times fx_len.  On a periodic axis the frame is
+  // the box (2^32 units = L): the wrapped difference is the minimum image.
+  // On an open axis it is four times the particles' extent, centred on them,
+  // so no difference wraps.  Zero scale on axes beyond dim.
+  double fx_lo[3];
+  double fx_scale[3];
+  float fx_len[3];
 };
 
 __device__ __forceinline__ const Grid& grid_of(const Grid* __restrict__ grids, const int* __restrict__ inst, int i) {
@@ -414,7 +423,29 @@ __host__ __device__ inline int plan_instance(const PlanSpec& S, int n, double hm
   g.cut = hplan < 1e30 ? mul_rn(mul_rn(S.R, add_rn(1.0, S.list_margin)), hplan) : cutoff;
   if (g.cut < cutoff) g.cut = cutoff;
   g.ncells = g.nc[0] * g.nc[1] * g.nc[2];
+  for (int a = 0; a < 3; a++) {
+    if (a >= S.dim) {
+      g.fx_lo[a] = 0.0;
+      g.fx_scale[a] = 0.0;
+      g.fx_len[a] = 0.f;
+      continue;
+    }
+    double span = S.periodic[a] ? S.L[a] : mul_rn(4.0, extent[a]);
+    if (!(span > 1e-250)) span = 1e-250;  // a degenerate open axis (every particle on one coordinate)
+    g.fx_lo[a] = S.periodic[a] ? S.lo[a] : add_rn(g.lo[a], -mul_rn(1.5, extent[a]));
+    g.fx_scale[a] = div_rn(4294967296.0, span);
+    g.fx_len[a] = (float)div_rn(span, 4294967296.0);
+  }
   return MHD_OK;
+}
+
+// Fixed-point coordinate of x along axis a (see Grid::fx_lo).
+__device__ __forceinline__ unsigned fixed_coord(const Grid& g, int a, double x) {
+  return (unsigned)(unsigned long long)(long long)floor((x - g.fx_lo[a]) * g.fx_scale[a]);
+}
+// FP32 displacement from two fixed-point coordinates.
+__device__ __forceinline__ float fixed_delta(const Grid& g, int a, unsigned ui, unsigned uj) {
+  return __int2float_rn((int)(ui - uj)) * g.fx_len[a];
 }
 
 // Mean h from the fixed-point sum of h / h_max.

@@ -3,21 +3,18 @@
 //
 // k_force_prologue: DensityFromSmoothingLength, IdealGasEOS and
 //   MagneticStateReconstruction (src/equations.py:109-118, 97-106, 474-485),
-//   then the per-particle factors the pair loop reuses, packed into
-//   4-vectors of the pair precision T (sorted order):
-//     r0 = {m, rho, 1/rho, omega}        r1 = {p omega/rho^2, alpha1 v_wave, v_wave, p}
-//     r2 = {upred, vpred, wpred, epred}  r3 = {au', av', aw', 1/h}   (a' = previous RHS)
-//     r4 = {Bx, By, Bz, psi c_h}         r5 = {Bx/rho, By/rho, Bz/rho, |B/rho|^2/mu0}
-//   and an FP64 {x, y, z, h} record.  The FP64 form takes pair geometry
-//   from that record and applies the exact FP64 neighbour rule of the
-//   oracle (r^2 < (R h_i)^2 or r^2 < (R h_j)^2), so its neighbour sets are
-//   bit-identical to the reference's.  The FP32 form takes geometry from the
-//   packed cell-relative FP32 positions and tests r^2 < (R max(h_i, h_j))^2
-//   in FP32: a pair within ~1e-7 (relative) of the cut-off may be admitted
-//   or rejected differently from the exact rule.  Every compact kernel
-//   vanishes there, so the sums change by nothing but FP32 rounding; for the
-//   Gaussian kernels (truncated at R = 3, W(R) ~ 1e-4 W(0)) such a pair
-//   changes a sum by at most one truncated-tail term.
+//   then one packed record per particle (ForceRec, sorted order) holding
+//   everything a neighbour contributes.  The FP64 form takes pair geometry
+//   from the record's FP64 positions and applies the exact FP64 neighbour
+//   rule of the oracle (r^2 < (R h_i)^2 or r^2 < (R h_j)^2), so its
+//   neighbour sets are bit-identical to the reference's.  The FP32 form
+//   takes geometry from fixed-point positions (one wrapped 32-bit
+//   difference per axis, the minimum image for free) and tests
+//   r^2 < (R max(h_i, h_j))^2 in FP32: a pair within ~1e-7 (relative) of the
+//   cut-off may be admitted or rejected differently from the exact rule.
+//   Every compact kernel vanishes there, so the sums change by nothing but
+//   FP32 rounding; for the Gaussian kernels (truncated at R = 3, W(R) ~ 1e-4
+//   W(0)) such a pair changes a sum by at most one truncated-tail term.
 // k_force_pass: CullenDehnenAlphaDiagnostics, MHDAccelerations,
 //   MagneticStressAccelerations and MagneticStateRates as one loop over the
 //   compacted neighbour list (src/equations.py:318-354, 217-275, 149-195,
@@ -25,9 +22,12 @@
 //   EnergyLimiter, DivBCorrection and AdaptiveTimestep (src/equations.py:
 //   357-429, 278-280, 133-140, 562-567, 588-624, 570-585) per particle in
 //   FP64.  Gather formulation: one thread per particle, no atomics on forces.
-//   With T = float the momentum, energy, induction and divergence sums are
-//   Kahan-compensated; the Cullen-Dehnen moments feed a clipped limiter and
-//   use plain FP32 sums.
+//   The pair terms are the reference's, regrouped around the displacement
+//   x_ij (grad_i r-hat = omega_i |grad W_i| r-hat = omega_i t_i x_ij) so that
+//   r-hat is never formed and the thermal and isotropic magnetic pressures
+//   share one coefficient.  With T = float the momentum, energy, induction
+//   and divergence sums are Kahan-compensated; the Cullen-Dehnen moments
+//   feed a clipped limiter and use plain FP32 sums.
 #include <cuda_runtime.h>
 
 #include "mhd_common.cuh"
@@ -84,14 +84,24 @@ __device__ __forceinline__ float fast_sqrt(float x) { return x > 0.f ? x * rsqrt
 __device__ __forceinline__ double fast_sqrt(double x) { return sqrt(x); }
 
 // ------------------------------------------------------------ records
+// The force-pass records of the particles, in the cell-sorted order: seven
+// planes of four-vectors of the pair precision T (structure of arrays, so
+// the 32 lanes of a warp, which mostly read consecutive neighbours, load a
+// plane's entries from a few whole lines):
+//   q0  FP32 {x, y, z fixed point (Grid::fx_lo), h}; FP64 {x, y, z, h}
+//   q1  {m, rho, 1/rho, omega}
+//   q2  {Ptot, alpha1 v_wave, v_wave, 1/rho^2}
+//   q3  {upred, vpred, wpred, epred}
+//   q4  {au', av', aw', 1/h}                     (a' = previous RHS)
+//   q5  {Bx, By, Bz, p}
+//   q6  {Bx, By, Bz / (rho sqrt(mu0)), psi c_h / rho^2}
+// with Ptot = p / rho^2 + |B|^2 / (2 mu0 rho^2), the thermal and isotropic
+// magnetic pressure terms that MHDAccelerations and
+// MagneticStressAccelerations both weight by omega grad W.
+constexpr int kForcePlanes = 7;
 template <class T>
-struct ForceRecords {
-  const V4<double>* pos;  // {x, y, z, h}
-  const V4<T>* r[6];
-  const float4* posf;     // packed FP32 positions (geometry of the FP32 form)
-  const int* cellc;
-  const Grid* grids;  // per-instance geometry
-  const int* inst;    // instance of each particle (null: one instance)
+struct ForceRec {
+  V4<T>* q[kForcePlanes];
 };
 
 template <class T>
@@ -108,10 +118,8 @@ struct ForceOut {
 template <int DIM, class T>
 __global__ void __launch_bounds__(256) k_force_prologue(int n, DevParams P, MhdState s, const double* __restrict__ aup,
                                                         const double* __restrict__ avp,
-                                                        const double* __restrict__ awp, V4<double>* __restrict__ pos,
-                                                        V4<T>* __restrict__ r0, V4<T>* __restrict__ r1,
-                                                        V4<T>* __restrict__ r2, V4<T>* __restrict__ r3,
-                                                        V4<T>* __restrict__ r4, V4<T>* __restrict__ r5,
+                                                        const double* __restrict__ awp, const Grid* __restrict__ grids,
+                                                        const int* __restrict__ inst, ForceRec<T> rec,
                                                         float4* __restrict__ posf) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -130,17 +138,25 @@ __global__ void __launch_bounds__(256) k_force_prologue(int n, DevParams P, MhdS
   s.Bxpred[i] = bx;
   s.Bypred[i] = by;
   s.Bzpred[i] = bz;
-  const double vw = sqrt(cs * cs + (bx * bx + by * by + bz * bz) / (P.mu0 * rho));
-  const double ir = 1.0 / rho;
+  const double b2 = bx * bx + by * by + bz * bz;
+  const double vw = sqrt(cs * cs + b2 / (P.mu0 * rho));
+  const double ir = 1.0 / rho, ir2 = ir * ir;
   const double om = s.omega[i];
-  const double brx = bx * ir, bry = by * ir, brz = bz * ir;
-  pos[i] = V4<double>{s.x[i], s.y[i], s.z[i], h};
-  r0[i] = V4<T>{(T)s.m[i], (T)rho, (T)ir, (T)om};
-  r1[i] = V4<T>{(T)(p * ir * ir * om), (T)(s.alpha1[i] * vw), (T)vw, (T)p};
-  r2[i] = V4<T>{(T)s.upred[i], (T)s.vpred[i], (T)s.wpred[i], (T)s.epred[i]};
-  r3[i] = V4<T>{(T)aup[i], (T)avp[i], (T)awp[i], (T)(1.0 / h)};
-  r4[i] = V4<T>{(T)bx, (T)by, (T)bz, (T)(s.psipred[i] * (P.clean_speed * vw))};
-  r5[i] = V4<T>{(T)brx, (T)bry, (T)brz, (T)((brx * brx + bry * bry + brz * brz) * P.inv_mu0)};
+  const double bs = ir * sqrt(P.inv_mu0);
+  const double x = s.x[i], y = s.y[i], z = DIM == 3 ? s.z[i] : 0.0;
+  if constexpr (sizeof(T) == 4) {
+    const Grid& G = grid_of(grids, inst, i);
+    rec.q[0][i] = V4<T>{__uint_as_float(fixed_coord(G, 0, x)), __uint_as_float(fixed_coord(G, 1, y)),
+                        DIM == 3 ? __uint_as_float(fixed_coord(G, 2, z)) : 0.f, (float)h};
+  } else {
+    rec.q[0][i] = V4<T>{(T)x, (T)y, (T)z, (T)h};
+  }
+  rec.q[1][i] = V4<T>{(T)s.m[i], (T)rho, (T)ir, (T)om};
+  rec.q[2][i] = V4<T>{(T)(p * ir2 + 0.5 * b2 * P.inv_mu0 * ir2), (T)(s.alpha1[i] * vw), (T)vw, (T)ir2};
+  rec.q[3][i] = V4<T>{(T)s.upred[i], (T)s.vpred[i], (T)s.wpred[i], (T)s.epred[i]};
+  rec.q[4][i] = V4<T>{(T)aup[i], (T)avp[i], (T)awp[i], (T)(1.0 / h)};
+  rec.q[5][i] = V4<T>{(T)bx, (T)by, (T)bz, (T)p};
+  rec.q[6][i] = V4<T>{(T)(bx * bs), (T)(by * bs), (T)(bz * bs), (T)(s.psipred[i] * (P.clean_speed * vw) * ir2)};
 }
 
 // Launch shapes (threads per block, minimum resident blocks per SM): the
@@ -150,27 +166,32 @@ constexpr int kForceShapeCount = 4;
 
 template <int K, int DIM, class T, int SHAPE>
 __global__ void __launch_bounds__(kForceShapes[SHAPE][0], kForceShapes[SHAPE][1])
-    k_force_pass(int n, DevParams P, NbrList L, ForceRecords<T> R, ForceOut<T> o) {
+    k_force_pass(int n, DevParams P, NbrList L, const Grid* __restrict__ grids, const int* __restrict__ inst,
+                 const ForceRec<T> rec, ForceOut<T> o) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const Grid& G = grid_of(R.grids, R.inst, i);
-  const V4<double> pi = R.pos[i];
-  const V4<T> i0 = R.r[0][i], i1 = R.r[1][i], i2 = R.r[2][i], i3 = R.r[3][i], i4 = R.r[4][i], i5 = R.r[5][i];
-  const double xi = pi.x, yi = pi.y, zi = DIM == 3 ? pi.z : 0.0, hi = pi.w;
-  const double rhi2 = rh2_exact(P.R, hi);
-  const T h1i = i3.w;
+  const Grid& G = grid_of(grids, inst, i);
+  const V4<T> pi = rec.q[0][i], i1 = rec.q[1][i], i2 = rec.q[2][i], i3 = rec.q[3][i], i4 = rec.q[4][i],
+              i5 = rec.q[5][i], i6 = rec.q[6][i];
+  const T h1i = i4.w;
   const T norm = prm_t<T>(P.normf, P.norm);
-  const T faci = norm * (DIM == 2 ? h1i * h1i : h1i * h1i * h1i);
-  const T rhoi = i0.y, irhoi = i0.z, omegai = i0.w;
-  const T PI = i1.x, AI = i1.y, vwi = i1.z, p_i = i1.w;
-  const T ui = i2.x, vi = i2.y, wi = i2.z, epi = i2.w;
-  const T aui = i3.x, avi = i3.y, awi = i3.z;
-  const T bxi = i4.x, byi = i4.y, bzi = i4.z, psichi = i4.w;
-  const T brxi = i5.x, bryi = i5.y, brzi = i5.z, bro2i = i5.w;
-  const T rhoi2inv = irhoi * irhoi;
+  // grad W(h_i) = faci1 dw(q) / r * x_ij
+  const T faci1 = norm * (DIM == 2 ? h1i * h1i * h1i : (h1i * h1i) * (h1i * h1i));
+  const T rhoi = i1.y, irhoi = i1.z, omegai = i1.w;
+  const T ptoti = i2.x, AI = i2.y, vwi = i2.z, irho2i = i2.w;
+  const T ui = i3.x, vi = i3.y, wi = i3.z, epi = i3.w;
+  const T aui = i4.x, avi = i4.y, awi = i4.z;
+  const T bxi = i5.x, byi = i5.y, bzi = i5.z, p_i = i5.w;
+  const T bsxi = i6.x, bsyi = i6.y, bszi = i6.z, psii = i6.w;
+  const T pr2i = p_i * irho2i;
   const T av = prm_t<T>(P.avf, P.av), ac = prm_t<T>(P.acf, P.ac), ar = prm_t<T>(P.arf, P.ar),
           inv_mu0 = prm_t<T>(P.inv_mu0f, P.inv_mu0);
   const T two = (T)2, half = (T)0.5, zero = (T)0;
+  // neighbour test r^2 < (R max(h_i, h_j))^2: FP32 on the FP32 form, the
+  // exact FP64 rule of the oracle on the FP64 form
+  const float Rf = P.Rf;
+  const float rhi2f = (Rf * (float)pi.w) * (Rf * (float)pi.w);
+  const double rhi2 = rh2_exact(P.R, (double)pi.w);
 
   // Cullen-Dehnen moments (src/equations.py:329-354)
   T rxx = 0, rxy = 0, rxz = 0, ryy = 0, ryz = 0, rzz = 0;
@@ -181,13 +202,6 @@ __global__ void __launch_bounds__(kForceShapes[SHAPE][0], kForceShapes[SHAPE][1]
 
   const int cnt = L.cnt[i];
   const int* __restrict__ row = L.idx + (size_t)(i >> 5) * L.cap * 32 + (i & 31);
-  float4 pif = make_float4(0.f, 0.f, 0.f, 0.f);
-  int cif = 0;
-  if constexpr (sizeof(T) == 4) {
-    pif = R.posf[i];
-    cif = R.cellc[i];
-  }
-  const float Rf = P.Rf;
   // the list entry is fetched one pair ahead, and every record of a pair is
   // requested before its neighbour test, so a pair waits on one memory
   // round trip instead of three (entry, position, records)
@@ -202,52 +216,52 @@ __global__ void __launch_bounds__(kForceShapes[SHAPE][0], kForceShapes[SHAPE][1]
       dtc = fmax(dtc, vwi);
       continue;
     }
-    const V4<T> j0 = ld4(R.r[0] + j), j1 = ld4(R.r[1] + j), j2 = ld4(R.r[2] + j), j3 = ld4(R.r[3] + j);
-    const V4<T> j4 = ld4(R.r[4] + j), j5 = ld4(R.r[5] + j);
-    T dx, dy, dz, r, inv_r0;
+    const V4<T> pj = ld4(rec.q[0] + j), j1 = ld4(rec.q[1] + j), j2 = ld4(rec.q[2] + j), j3 = ld4(rec.q[3] + j);
+    const V4<T> j4 = ld4(rec.q[4] + j), j5 = ld4(rec.q[5] + j), j6 = ld4(rec.q[6] + j);
+    T dx, dy, dz, r, inv_r;
     if constexpr (sizeof(T) == 4) {
-      // FP32 geometry from the packed positions; FP32 neighbour test
-      const float4 pj = __ldg(R.posf + j);
-      rel_dx<DIM>(G, pif, cif, pj, __ldg(R.cellc + j), dx, dy, dz);
+      // FP32 geometry: one wrapped fixed-point difference per axis
+      dx = fixed_delta(G, 0, __float_as_uint(pi.x), __float_as_uint(pj.x));
+      dy = fixed_delta(G, 1, __float_as_uint(pi.y), __float_as_uint(pj.y));
+      dz = DIM == 3 ? fixed_delta(G, 2, __float_as_uint(pi.z), __float_as_uint(pj.z)) : 0.f;
       const float r2 = dx * dx + dy * dy + dz * dz;
-      const float rh = Rf * fmaxf(pif.w, pj.w);
-      if (!(r2 < rh * rh)) continue;
-      inv_r0 = r2 > 0.f ? rsqrtf(r2) : 0.f;
-      r = r2 * inv_r0;
+      const float rhj = Rf * pj.w;
+      if (!(r2 < fmaxf(rhi2f, rhj * rhj))) continue;
+      inv_r = r2 > 0.f ? rsqrtf(r2) : 0.f;
+      r = r2 * inv_r;
     } else {
       // FP64 geometry and the exact neighbour test of the oracle
-      const V4<double> pj = ld4(R.pos + j);
-      const double dxd = min_image(xi - pj.x, G.L[0], G.half[0], G.periodic[0]);
-      const double dyd = min_image(yi - pj.y, G.L[1], G.half[1], G.periodic[1]);
-      const double dzd = DIM == 3 ? min_image(zi - pj.z, G.L[2], G.half[2], G.periodic[2]) : 0.0;
+      const double dxd = min_image((double)pi.x - pj.x, G.L[0], G.half[0], G.periodic[0]);
+      const double dyd = min_image((double)pi.y - pj.y, G.L[1], G.half[1], G.periodic[1]);
+      const double dzd = DIM == 3 ? min_image((double)pi.z - pj.z, G.L[2], G.half[2], G.periodic[2]) : 0.0;
       const double r2d = r2_exact(dxd, dyd, dzd);
       if (!(r2d < rhi2 || r2d < rh2_exact(P.R, pj.w))) continue;
       dx = dxd;
       dy = dyd;
       dz = dzd;
       r = sqrt(r2d);
-      inv_r0 = 0;
+      inv_r = r > 0.0 ? 1.0 / r : 0.0;
     }
-    const T mj = j0.x, rhoj = j0.y, irhoj = j0.z, omegaj = j0.w;
-    const T h1j = j3.w;
-    // DWI = ti * XIJ, DWJ = tj * XIJ (zero at r <= 1e-12)
-    T ti = 0, tj = 0, inv_r = 0;
+    const T mj = j1.x, rhoj = j1.y, irhoj = j1.z, omegaj = j1.w;
+    const T h1j = j4.w;
+    // DWI = ti XIJ, DWJ = tj XIJ (zero at r <= 1e-12); oti, otj carry omega
+    T ti = 0, tj = 0;
     if (r > (T)kPairDistanceEpsilon) {
-      inv_r = sizeof(T) == 4 ? inv_r0 : fast_rcp(r);
       T w, dw;
       w_dw<K>(r * h1i, DIM, w, dw);
-      ti = faci * dw * h1i * inv_r;
+      ti = faci1 * dw * inv_r;
       w_dw<K>(r * h1j, DIM, w, dw);
-      tj = norm * (DIM == 2 ? h1j * h1j : h1j * h1j * h1j) * dw * h1j * inv_r;
+      tj = norm * (DIM == 2 ? h1j * h1j * h1j : (h1j * h1j) * (h1j * h1j)) * dw * inv_r;
     }
-    const T dvx = ui - j2.x, dvy = vi - j2.y, dvz = wi - j2.z;
+    const T oti = omegai * ti, otj = omegaj * tj;
+    const T dvx = ui - j3.x, dvy = vi - j3.y, dvz = wi - j3.z;
     const T vdotx = dvx * dx + dvy * dy + dvz * dz;
 
     // ---- CullenDehnenAlphaDiagnostics.loop
     {
       const T c = mj * ti;
       const T cx = c * dx, cy = c * dy, cz = c * dz;
-      const T dax = aui - j3.x, day = avi - j3.y, daz = awi - j3.z;
+      const T dax = aui - j4.x, day = avi - j4.y, daz = awi - j4.z;
       if (DIM == 3) {
         rxx -= dx * cx; rxy -= dx * cy; rxz -= dx * cz;
         ryy -= dy * cy; ryz -= dy * cz; rzz -= dz * cz;
@@ -260,71 +274,53 @@ __global__ void __launch_bounds__(kForceShapes[SHAPE][0], kForceShapes[SHAPE][1]
       vzx += dvz * cx; vzy += dvz * cy;
       axx += dax * cx; ayy += day * cy;
     }
-    // ---- MHDAccelerations.loop (r-hat is zero below 1e-8 here); its
-    // momentum and energy terms join the magnetic ones below in one
-    // compensated add per sum
-    T mf, fei;
-    {
-      const bool far = r >= (T)kInteractionDistanceEpsilon;
-      const T dot = far ? vdotx * inv_r : zero;
-      const T g6 = far ? r : zero;
-      const T grad_i = omegai * ti * g6;
-      const T grad_j = omegaj * tj * g6;
-      fdiv.add(mj * dot * grad_i);
-      const T pj = j1.w, vwj = j1.z;
-      const T vsig2 = fast_sqrt(fabs(p_i - pj) * fast_rcp(half * (rhoi + rhoj)));
-      T c = vwi - two * dot;
-      c = fmax(c, vwj - two * dot);
-      c = fmax(c, zero);
-      dtc = fmax(dtc, c);
-      T fcoef = PI * ti + j1.x * tj;
-      fei = mj * PI * ti * vdotx;
-      if (dot < zero) {
-        const T vsigav_i = fmax(AI - two * dot, zero);
-        const T vsigav_j = fmax(j1.y - two * dot, zero);
-        const T qi = -half * irhoi * vsigav_i * dot * av;
-        const T qj = -half * irhoj * vsigav_j * dot * av;
-        fcoef += qi * omegai * ti + qj * omegaj * tj;
-        fei += mj * qi * dot * grad_i;
-      }
-      mf = mj * fcoef;
-      const T eij = epi - j2.w;
-      fei += ac * vsig2 * eij * (half * mj * (irhoi * grad_i + irhoj * grad_j));
+    // ---- MHDAccelerations, MagneticStressAccelerations and
+    // MagneticStateRates loops, in the displacement x_ij instead of r-hat:
+    // grad_i r-hat = omega_i ti x_ij = oti x_ij wherever grad_i != 0.
+    // MHDAccelerations drops r-hat (and so dot, the viscosity, conduction
+    // and div v terms) below r = 1e-8.
+    const bool far = r >= (T)kInteractionDistanceEpsilon;
+    const T vdf = far ? vdotx : zero;  // (v_ij . r-hat) r
+    const T dot = vdf * inv_r;
+    // artificial viscosity (v_ij . r-hat < 0)
+    T qi = zero, qj = zero;
+    if (dot < zero) {
+      qi = -half * irhoi * fmax(AI - two * dot, zero) * dot * av;
+      qj = -half * irhoj * fmax(j2.y - two * dot, zero) * dot * av;
     }
-    // ---- MagneticStressAccelerations.loop and MagneticStateRates.loop
-    {
-      const T rux = dx * inv_r, ruy = dy * inv_r, ruz = dz * inv_r;
-      const T g8 = r > (T)kPairDistanceEpsilon ? r : zero;
-      const T grad_i = omegai * ti * g8;
-      const T grad_j = omegaj * tj * g8;
-      const T gradp = mj * half * (bro2i * grad_i + j5.w * grad_j);
-      const T si = (brxi * rux + bryi * ruy + brzi * ruz) * grad_i;
-      const T sj = (j5.x * rux + j5.y * ruy + j5.z * ruz) * grad_j;
-      const T ms = mj * inv_mu0;
-      const T bxj = j4.x, byj = j4.y, bzj = j4.z;
-      const T proj_bi = bxi * rux + byi * ruy + bzi * ruz;
-      const T proj_bj = bxj * rux + byj * ruy + bzj * ruz;
-      const T dbx = bxi - bxj, dby = byi - byj, dbz = bzi - bzj;
-      const T proj_db = dbx * rux + dby * ruy + dbz * ruz;
-      const T delta_b2 = dbx * dbx + dby * dby + dbz * dbz;
-      const T pmi = mj * rhoi2inv * grad_i;
-      const T pmj = mj * irhoj * irhoj * grad_j;
-      const T d_brho = -(pmi * proj_bi);
-      const T projv = vdotx * inv_r;
-      const T tx = dvx - projv * rux, ty = dvy - projv * ruy, tz = dvz - projv * ruz;
-      const T vsig_b = fast_sqrt(tx * tx + ty * ty + tz * tz);
-      const T diss = half * (pmi + pmj) * vsig_b * ar;
-      const T dpsi = pmi * psichi + pmj * j4.w;
-      fx.add(-mf * dx + (-rux * gradp + ms * (brxi * si + j5.x * sj)));
-      fy.add(-mf * dy + (-ruy * gradp + ms * (bryi * si + j5.y * sj)));
-      fz.add(-mf * dz + (-ruz * gradp + ms * (brzi * si + j5.z * sj)));
-      bxr.add(d_brho * dvx + diss * dbx - dpsi * rux);
-      byr.add(d_brho * dvy + diss * dby - dpsi * ruy);
-      bzr.add(d_brho * dvz + diss * dbz - dpsi * ruz);
-      fe.add(fei + (-half * delta_b2 * diss * inv_mu0));
-      dbs.add(pmi * proj_bi + pmj * proj_bj);
-      dbd.add(-mj * proj_db * grad_i);
-    }
+    dtc = fmax(dtc, fmax(vwi, j2.z) - two * dot);
+    // momentum: -x_ij m_j (oti (Ptot_i + q_i) + otj (Ptot_j + q_j)) + the
+    // anisotropic Maxwell stress m_j (b_i (b_i . x_ij) oti + b_j (b_j . x_ij) otj)
+    const T S = oti * (ptoti + qi) + otj * (j2.x + qj);
+    const T ai = oti * (bsxi * dx + bsyi * dy + bszi * dz);
+    const T aj = otj * (j6.x * dx + j6.y * dy + j6.z * dz);
+    fx.add(mj * (-dx * S + (bsxi * ai + j6.x * aj)));
+    fy.add(mj * (-dy * S + (bsyi * ai + j6.y * aj)));
+    fz.add(mj * (-dz * S + (bszi * ai + j6.z * aj)));
+    // div v, energy (thermal, viscous, conduction with v_sig = sqrt(|dp| / rho_bar))
+    const T mo = mj * oti;
+    fdiv.add(mo * vdf);
+    const T vsig2 = fast_sqrt(fabs(p_i - j5.w) * fast_rcp(half * (rhoi + rhoj)));
+    const T rf = far ? r : zero;
+    T fei = mo * (pr2i * vdotx + qi * vdf);
+    fei += ac * vsig2 * (epi - j3.w) * (half * mj * rf * (oti * irhoi + otj * irhoj));
+    // induction, resistivity (v_sig,B = |v_ij - (v_ij . r-hat) r-hat|), cleaning
+    const T xbi = bxi * dx + byi * dy + bzi * dz;
+    const T xbj = j5.x * dx + j5.y * dy + j5.z * dz;
+    const T wi_ = oti * irho2i, wj_ = otj * j2.w;
+    const T pv = vdotx * (inv_r * inv_r);
+    const T tx = dvx - pv * dx, ty = dvy - pv * dy, tz = dvz - pv * dz;
+    const T vsig_b = fast_sqrt(tx * tx + ty * ty + tz * tz);
+    const T diss = half * mj * r * (wi_ + wj_) * vsig_b * ar;
+    const T dbx = bxi - j5.x, dby = byi - j5.y, dbz = bzi - j5.z;
+    const T d_brho = -mj * wi_ * xbi;
+    const T cpsi = mj * (oti * psii + otj * j6.w);
+    bxr.add(d_brho * dvx + diss * dbx - cpsi * dx);
+    byr.add(d_brho * dvy + diss * dby - cpsi * dy);
+    bzr.add(d_brho * dvz + diss * dbz - cpsi * dz);
+    fe.add(fei + (-half * (dbx * dbx + dby * dby + dbz * dbz) * diss * inv_mu0));
+    dbs.add(mj * (wi_ * xbi + wj_ * xbj));
+    dbd.add(-mo * (xbi - xbj));
   }
 
   // ---- per-particle epilogue in FP64
@@ -366,7 +362,7 @@ __global__ void __launch_bounds__(kForceShapes[SHAPE][0], kForceShapes[SHAPE][1]
   const double fac = compression * compression;
   const double denominator = fac + (curlx * curlx + curly * curly + curlz * curlz);
   const double xil = denominator > 0.0 ? fac / denominator : 1.0;
-  const double hid = hi;
+  const double hid = o.h[i];
   const double source = 10.0 * hid * hid * xil * fmax(-divvdt, 0.0);
   const double csi = o.cs[i];
   // alpha clip: reference literal [0, 1] (src/equations.py:428); alpha_min/max extend it
@@ -440,7 +436,6 @@ __global__ void __launch_bounds__(kForceShapes[SHAPE][0], kForceShapes[SHAPE][1]
   o.apsi[i] = apsi;
   o.divBsymm[i] = rhoi_d * dbsv;
   o.divBdiff[i] = dbdv;
-  (void)rhoi;
 }
 
 // 2-D complement of the Cullen-Dehnen moments.  In a 2-D layout the force
@@ -502,28 +497,22 @@ __global__ void __launch_bounds__(128) k_cd_complement_2d(int n, DevParams P, Nb
 
 // ------------------------------------------------------------- dispatch
 template <class T>
-static ForceRecords<T> records(Ctx* c) {
-  ForceRecords<T> R;
-  R.pos = reinterpret_cast<const V4<double>*>(c->rec_pos);
-  for (int k = 0; k < 6; k++) R.r[k] = reinterpret_cast<const V4<T>*>(c->rec[k]);
-  R.posf = c->posf;
-  R.cellc = c->cellc;
-  R.grids = c->d_grids;
-  R.inst = c->inst;
-  return R;
+static ForceRec<T> records(Ctx* c) {
+  ForceRec<T> r;
+  V4<T>* base = reinterpret_cast<V4<T>*>(c->frec);
+  for (int k = 0; k < kForcePlanes; k++) r.q[k] = base + (size_t)k * c->n_pad;
+  return r;
 }
 
 template <class T>
 static void prologue_launch(Ctx* c, MhdState* s, int n, cudaStream_t st) {
-  V4<T>* r[6];
-  for (int k = 0; k < 6; k++) r[k] = reinterpret_cast<V4<T>*>(c->rec[k]);
-  V4<double>* pos = reinterpret_cast<V4<double>*>(c->rec_pos);
+  const ForceRec<T> rec = records<T>(c);
   if (c->P.dim == 3)
-    k_force_prologue<3, T><<<(n + 255) / 256, 256, 0, st>>>(n, c->P, *s, c->au_prev, c->av_prev, c->aw_prev, pos,
-                                                            r[0], r[1], r[2], r[3], r[4], r[5], c->posf);
+    k_force_prologue<3, T><<<(n + 255) / 256, 256, 0, st>>>(n, c->P, *s, c->au_prev, c->av_prev, c->aw_prev,
+                                                            c->d_grids, c->inst, rec, c->posf);
   else
-    k_force_prologue<2, T><<<(n + 255) / 256, 256, 0, st>>>(n, c->P, *s, c->au_prev, c->av_prev, c->aw_prev, pos,
-                                                            r[0], r[1], r[2], r[3], r[4], r[5], c->posf);
+    k_force_prologue<2, T><<<(n + 255) / 256, 256, 0, st>>>(n, c->P, *s, c->au_prev, c->av_prev, c->aw_prev,
+                                                            c->d_grids, c->inst, rec, c->posf);
 }
 
 void launch_force_prologue(Ctx* c, MhdState* s, int n, cudaStream_t st) {
@@ -538,16 +527,17 @@ void launch_force_prologue(Ctx* c, MhdState* s, int n, cudaStream_t st) {
 
 template <int K, int DIM, class T>
 static void force_launch_t(Ctx* c, const ForceOut<T>& o, int n, cudaStream_t st) {
-  // default shapes measured on the 128^3 blast: FP64 uncapped (208-220
-  // registers, no spills), FP32 capped at 128 registers (16 warps per SM)
+  // default shapes measured on the 128^3 blast (FP64 uncapped, FP32 capped
+  // for occupancy); the autotuner may pick another
   const int s = c->force_shape >= 0 ? c->force_shape : (sizeof(T) == 4 ? 2 : 0);
   const int bs = kForceShapes[s][0];
   const int grid = (n + bs - 1) / bs;
+  const ForceRec<T> rec = records<T>(c);
   switch (s) {
-    case 1: k_force_pass<K, DIM, T, 1><<<grid, bs, 0, st>>>(n, c->P, c->lists(), records<T>(c), o); break;
-    case 2: k_force_pass<K, DIM, T, 2><<<grid, bs, 0, st>>>(n, c->P, c->lists(), records<T>(c), o); break;
-    case 3: k_force_pass<K, DIM, T, 3><<<grid, bs, 0, st>>>(n, c->P, c->lists(), records<T>(c), o); break;
-    default: k_force_pass<K, DIM, T, 0><<<grid, bs, 0, st>>>(n, c->P, c->lists(), records<T>(c), o);
+    case 1: k_force_pass<K, DIM, T, 1><<<grid, bs, 0, st>>>(n, c->P, c->lists(), c->d_grids, c->inst, rec, o); break;
+    case 2: k_force_pass<K, DIM, T, 2><<<grid, bs, 0, st>>>(n, c->P, c->lists(), c->d_grids, c->inst, rec, o); break;
+    case 3: k_force_pass<K, DIM, T, 3><<<grid, bs, 0, st>>>(n, c->P, c->lists(), c->d_grids, c->inst, rec, o); break;
+    default: k_force_pass<K, DIM, T, 0><<<grid, bs, 0, st>>>(n, c->P, c->lists(), c->d_grids, c->inst, rec, o);
   }
 }
 

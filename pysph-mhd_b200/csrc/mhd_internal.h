@@ -82,10 +82,10 @@ struct Ctx {
   double* au_prev = nullptr;
   double* av_prev = nullptr;
   double* aw_prev = nullptr;
-  // packed per-particle records of the force pass: FP64 {x, y, z, h} and six
-  // 4-vectors in the pair precision (sized for FP64)
-  void* rec_pos = nullptr;
-  void* rec[6] = {};
+  // packed per-particle records of the force pass (sorted order): 8
+  // four-vectors of the pair precision, 128 B (FP32) or 256 B (FP64) per
+  // particle; sized for FP64
+  void* frec = nullptr;
 
   double* spare[kGatherMax] = {};  // replan buffers, allocated on first use
   double grid_margin = 1.0;        // cells are R * h_cell * grid_margin * (1 + list_margin) wide
@@ -94,7 +94,7 @@ struct Ctx {
   // packed FP32 positions relative to the cell origin, and packed cell
   // coordinates, of the sorted particles (written after every sort)
   float4* posf = nullptr;
-  float4* posm = nullptr;  // {x, y, z relative to the cell, m}: the FP32 density pass
+  uint4* posq = nullptr;  // {x, y, z fixed-point (Grid::fx_lo), m as float bits}: the FP32 density pass
   int* cellc = nullptr;
   int num_sms = 148;       // multiprocessors of the context's device
   int stencil = 2;       // cells are >= list cut-off / stencil wide

@@ -46,8 +46,7 @@ __device__ __forceinline__ bool density_particle(int i, const DevParams& P, cons
                                                  const double* __restrict__ h0, double* __restrict__ rho_sum,
                                                  double* __restrict__ omega, double* __restrict__ converged,
                                                  const Grid* __restrict__ grids, const int* __restrict__ inst,
-                                                 const float4* __restrict__ posm, const int* __restrict__ cellc,
-                                                 DevScalars* sc) {
+                                                 const uint4* __restrict__ posq, DevScalars* sc) {
   const double hi = h_in[i];
   if (converged[i] == 1.0) {
     // Already finalised: its h is frozen; a re-summation would only refresh
@@ -65,14 +64,12 @@ __device__ __forceinline__ bool density_particle(int i, const DevParams& P, cons
   SumT<T> rs, ds;
   const int cnt = L.cnt[i];
   const int* __restrict__ row = L.idx + (size_t)(i >> 5) * L.cap * 32 + (i & 31);
-  // FP32 form: geometry and mass from the packed {x, y, z, m} records;
-  // FP64: exact geometry.
-  float4 pif = make_float4(0.f, 0.f, 0.f, 0.f);
-  int cif = 0;
+  // FP32 form: geometry and mass from the packed {x, y, z fixed point, m}
+  // records; FP64: exact geometry.
+  uint4 piq = make_uint4(0u, 0u, 0u, 0u);
   float rhi2f = 0.f;
   if constexpr (sizeof(T) == 4) {
-    pif = posm[i];
-    cif = cellc[i];
+    piq = posq[i];
     const float rh = (float)P.R * (float)hi;
     rhi2f = rh * rh;
   }
@@ -85,10 +82,11 @@ __device__ __forceinline__ bool density_particle(int i, const DevParams& P, cons
     T r, mj;
     bool nb;
     if constexpr (sizeof(T) == 4) {
-      float dx, dy, dz;
-      const float4 pj = __ldg(posm + j);
-      mj = pj.w;
-      rel_dx<DIM>(G, pif, cif, pj, __ldg(cellc + j), dx, dy, dz);
+      const uint4 pj = __ldg(posq + j);
+      mj = __uint_as_float(pj.w);
+      const float dx = fixed_delta(G, 0, piq.x, pj.x);
+      const float dy = fixed_delta(G, 1, piq.y, pj.y);
+      const float dz = DIM == 3 ? fixed_delta(G, 2, piq.z, pj.z) : 0.f;
       const float r2 = dx * dx + dy * dy + dz * dz;
       nb = r2 < rhi2f;
       if (!compact && !nb) {
@@ -156,8 +154,7 @@ __global__ void __launch_bounds__(128) k_density_pass(int n, int pass, DevParams
                                                       const double* __restrict__ h0, double* __restrict__ rho_sum,
                                                       double* __restrict__ omega, double* __restrict__ converged,
                                                       const Grid* __restrict__ grids, const int* __restrict__ inst,
-                                                      const float4* __restrict__ posm,
-                                                      const int* __restrict__ cellc, DevScalars* sc) {
+                                                      const uint4* __restrict__ posq, DevScalars* sc) {
   // Stop when the iterated group already stopped after pass `pass` (1-based
   // count), or when the neighbour lists no longer cover the current h.
   if (sc->relist) return;
@@ -169,7 +166,7 @@ __global__ void __launch_bounds__(128) k_density_pass(int n, int pass, DevParams
   const int stride = gridDim.x * blockDim.x;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
     const bool unconv = density_particle<K, DIM, T>(i, P, L, x, y, z, m, h_in, h_out, h0, rho_sum, omega,
-                                                    converged, grids, inst, posm, cellc, sc);
+                                                    converged, grids, inst, posq, sc);
     const unsigned act = __activemask();
     const unsigned b = __ballot_sync(act, unconv);
     if (b && (int)(threadIdx.x & 31) == __ffs(act) - 1) atomicAdd(&sc->n_unconverged[pass], __popc(b));
@@ -968,12 +965,12 @@ static void density_launch(Ctx* c, MhdState* s, int n, int pass, const double* h
   if (c->P.fp32) {
     k_density_pass<K, DIM, float><<<grid, 128, 0, st>>>(n, pass, c->P, c->lists(), s->x, s->y, s->z, s->m, h_in, h_out,
                                                         s->h0, s->rho_sum, s->omega, s->converged, c->d_grids, c->inst,
-                                                        c->posm, c->cellc, c->d_sc);
+                                                        c->posq, c->d_sc);
     return;
   }
   k_density_pass<K, DIM, double><<<grid, 128, 0, st>>>(n, pass, c->P, c->lists(), s->x, s->y, s->z, s->m, h_in, h_out,
                                                        s->h0, s->rho_sum, s->omega, s->converged, c->d_grids, c->inst,
-                                                       c->posm, c->cellc, c->d_sc);
+                                                       c->posq, c->d_sc);
 }
 
 #define MHD_DISPATCH(FN, ...)                                                   \
