@@ -117,6 +117,8 @@ int fill_params(Ctx* c, const MhdParams* p) {
   P.arf = (float)P.ar;
   P.inv_mu0f = (float)P.inv_mu0;
   P.fp32 = p->precision == MHD_PRECISION_FP32 ? 1 : 0;
+  const cudaError_t e = configure_force_pass(c);
+  if (e != cudaSuccess) FAIL(MHD_ERR_CUDA, std::string("force pass set-up: ") + cudaGetErrorString(e));
   return MHD_OK;
 }
 
@@ -679,6 +681,7 @@ int mhd_ctx_create(const MhdParams* params, int64_t n_max, void** out) {
   if (const char* m = getenv("MHD_CELL_KAPPA")) c->cell_kappa = std::max(1.0, atof(m));
   if (const char* m = getenv("MHD_LIST_MARGIN")) c->list_margin = std::max(0.005, std::min(0.5, atof(m)));
   if (const char* m = getenv("MHD_LIST_REUSE")) c->list_reuse = atoi(m) != 0;
+  if (const char* m = getenv("MHD_FORCE_STAGED")) c->force_staged = atoi(m) != 0;
   *out = c;
   return MHD_OK;
 }

@@ -99,6 +99,7 @@ struct Ctx {
   int num_sms = 148;       // multiprocessors of the context's device
   int stencil = 2;       // cells are >= list cut-off / stencil wide
   int force_shape = -1;  // launch-shape variant of the force pass (kForceShapes); -1 = per-precision default
+  bool force_staged = true;  // force-pass records staged in shared memory (MHD_FORCE_STAGED=0: register gather)
   double list_cut = 0;   // R * h_max * (1 + list_margin) of the current grid
 
   // compacted neighbour lists (NbrList layout), built with every grid.  The
@@ -205,6 +206,9 @@ void launch_pair_stats(Ctx* c, const MhdState* s, int n, cudaStream_t st);
 // density pass `pass` (0-based) reading h_in, writing h_out
 void launch_density_pass(Ctx* c, MhdState* s, int n, int pass, const double* h_in, double* h_out, cudaStream_t st);
 void launch_finish_density(Ctx* c, MhdState* s, int n, int passes, cudaStream_t st);
+// Raises the dynamic shared-memory limit of the staged force passes for the
+// context's kernel, dimension and precision (set-up only).
+cudaError_t configure_force_pass(Ctx* c);
 void launch_force_prologue(Ctx* c, MhdState* s, int n, cudaStream_t st);
 void launch_force_pass(Ctx* c, MhdState* s, int n, cudaStream_t st);
 
