@@ -52,17 +52,29 @@ for _p in (ROOT, PKG):
 METRIC = "particle-steps/s on 1 B200, FP32/batched vs plain FP64 at stated L2 error"
 UNIT = "particle-steps/s"
 
-# Algorithmic bytes per particle of the fused force pass: reads the FP64
-# {x, y, z, h} record, six 4-vectors of the pair precision and six FP64
-# epilogue inputs (rho omega cs psi p epred), writes 16 FP64 outputs (au av aw
-# ae ah div div_psi dt_cfl dt_adapt dB/dt x3 dpsi/dt divBsymm divBdiff
-# alphaloc); each neighbour record counted once (ideal reuse).
-FORCE_BYTES_PER_PARTICLE = {"fp64": 32 + 6 * 32 + 6 * 8 + 16 * 8, "fp32": 32 + 6 * 16 + 6 * 8 + 16 * 8}
-# FP64 operations per neighbour pair of the force pass and per distance
-# test (add, sub, mul, div, sqrt count 1; fma counts 2), counted from
-# csrc/mhd_pairs.cu.
-FORCE_FLOPS_PER_PAIR = 300
+# Algorithmic bytes per particle of the fused force pass: its seven record
+# planes of four values (FP32: 16 B each, FP64: 32 B), each neighbour's
+# counted once (ideal reuse), the seven FP64 epilogue inputs (rho omega cs
+# psipred p epred h) and the 16 FP64 outputs (au av aw ae ah div div_for_psi
+# dt_cfl dt_adapt aBevol x3 apsi divBsymm divBdiff alphaloc).
+FORCE_BYTES_PER_PARTICLE = {"fp64": 7 * 32 + 7 * 8 + 16 * 8, "fp32": 7 * 16 + 7 * 8 + 16 * 8}
+# Floating-point operations of one neighbour pair of k_force_pass
+# (csrc/mhd_force.cu), counted statically from its source: +, -, *, /,
+# sqrt, rsqrt and reciprocal count 1, a fused multiply-add 2; comparisons,
+# max/min and int -> float conversions are not counted.  Cubic kernel, the
+# pair inside the kernel's outer segment (1 < q <= 2, 7 of 8 pairs on a
+# lattice), the viscosity branch not taken.  FP32: geometry 12, the two
+# kernel gradients 15, omega factors, dv and v.x 10, Cullen-Dehnen moments
+# 55, signal speed 3, pressure coefficient 5, Maxwell projections 12,
+# momentum 27 (three Kahan adds), div v 6, conduction speed 7, energy terms
+# 15, field projections and resistive speed 27, dissipation 6, induction
+# and cleaning terms 9 + 27, energy sum 13, div B sums 14 -- 253, of which
+# 40 are the compensation of the ten Kahan sums; FP64 (plain sums) 223.  A
+# list entry beyond the cut-off costs its geometry (12).  The density pass:
+# 33 per pair in FP32 (geometry 10, kernel 8, two Kahan sums 15).
+FORCE_FLOPS_PER_PAIR = {"fp32": 253, "fp64": 223}
 FORCE_FLOPS_PER_CANDIDATE = 12
+DENSITY_FLOPS_PER_PAIR = {"fp32": 33, "fp64": 25}
 
 
 def blast_case(n: int, precision: str = "fp64"):
@@ -659,7 +671,10 @@ def run_b200(args, rank, world):
     bytes_per_launch = FORCE_BYTES_PER_PARTICLE[args.precision] * n
     hbm_peak, peak_src = measured_peaks()
     achieved_gbs = bytes_per_launch / (force_ms * 1e-3) / 1e9
-    flops = (FORCE_FLOPS_PER_PAIR * head["pairs"] + FORCE_FLOPS_PER_CANDIDATE * head["candidates"]) / args.steps
+    # pairs counts the self pair of every particle, which does no arithmetic
+    pairs_ns = head["pairs"] - n * args.steps
+    flops = (FORCE_FLOPS_PER_PAIR[args.precision] * pairs_ns
+             + FORCE_FLOPS_PER_CANDIDATE * (head["candidates"] - head["pairs"])) / args.steps
     achieved_tf = flops / (force_ms * 1e-3) / 1e12
 
     e2e = run_e2e(args, dev, barrier, dist, world)
@@ -720,42 +735,70 @@ def run_b200(args, rank, world):
 
 
 def run_e2e(args, dev, barrier=lambda: None, dist=False, world=1):
+    """The metric end to end through the reference-facing application:
+    ``MHDApplication`` built from configs/mhdblast3d.toml (the same 128^3
+    blast), its warm-up, then ``MHDSolver.solve`` for K steps with the
+    fused loop (``execution.fused``: captured chunks, device dt).  Timed:
+    the host -> device copy of the whole state from pinned host memory, the
+    K steps, and the device -> host copy of OUTPUT_PROPERTIES at the dump
+    every 20 steps (a post-step callback; no files are written).  One
+    untimed solve first captures the chunk's graph, which the timed solve
+    reuses."""
+    from dataclasses import replace
+
     import torch
 
-    from src.engine import Engine, params_from_dict
-    from src.particle_array import ParticleArray
+    from src.config import load_config
     from src.particles import OUTPUT_PROPERTIES
+    from src.run import CASES
 
-    ic, prm = blast_case(args.n, args.precision)
-    n = args.n ** 3
-    # Warm-up on the device is part of start-up (excluded, as in the metric).
-    eng = Engine(params_from_dict(prm), ParticleArray("fluid", ic, device=dev))
-    eng.warmup()
-    dt = eng.initial_dt()
-    host = {k: torch.empty(n, dtype=v.dtype, pin_memory=True) for k, v in eng.pa.properties.items()}
-    for k, v in eng.pa.properties.items():
-        host[k].copy_(v)
-    out = {k: torch.empty(n, dtype=eng.pa.properties[k].dtype, pin_memory=True) for k in OUTPUT_PROPERTIES}
-    torch.cuda.synchronize()
+    cfg = load_config(os.path.join(PKG, "configs", "mhdblast3d.toml"), {k: v.config_type for k, v in CASES.items()})
     pfreq = 20
-    h2d = sum(t.numel() * t.element_size() for t in host.values())
-    d2h = 0
-    barrier()
-    t0 = time.perf_counter()
-    for k, t in host.items():
-        eng.pa.properties[k].copy_(t, non_blocking=True)
-    t = 0.0
-    for step in range(args.steps):
-        eng.step(dt)
-        t += dt
-        dt = eng.timestep(t)
-        d2h += 8
-        if (step + 1) % pfreq == 0 or step == args.steps - 1:
+    cfg = replace(cfg, case=replace(cfg.case, nx=args.n),
+                  solver=replace(cfg.solver, max_steps=args.steps, pfreq=pfreq),
+                  execution=replace(cfg.execution, precision=args.precision, fused=True))
+    app = CASES[cfg.case.name](cfg)
+    app.diagnostics = False  # the diagnostic outputs no equation reads, as in the device-timed value
+    app.setup(device=dev)
+    app._warm_initial_derivatives(app.solver)  # start-up, excluded as in the metric
+    app._compute_initial_dt(app.solver)
+    pa = app.particles[0]
+    n = pa.n
+    solver = app.solver
+    solver.output_directory = None
+    t0, dt0 = solver.t, solver.dt
+    host = {k: torch.empty(n, dtype=v.dtype, pin_memory=True) for k, v in pa.properties.items()}
+    for k, v in pa.properties.items():
+        host[k].copy_(v)
+    out = {k: torch.empty(n, dtype=pa.properties[k].dtype, pin_memory=True) for k in OUTPUT_PROPERTIES}
+    d2h = [0]
+
+    def pull(sv):
+        if sv.count % pfreq == 0 or sv.count >= sv.max_steps:
             for k in OUTPUT_PROPERTIES:
-                out[k].copy_(eng.pa.properties[k], non_blocking=True)
-                d2h += out[k].numel() * out[k].element_size()
+                out[k].copy_(pa.properties[k], non_blocking=True)
+                d2h[0] += out[k].numel() * out[k].element_size()
             torch.cuda.synchronize()
-    el = time.perf_counter() - t0
+
+    solver.post_step_callbacks.append(pull)
+
+    def run_once():
+        for k, t in host.items():
+            pa.properties[k].copy_(t, non_blocking=True)
+        solver.t, solver.dt, solver.count = t0, dt0, 0
+        solver.initial_acceleration_is_current = True
+        solver.solve()
+        torch.cuda.synchronize()
+
+    run_once()  # captures the chunk's graph
+    d2h[0] = 0
+    h2d = sum(t.numel() * t.element_size() for t in host.values())
+    barrier()
+    torch.cuda.synchronize()
+    t_start = time.perf_counter()
+    run_once()
+    el = time.perf_counter() - t_start
+    steps = solver.count
     if dist:
         # every rank's replica, timed as the slowest rank
         import torch.distributed as tdist
@@ -764,11 +807,12 @@ def run_e2e(args, dev, barrier=lambda: None, dist=False, world=1):
         tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
         el = float(t.item())
     barrier()
-    eng.close()
-    return {"value": world * n * args.steps / el, "unit": UNIT, "h2d_bytes_per_step": world * h2d / args.steps,
-            "d2h_bytes_per_step": world * d2h / args.steps,
-            "path": "ParticleArray push from pinned host + Engine.step (literal MHDStep stages, host dt per step) "
-                    "+ OUTPUT_PROPERTIES pulled every 20 steps and at the end"}
+    app.engine.close()
+    return {"value": world * n * steps / el, "unit": UNIT, "h2d_bytes_per_step": world * h2d / steps,
+            "d2h_bytes_per_step": world * (d2h[0] + 8 * steps) / steps,
+            "path": "MHDApplication (configs/mhdblast3d.toml) -> MHDSolver.solve, fused loop: pinned-host state "
+                    "pushed, K steps in captured chunks with device dt, OUTPUT_PROPERTIES pulled at the dump "
+                    "every 20 steps; diagnostic outputs off"}
 
 
 def main():

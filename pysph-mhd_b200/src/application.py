@@ -104,7 +104,18 @@ class MHDApplication:
         self.solver = self.scheme.solver
         self.solver.particles = self.particles
         prm = self.scheme.kernel_params(self.domain, self.tf)
-        self.engine = Engine(params_from_dict(prm), self.particles[0])
+        # execution.fused: the reference asks PySPH for fused CUDA kernels;
+        # here it selects the fused production loop -- captured runs of
+        # corrector-predictor steps with the adaptive step size kept on the
+        # device (the literal MHDStep stages otherwise)
+        fused = bool(self.config.execution.fused) and self.adaptive_timestep
+        if fused:
+            from .batch import BatchEngine
+
+            self.engine = BatchEngine.single(params_from_dict(prm), self.particles[0])
+        else:
+            self.engine = Engine(params_from_dict(prm), self.particles[0])
+        self.solver.fused = fused
         self.solver.integrator.set_engine(self.engine)
         return self
 

@@ -66,6 +66,20 @@ class BatchEngine(Engine):
         self.tuned = None
         self.set_instances()
 
+    @classmethod
+    def single(cls, params: _abi.MhdParams, pa: ParticleArray, cell_headroom: float = 1.25):
+        """One simulation on the device planner and captured runs: the fused
+        production loop of ``MHDSolver`` (``execution.fused``)."""
+        self = cls.__new__(cls)
+        self.start = np.array([0, pa.n], dtype=np.int64)
+        self.n_inst = 1
+        self.cell_headroom = float(cell_headroom)
+        Engine.__init__(self, params, pa)
+        self.replays = 0
+        self.tuned = None
+        self.set_instances()
+        return self
+
     # ------------------------------------------------------------ set-up
     def set_instances(self):
         """(Re)declare the instances; plans capacities, resets the clocks."""

@@ -49,6 +49,11 @@ class MHDSolver:
         self.pre_step_callbacks = []
         self.post_step_callbacks = []
         self.particles = None
+        # the fused loop (set by MHDApplication from execution.fused): steps
+        # run as captured chunks that end at every dump; callbacks then run
+        # once per chunk
+        self.fused = False
+        self.chunk = 50
 
     def _get_timestep(self):
         if self.adaptive_timestep:
@@ -82,6 +87,32 @@ class MHDSolver:
         self.dt = float(solver_data["dt"])
         self.initial_acceleration_is_current = True
 
+    def _solve_fused(self):
+        """The same loop in captured chunks of at most ``chunk`` steps: each
+        chunk is the predictor of its first step, then fused corrector-
+        predictor steps with dt = min(dt_adapt) (clipped to tf) reduced on
+        the device, the last step finished by its corrector; a chunk ends at
+        every dump, at max_steps, and within two of its steps of tf (the
+        steps there run one by one, so the last is the one clipped to tf)."""
+        eng = self.integrator.engine
+        while (self.tf - self.t) > self._epsilon and self.count < self.max_steps:
+            k = min(self.pfreq - self.count % self.pfreq, self.max_steps - self.count, self.chunk)
+            if (self.tf - self.t) <= 2.0 * k * self.dt:
+                k = 1
+            for cb in self.pre_step_callbacks:
+                cb(self)
+            eng.begin(self.dt, self.t)
+            eng.advance(k, finish=True, capture=k > 1)
+            t, dt = eng.clocks()
+            self.t = float(t[0] + dt[0])
+            self.count += k
+            self._epsilon = EPSILON * self.tf * self.count
+            for cb in self.post_step_callbacks:
+                cb(self)
+            self.dt = self._get_timestep()
+            if self.count % self.pfreq == 0:
+                self.dump_output()
+
     def solve(self, show_progress=False):
         self._epsilon = EPSILON * self.tf
         self.dump_output()
@@ -90,6 +121,10 @@ class MHDSolver:
         else:
             self.integrator.initial_acceleration(self.t, self.dt)
         self.dt = self._get_timestep()
+        if self.fused:
+            self._solve_fused()
+            self.dump_output()
+            return
         while (self.tf - self.t) > self._epsilon and self.count < self.max_steps:
             for cb in self.pre_step_callbacks:
                 cb(self)

@@ -2,7 +2,8 @@
 
 ``src.run.main`` mirrors ``python -m src.run <config>`` (src/run.py:32-39):
 the application warms up, takes the initial dt and runs MHDSolver.solve with
-the literal PEC step; the result must match the oracle driven the same way.
+the fused loop (``execution.fused``) or the literal PEC step; the result must
+match the oracle driven the same way.
 """
 
 import os
@@ -32,13 +33,19 @@ def _small_config(tmp_path, name, nx, steps, extra=""):
     return str(p)
 
 
-def test_run_blast3d_config_matches_oracle(tmp_path):
+@pytest.mark.parametrize("fused", [True, False])
+def test_run_blast3d_config_matches_oracle(tmp_path, fused):
+    # execution.fused: captured chunks of corrector-predictor steps with the
+    # step size on the device; otherwise the literal MHDStep stages
     from src.run import main
 
     path = _small_config(tmp_path, "mhdblast3d", 12, 3)
     text = open(path).read().replace('precision = "fp32"', 'precision = "fp64"')
+    if not fused:
+        text = text.replace("fused = true", "fused = false")
     open(path, "w").write(text)
     app, pa = main([path])
+    assert app.solver.fused is fused
     got = pa.pull("x", "u", "v", "rho", "e", "Bx", "By", "alpha1", "h", order="gid")
     assert app.solver.count == 3
 
