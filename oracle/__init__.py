@@ -91,6 +91,10 @@ def lib():
         _lib.oracle_neighbour_counts.restype = ctypes.c_int
         _lib.oracle_neighbour_counts.argtypes = [ctypes.POINTER(OracleParams), ctypes.c_int64,
                                                  ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p]
+        for fn in (_lib.oracle_predict, _lib.oracle_correct):
+            fn.restype = ctypes.c_int
+            fn.argtypes = [ctypes.POINTER(OracleParams), ctypes.c_int64, ctypes.POINTER(ctypes.c_void_p),
+                           ctypes.c_void_p, ctypes.c_double]
         _lib.oracle_min_dt.restype = ctypes.c_double
         _lib.oracle_min_dt.argtypes = [ctypes.c_int64, ctypes.POINTER(ctypes.c_void_p)]
     return _lib
@@ -167,6 +171,14 @@ class Oracle:
         k = lib().oracle_step(ctypes.byref(self.cp), s.n, s._ptrs, s.itype.ctypes.data, float(dt))
         self.density_passes.append(k)
         return k
+
+    def predict(self, s: State, dt: float):
+        """MHDStep.initialize + stage1 + wrap: the half of one_timestep before its RHS."""
+        lib().oracle_predict(ctypes.byref(self.cp), s.n, s._ptrs, s.itype.ctypes.data, float(dt))
+
+    def correct(self, s: State, dt: float):
+        """MHDStep.stage2 + wrap: the half of one_timestep after its RHS."""
+        lib().oracle_correct(ctypes.byref(self.cp), s.n, s._ptrs, s.itype.ctypes.data, float(dt))
 
     def min_dt(self, s: State):
         return lib().oracle_min_dt(s.n, s._ptrs)

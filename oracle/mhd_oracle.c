@@ -983,6 +983,25 @@ int oracle_step(const OracleParams* pr, int64_t n, double** P, int32_t* itype, d
   return passes;
 }
 
+/* The two halves of PECIntegrator.one_timestep around its right-hand side,
+   for drivers that evaluate the right-hand side themselves (the domain
+   decomposition tests): MHDStep.initialize + stage1 + wrap, and
+   MHDStep.stage2 + wrap (src/integrator.py:12-82). */
+int oracle_predict(const OracleParams* pr, int64_t n, double** P, int32_t* itype, double dt) {
+  set_threads(pr);
+  stage_initialize(n, P);
+  stage_1(pr, n, P, itype, dt);
+  wrap(pr, n, P);
+  return 0;
+}
+
+int oracle_correct(const OracleParams* pr, int64_t n, double** P, int32_t* itype, double dt) {
+  set_threads(pr);
+  stage_2(pr, n, P, itype, dt);
+  wrap(pr, n, P);
+  return 0;
+}
+
 /* min over particles of dt_adapt (the adaptive-timestep rule). */
 double oracle_min_dt(int64_t n, double** P) {
   double m = INFINITY;

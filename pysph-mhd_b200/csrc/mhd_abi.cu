@@ -651,6 +651,7 @@ int mhd_ctx_create(const MhdParams* params, int64_t n_max, void** out) {
     ok = ok && dev_alloc(c, &c->posf, c->n_pad) == MHD_OK && dev_alloc(c, &c->posq, c->n_pad) == MHD_OK &&
          dev_alloc(c, &c->cellc, c->n_pad) == MHD_OK;
     ok = ok && dev_alloc(c, &c->nbr_hlim, c->n_pad) == MHD_OK && dev_alloc(c, &c->big_idx, c->n_pad) == MHD_OK &&
+         dev_alloc(c, &c->app_idx, c->n_pad) == MHD_OK &&
          dev_alloc(c, &c->new_of_old, c->n_pad) == MHD_OK && dev_alloc(c, &c->nbr_mark, c->n_pad) == MHD_OK;
     for (Ctx::ListSlot& S : c->slots)
       ok = ok && dev_alloc(c, &S.cnt, c->n_pad) == MHD_OK && dev_alloc(c, &S.gcnt, c->n_pad) == MHD_OK &&
@@ -716,6 +717,7 @@ int mhd_ctx_destroy(void* ctx) {
   cudaFree(c->nbr_mark);
   for (unsigned* p : c->cell_scr) cudaFree(p);
   cudaFree(c->big_idx);
+  cudaFree(c->app_idx);
   cudaFree(c->nbr_hlim);
   for (double* p : c->spare) cudaFree(p);
   for (auto& e : c->events) {

@@ -96,6 +96,7 @@ struct DevScalars {
   unsigned int ticket;              // last-block counter of the dt reduction
   int events;                       // captured runs: bit 0 = density passes ran out before the group stopped
   int n_big;                        // big particles met by the last list build
+  int n_app;                        // particles the last build's scatter pass appended entries to
   unsigned long long n_pairs;       // force-pass neighbour pairs (accumulating)
   unsigned long long n_candidates;  // force-pass distance tests (accumulating)
   int n_unconverged[256 + 8];       // per density pass

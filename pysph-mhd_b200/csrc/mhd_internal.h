@@ -114,6 +114,7 @@ struct Ctx {
   int* nbr_cnt = nullptr;
   int* nbr_gcnt = nullptr;  // entries of the gather pass (the rest were scattered)
   int* big_idx = nullptr;   // big particles of the last build (DevScalars::n_big of them)
+  int* app_idx = nullptr;   // particles given scattered entries by the last build (DevScalars::n_app)
   double* nbr_hlim = nullptr;
 
   // Lists persist across sorts in two slots, one per state buffer the caller

@@ -12,6 +12,8 @@
 // The fused force pass (groups G2-G10) is in mhd_force.cu.
 #include <cuda_runtime.h>
 
+#include <climits>
+
 #include "mhd_common.cuh"
 #include "mhd_internal.h"
 
@@ -296,8 +298,16 @@ __global__ void __launch_bounds__(128) k_density_pass_diag(int n, int pass, DevP
 // (each particle's own search), scatter (big particles add themselves where
 // a smaller search cannot reach them), ordering of the scattered entries.
 
-// Grid of the scatter pass (a grid-stride loop over the big particles).
-constexpr int kScatterBlocks = 148 * 4;
+// Grid of the big-particle passes (a grid-stride loop over the big
+// particles, one warp each): up to 16 blocks of 4 warps per multiprocessor,
+// enough for every big particle of a step to start at once (a big
+// particle's search is a chain of dependent row lookups, so these passes
+// are bound by latency, not by issue).
+static int big_blocks(const Ctx* c, int n) {
+  const int want = (n + 3) / 4;
+  const int cap = c->num_sms * 16;
+  return want < 1 ? 1 : (want < cap ? want : cap);
+}
 
 // FP32 squared distance from the packed positions, rounded op by op so that
 // it is the same whichever particle of the pair computes it.
@@ -430,7 +440,8 @@ __global__ void __launch_bounds__(128) k_scatter_big(DevParams P, const Grid* __
                                                      const int* __restrict__ cellc, float grow, int cap,
                                                      int* __restrict__ idx, int* __restrict__ cnt,
                                                      const int* __restrict__ big_idx, const int* __restrict__ mark,
-                                                     const int* __restrict__ gcnt, DevScalars* sc) {
+                                                     const int* __restrict__ gcnt, int* __restrict__ app_idx,
+                                                     DevScalars* sc) {
   // one warp per big particle: the lanes take consecutive candidates
   const int nb = sc->n_big, lane = threadIdx.x & 31;
   const float Rg = __fmul_rn((float)P.R, grow);
@@ -464,6 +475,8 @@ __global__ void __launch_bounds__(128) k_scatter_big(DevParams P, const Grid* __
           if (held) continue;
         }
         const int slot = atomicAdd(cnt + i, 1);
+        // the first entry appended to i's list enrols i for the ordering pass
+        if (slot == __ldg(gcnt + i)) app_idx[atomicAdd(&sc->n_app, 1)] = i;
         if (slot < cap) {
           irow[(size_t)slot * 32] = j;
         } else {
@@ -561,46 +574,48 @@ __global__ void __launch_bounds__(128) k_build_lists_big(DevParams P, const Grid
 
 // Order the scattered entries of every list by index (the scatter pass
 // appends them in whatever order its atomics resolve) and cap the counts.
-constexpr int kSortLocal = 48;  // appended entries sorted in a private copy
-
-__global__ void __launch_bounds__(128) k_sort_appended(int n, int cap, int* __restrict__ idx, int* __restrict__ cnt,
-                                                       const int* __restrict__ gcnt) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  int c = cnt[i];
-  if (c > cap) {
-    c = cap;
-    cnt[i] = cap;
-  }
-  const int g = gcnt[i];
-  const int m = c - g;
-  if (m < 2) return;
-  int* __restrict__ row = idx + (size_t)(i >> 5) * cap * 32 + (i & 31);
-  if (m <= kSortLocal) {
-    // sort a private copy (thread-local memory, L1-resident) instead of
-    // shifting the strided list entries in place
-    int v[kSortLocal];
-    for (int a = 0; a < m; a++) v[a] = row[(size_t)(g + a) * 32];
-    for (int a = 1; a < m; a++) {
-      const int t = v[a];
-      int b = a - 1;
-      while (b >= 0 && v[b] > t) {
-        v[b + 1] = v[b];
-        b--;
+// One warp per particle the scatter pass enrolled: up to 32 appended entries
+// are sorted across the lanes by a bitonic network (one entry per lane,
+// padded with INT_MAX); longer runs, rare, by one lane's insertion sort.
+__global__ void __launch_bounds__(128) k_sort_appended(int cap, int* __restrict__ idx, int* __restrict__ cnt,
+                                                       const int* __restrict__ gcnt,
+                                                       const int* __restrict__ app_idx,
+                                                       const DevScalars* __restrict__ sc) {
+  const int na = sc->n_app, lane = threadIdx.x & 31;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < na; t += nwarps) {
+    const int i = app_idx[t];
+    int c = cnt[i];
+    if (c > cap) c = cap;
+    __syncwarp();
+    if (lane == 0) cnt[i] = c;
+    const int g = gcnt[i];
+    const int m = c - g;
+    if (m < 2) continue;
+    int* __restrict__ row = idx + (size_t)(i >> 5) * cap * 32 + (i & 31);
+    if (m <= 32) {
+      int v = lane < m ? row[(size_t)(g + lane) * 32] : INT_MAX;
+#pragma unroll
+      for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+          const int o = __shfl_xor_sync(0xffffffffu, v, j);
+          const bool ascending = (lane & k) == 0, lower = (lane & j) == 0;
+          v = (lower == ascending) ? min(v, o) : max(v, o);
+        }
       }
-      v[b + 1] = t;
+      if (lane < m) row[(size_t)(g + lane) * 32] = v;
+    } else if (lane == 0) {
+      for (int a = g + 1; a < c; a++) {
+        const int v = row[(size_t)a * 32];
+        int b = a - 1;
+        while (b >= g && row[(size_t)b * 32] > v) {
+          row[(size_t)(b + 1) * 32] = row[(size_t)b * 32];
+          b--;
+        }
+        row[(size_t)(b + 1) * 32] = v;
+      }
     }
-    for (int a = 0; a < m; a++) row[(size_t)(g + a) * 32] = v[a];
-    return;
-  }
-  for (int a = g + 1; a < c; a++) {
-    const int v = row[a * 32];
-    int b = a - 1;
-    while (b >= g && row[b * 32] > v) {
-      row[(b + 1) * 32] = row[b * 32];
-      b--;
-    }
-    row[(b + 1) * 32] = v;
   }
 }
 
@@ -910,13 +925,13 @@ static void build_lists_dim(Ctx* c, const MhdState* s, int n, cudaStream_t st, c
   k_build_lists<DIM><<<nb, 128, 0, st>>>(n, c->P, c->d_grids, c->inst, c->cell_start, s->x, s->y, s->z, s->h,
                                          c->posf, c->cellc, grow, c->list_cap, S.idx, S.cnt, S.gcnt, c->nbr_hlim,
                                          c->big_idx, mark, c->d_sc);
-  k_build_lists_big<DIM><<<kScatterBlocks, 128, 0, st>>>(c->P, c->d_grids, c->inst, c->cell_start, s->x, s->y,
+  k_build_lists_big<DIM><<<big_blocks(c, n), 128, 0, st>>>(c->P, c->d_grids, c->inst, c->cell_start, s->x, s->y,
                                                          s->z, s->h, c->posf, c->cellc, grow, c->list_cap, S.idx,
                                                          S.cnt, S.gcnt, c->nbr_hlim, c->big_idx, c->d_sc);
-  k_scatter_big<DIM><<<kScatterBlocks, 128, 0, st>>>(c->P, c->d_grids, c->inst, c->cell_start, s->x, s->y, s->z,
+  k_scatter_big<DIM><<<big_blocks(c, n), 128, 0, st>>>(c->P, c->d_grids, c->inst, c->cell_start, s->x, s->y, s->z,
                                                      c->posf, c->cellc, grow, c->list_cap, S.idx, S.cnt,
-                                                     c->big_idx, mark, S.gcnt, c->d_sc);
-  k_sort_appended<<<nb, 128, 0, st>>>(n, c->list_cap, S.idx, S.cnt, S.gcnt);
+                                                     c->big_idx, mark, S.gcnt, c->app_idx, c->d_sc);
+  k_sort_appended<<<big_blocks(c, n), 128, 0, st>>>(c->list_cap, S.idx, S.cnt, S.gcnt, c->app_idx, c->d_sc);
   c->launches += 4;
 }
 
@@ -936,7 +951,7 @@ void launch_build_lists(Ctx* c, const MhdState* s, int n, cudaStream_t st, const
   c->nbr_idx = S.idx;
   c->nbr_cnt = S.cnt;
   c->nbr_gcnt = S.gcnt;
-  cudaMemsetAsync(&c->d_sc->n_big, 0, sizeof(int), st);
+  cudaMemsetAsync(&c->d_sc->n_big, 0, 2 * sizeof(int), st);  // n_big and n_app
   if (c->P.dim == 3)
     build_lists_dim<3>(c, s, n, st, carry ? &c->slots[od] : nullptr, S);
   else
