@@ -77,14 +77,14 @@ FORCE_FLOPS_PER_CANDIDATE = 12
 DENSITY_FLOPS_PER_PAIR = {"fp32": 33, "fp64": 25}
 
 
-def blast_case(n: int, precision: str = "fp64"):
+def blast_case(n: int, precision: str = "fp64", hot_radius: float = 0.1):
     dx = 1.0 / n
     ax = -0.5 + (np.arange(n) + 0.5) * dx
     x, y, z = np.meshgrid(ax, ax, ax, indexing="ij")
     x, y, z = x.ravel(), y.ravel(), z.ravel()
     cnt = x.size
     gamma = 5.0 / 3.0
-    p = np.where(x * x + y * y + z * z < 0.1 * 0.1, 10.0, 0.1)
+    p = np.where(x * x + y * y + z * z < hot_radius * hot_radius, 10.0, 0.1)
     b = 1.0 / math.sqrt(2.0)
     ic = dict(x=x, y=y, z=z, u=np.zeros(cnt), v=np.zeros(cnt), w=np.zeros(cnt), rho=np.ones(cnt),
               h=np.full(cnt, 1.2 * dx), m=np.full(cnt, dx ** 3), e=p / (gamma - 1.0), Bx=np.full(cnt, b),
@@ -390,6 +390,27 @@ def _batched(args, dev, rank=0, world=1):
         loop_ms += ev0.elapsed_time(ev1)
         eng.close()
     loop = total * k_loop / (loop_ms * 1e-3)
+    # the plain FP64 path at its fastest one instance at a time: each
+    # instance alone on the device planner, its `steps` steps captured once
+    # and timed as one graph launch (summed device time over the instances)
+    cap_ms, cap_launches = 0.0, 0
+    for a in inst:
+        eng = BatchEngine(params_from_dict(prm, "fp64"), [dict(a)])
+        eng.warmup()
+        eng.begin(eng.initial_dt())
+        snap = eng.snapshot()
+        eng.advance(steps, finish=True, snapshot=snap)  # capture + first run
+        eng.restore(snap)
+        torch.cuda.synchronize()
+        l0 = eng.launches()
+        ev0.record()
+        eng.advance(steps, finish=True, snapshot=snap)
+        ev1.record()
+        ev1.synchronize()
+        cap_ms += ev0.elapsed_time(ev1)
+        cap_launches += eng.launches() - l0
+        eng.close()
+    captured = total * steps / (cap_ms * 1e-3)
     # control: the FP64 batch again with every x moved by 1e-10 of its
     # instance's spacing -- the spread that rounding of any kind reaches on
     # these unjittered lattices (their Cullen-Dehnen limiter starts as
@@ -414,9 +435,16 @@ def _batched(args, dev, rank=0, world=1):
                         f"{int(sizes.min())}..{int(sizes.max())}), B0 x U[0.8, 1.2], quintic hfact 1.2, "
                         f"{total} particles, {steps} steps in one captured graph launch",
             "particles": total, "steps": steps, "fp32": out["fp32"], "fp64": out["fp64"],
-            "fp64_instance_loop": {"value": loop, "steps_per_instance": k_loop, "ms": loop_ms},
+            "fp64_instance_loop": {"value": loop, "steps_per_instance": k_loop, "ms": loop_ms,
+                                   "how": "each instance uncaptured through Engine.advance, host-checked density "
+                                          "iteration"},
+            "fp64_instance_captured": {"value": captured, "steps_per_instance": steps, "ms": cap_ms,
+                                       "gpu_launches": cap_launches, "graph_launches": len(inst),
+                                       "how": "each instance alone as one captured graph of all its steps"},
             "speedup_fp32_vs_fp64_loop": out["fp32"]["value"] / loop,
             "speedup_fp64_vs_fp64_loop": out["fp64"]["value"] / loop,
+            "speedup_fp32_vs_fp64_captured": out["fp32"]["value"] / captured,
+            "speedup_fp64_vs_fp64_captured": out["fp64"]["value"] / captured,
             "fp32_vs_fp64_rel_l2": {"rho": rel(["rho"]), "v": rel(["u", "v"]), "B": rel(["Bx", "By"])},
             "fp64_moved_1e-10dx_vs_fp64_rel_l2": {"rho": rel(["rho"], "fp64_moved"), "v": rel(["u", "v"], "fp64_moved"),
                                                   "B": rel(["Bx", "By"], "fp64_moved")}}
@@ -453,7 +481,11 @@ def _derivative(args, dev):
     amplitude 0.1, single density pass) after `steps` steps with respect to
     (amplitude, alpha_max), by the checkpointed adjoint and by forward mode,
     against central differences of the FP64 drop-in path with the same
-    (frozen) step sizes."""
+    (frozen) step sizes.  The adjoint is timed twice: the first call (CUDA
+    module loading, context set-up) and a second, steady-state one.  The
+    Alfven wave does not compress, so its alpha_max gradient is zero; a
+    second configuration -- a 3-D blast whose shock drives alpha_loc to the
+    clip -- checks a non-zero alpha_max gradient against differences."""
     import torch
 
     from src.config import load_config
@@ -464,38 +496,99 @@ def _derivative(args, dev):
 
     cfg = load_config(os.path.join(PKG, "configs", "alfven2d.toml"), {k: v.config_type for k, v in CASES.items()})
     steps, every = args.derivative_steps, 16
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    la, ga, dts = magnetic_energy_adjoint(cfg, 0.1, 1.0, steps, every=every)
-    torch.cuda.synchronize()
+    times = []
+    for _ in range(2):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        la, ga, dts = magnetic_energy_adjoint(cfg, 0.1, 1.0, steps, every=every)
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t0)
     t1 = time.perf_counter()
     lt, gt, _ = magnetic_energy_and_gradient(cfg, 0.1, 1.0, steps, dts=dts)
     torch.cuda.synchronize()
     t2 = time.perf_counter()
 
-    def loss(a, am):
-        ic, _, prm = alfven_case(cfg, a, am)
+    def energy(o):
+        return float(np.sum(o["m"] * (o["Bx"] ** 2 + o["By"] ** 2 + o["Bz"] ** 2) / (2.0 * o["rho"])))
+
+    def drop_in(ic, prm, step_sizes):
         eng = Engine(params_from_dict(dict(prm, density="single")), ParticleArray("fluid", dict(ic), device=dev))
         eng.warmup()
-        for dt in dts:
+        for dt in step_sizes:
             eng.step(dt)
         o = eng.pa.pull("Bx", "By", "Bz", "m", "rho")
         eng.close()
-        return float(np.sum(o["m"] * (o["Bx"] ** 2 + o["By"] ** 2 + o["Bz"] ** 2) / (2.0 * o["rho"])))
+        return energy(o)
+
+    def loss(a, am):
+        ic, _, prm = alfven_case(cfg, a, am)
+        return drop_in(ic, prm, dts)
 
     ea = 1e-4 * 0.1
     fd_a = (loss(0.1 + ea, 1.0) - loss(0.1 - ea, 1.0)) / (2.0 * ea)
     fd_m = (loss(0.1, 1.1) - loss(0.1, 0.9)) / 0.2
-    return {"workload": f"2-D circularly polarised Alfven wave, 64 x 128 lattice, periodic box 1 x 2, rho 1, p 0.1, "
-                        f"B_par 1, amplitude 0.1, Wendland C6 hfact 1.9, artificial viscosity 1, single density "
-                        f"pass; final magnetic energy after {steps} steps (frozen step sizes)",
-            "loss": la, "grad_adjoint": {"amplitude": float(ga[0]), "alpha_max": float(ga[1])},
-            "grad_forward_mode": {"amplitude": float(gt[0]), "alpha_max": float(gt[1])},
-            "central_differences": {"amplitude": fd_a, "alpha_max": fd_m, "step_amplitude": ea, "step_alpha_max": 0.1},
-            "rel_err_adjoint_vs_fd_amplitude": abs(ga[0] - fd_a) / abs(fd_a),
-            "checkpoint_every": every, "adjoint_s": t1 - t0, "forward_mode_s": t2 - t1,
-            "note": "alpha_loc stays ~1e-9 in this linear wave, so the alpha_max clip is inactive and "
-                    "dL/dalpha_max = 0 exactly (also by differences)"}
+    out = {"workload": f"2-D circularly polarised Alfven wave, 64 x 128 lattice, periodic box 1 x 2, rho 1, p 0.1, "
+                       f"B_par 1, amplitude 0.1, Wendland C6 hfact 1.9, artificial viscosity 1, single density "
+                       f"pass; final magnetic energy after {steps} steps (frozen step sizes)",
+           "loss": la, "grad_adjoint": {"amplitude": float(ga[0]), "alpha_max": float(ga[1])},
+           "grad_forward_mode": {"amplitude": float(gt[0]), "alpha_max": float(gt[1])},
+           "central_differences": {"amplitude": fd_a, "alpha_max": fd_m, "step_amplitude": ea, "step_alpha_max": 0.1},
+           "rel_err_adjoint_vs_fd_amplitude": abs(ga[0] - fd_a) / abs(fd_a),
+           "checkpoint_every": every, "adjoint_s": times[1], "adjoint_first_call_s": times[0],
+           "forward_mode_s": t2 - t1,
+           "note": "alpha_loc stays ~1e-9 in this linear wave, so the alpha_max clip is inactive and "
+                   "dL/dalpha_max = 0 exactly (also by differences); alpha_max_active checks a non-zero one"}
+    out["alpha_max_active"] = _derivative_alpha_active(args, dev, drop_in)
+    return out
+
+
+def _derivative_alpha_active(args, dev, drop_in, n=16, steps=40, every=8, alpha_max=0.6):
+    """Adjoint gradient of the final magnetic energy of a small 3-D blast
+    (n^3 lattice, p = 10 inside r < 0.25, alpha in [0.1, alpha_max]) with
+    respect to (s, alpha_max), e -> e (1 + 0.01 s), against central
+    differences of the drop-in path: the shock drives alpha_loc to the clip,
+    so dL/dalpha_max is not zero."""
+    import torch
+
+    from src.derivative import AdjointEngine, TangentEngine, TangentState
+    from src.engine import params_from_dict
+
+    ic, prm = blast_case(n, "fp64", hot_radius=0.25)
+    prm = dict(prm, alpha_max=alpha_max, density="single")
+    params = params_from_dict(prm)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    te = TangentEngine(params, TangentState(dict(ic), {"e": [0.01 * ic["e"], None]}), alpha_max_seed=[0.0, 1.0])
+    te.warmup()
+    ae = AdjointEngine(params, te.ts.n)
+    values = {f: te.ts[f][:, 0].contiguous() for f in ae.fields}
+    values["m"] = te.ts["m"][:, 0].contiguous()
+    values["itype"] = te.ts["itype"]
+    tan0 = torch.stack([te.ts[f][:, 1:].clone() for f in ae.fields])
+    la, used, cps = ae.forward(values, steps, [te.initial_dt()] + [-1.0] * (steps - 1), every)
+    lam, dam = ae.backward(values, steps, used, every, cps)
+    ga = torch.einsum("fn,fnd->d", lam, tan0).cpu().numpy()
+    ga[1] += dam
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    te.run(steps, used)
+    clipped = int((te.ts.value("alphaloc") == alpha_max).sum())
+    ae.close()
+    te.close()
+
+    def loss(scale_e, am):
+        return drop_in(dict(ic, e=ic["e"] * (1.0 + 0.01 * scale_e)), dict(prm, alpha_max=am), used)
+
+    h = 1e-6
+    fd_e = (loss(h, alpha_max) - loss(-h, alpha_max)) / (2 * h)
+    fd_m = (loss(0.0, alpha_max + h) - loss(0.0, alpha_max - h)) / (2 * h)
+    return {"workload": f"3-D blast {n}^3 = {n ** 3} particles, p 10 inside r < 0.25 (0.1 outside), cubic hfact "
+                        f"1.2, alpha in [0.1, {alpha_max}], single density pass; final magnetic energy after "
+                        f"{steps} steps (frozen step sizes), parameters (s: e -> e (1 + 0.01 s), alpha_max)",
+            "loss": la, "grad_adjoint": {"s": float(ga[0]), "alpha_max": float(ga[1])},
+            "central_differences": {"s": fd_e, "alpha_max": fd_m, "step": h},
+            "rel_err_adjoint_vs_fd": {"s": abs(ga[0] - fd_e) / abs(fd_e), "alpha_max": abs(ga[1] - fd_m) / abs(fd_m)},
+            "alphaloc_at_clip_final": clipped, "checkpoint_every": every, "adjoint_s": t1 - t0}
 
 
 def _app_case(name, nx=None, precision=None):
