@@ -683,6 +683,7 @@ int mhd_ctx_create(const MhdParams* params, int64_t n_max, void** out) {
   if (const char* m = getenv("MHD_LIST_MARGIN")) c->list_margin = std::max(0.005, std::min(0.5, atof(m)));
   if (const char* m = getenv("MHD_LIST_REUSE")) c->list_reuse = atoi(m) != 0;
   if (const char* m = getenv("MHD_FORCE_STAGED")) c->force_staged = atoi(m) != 0;
+  if (const char* m = getenv("MHD_FORCE_TILES")) c->force_tiles = atoi(m) != 0;
   *out = c;
   return MHD_OK;
 }

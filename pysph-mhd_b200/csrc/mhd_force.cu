@@ -265,96 +265,57 @@ __device__ __forceinline__ void cd_post(const CdMoments<DIM, T>& M, int i, const
 constexpr int kForceShapes[][2] = {{128, 2}, {128, 3}, {128, 4}, {256, 2}};
 constexpr int kForceShapeCount = 4;
 
-// STAGED: each thread copies its next neighbour's record into its own slot
-// of a two-stage shared-memory buffer (cp.async) while it computes the
-// current pair, so a pair no longer waits on a gather from L1/L2.
-template <int K, int DIM, class T, int SHAPE, bool STAGED>
-__global__ void __launch_bounds__(kForceShapes[SHAPE][0], kForceShapes[SHAPE][1])
-    k_force_pass(int n, DevParams P, NbrList L, const Grid* __restrict__ grids, const int* __restrict__ inst,
-                 const ForceRec<T> rec, ForceOut<T> o) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const Grid& G = grid_of(grids, inst, i);
-  const V4<T> pi = rec.q[0][i], i1 = rec.q[1][i], i2 = rec.q[2][i], i3 = rec.q[3][i], i4 = rec.q[4][i],
-              i5 = rec.q[5][i], i6 = rec.q[6][i];
-  const T h1i = i4.w;
-  const T norm = prm_t<T>(P.normf, P.norm);
-  // grad W(h_i) = faci1 dw(q) / r * x_ij
-  const T faci1 = norm * (DIM == 2 ? h1i * h1i * h1i : (h1i * h1i) * (h1i * h1i));
-  const T rhoi = i1.y, irhoi = i1.z, omegai = i1.w;
-  const T ptoti = i2.x, AI = i2.y, vwi = i2.z, irho2i = i2.w;
-  const T ui = i3.x, vi = i3.y, wi = i3.z, epi = i3.w;
-  const T aui = i4.x, avi = i4.y, awi = i4.z;
-  const T bxi = i5.x, byi = i5.y, bzi = i5.z, p_i = i5.w;
-  const T bsxi = i6.x, bsyi = i6.y, bszi = i6.z, psii = i6.w;
-  const T pr2i = p_i * irho2i;
-  const T av = prm_t<T>(P.avf, P.av), ac = prm_t<T>(P.acf, P.ac), ar = prm_t<T>(P.arf, P.ar),
-          inv_mu0 = prm_t<T>(P.inv_mu0f, P.inv_mu0);
-  const T two = (T)2, half = (T)0.5, zero = (T)0;
-  // neighbour test r^2 < (R max(h_i, h_j))^2: FP32 on the FP32 form, the
-  // exact FP64 rule of the oracle on the FP64 form
-  const float Rf = P.Rf;
-  const float rhi2f = (Rf * (float)pi.w) * (Rf * (float)pi.w);
-  const double rhi2 = rh2_exact(P.R, (double)pi.w);
-
+// One particle i of the force pass: its record values, the pair sums and
+// the pair terms (CullenDehnenAlphaDiagnostics, MHDAccelerations,
+// MagneticStressAccelerations, MagneticStateRates loops) with neighbour
+// records j, and the FP64 epilogue.  Shared by the list-driven pass and the
+// cell-tile pass, which differ only in how they walk the neighbours.
+template <int K, int DIM, class T>
+struct ForceParticle {
+  V4<T> pi;
+  T h1i, norm, faci1, rhoi, irhoi, omegai, ptoti, AI, vwi, irho2i, ui, vi, wi, epi, aui, avi, awi, bxi, byi, bzi,
+      p_i, bsxi, bsyi, bszi, psii, pr2i, av, ac, ar, inv_mu0;
+  float Rf, rhi2f;
+  double rhi2;
   CdMoments<DIM, T> M;
   Acc<T> fx, fy, fz, fe, fdiv, bxr, byr, bzr, dbs, dbd;
-  T dtc = 0;
+  T dtc;
 
-  const int cnt = L.cnt[i];
-  const int* __restrict__ row = L.idx + (size_t)(i >> 5) * L.cap * 32 + (i & 31);
-  // Staged: slot [stage][plane][thread] of the dynamic shared buffer; the
-  // list entries run two pairs ahead of the computed pair, its record one.
-  // Register gather: the list entry is fetched one pair ahead and every
-  // record of a pair is requested before its neighbour test, so a pair waits
-  // on one memory round trip instead of three (entry, position, records).
-  constexpr int NT = kForceShapes[SHAPE][0];
-  extern __shared__ __align__(16) unsigned char force_smem[];
-  V4<T>* __restrict__ sb = reinterpret_cast<V4<T>*>(force_smem) + threadIdx.x;
-  auto fetch = [&](int stage, int jj) {
-#pragma unroll
-    for (int p = 0; p < kForcePlanes; p++) {
-      V4<T>* dst = sb + (stage * kForcePlanes + p) * NT;
-      const V4<T>* src = rec.q[p] + jj;
-#pragma unroll
-      for (int b = 0; b < (int)(sizeof(V4<T>) / 16); b++)
-        cp_async16(reinterpret_cast<char*>(dst) + 16 * b, reinterpret_cast<const char*>(src) + 16 * b);
-    }
-    cp_async_commit();
-  };
-  int jn = cnt > 0 ? row[0] : i;
-  int jn2 = i;
-  if constexpr (STAGED) {
-    fetch(0, jn);
-    jn2 = cnt > 1 ? row[32] : i;
+  __device__ __forceinline__ void init(int i, const DevParams& P, const ForceRec<T>& rec) {
+    pi = rec.q[0][i];
+    const V4<T> i1 = rec.q[1][i], i2 = rec.q[2][i], i3 = rec.q[3][i], i4 = rec.q[4][i], i5 = rec.q[5][i],
+                i6 = rec.q[6][i];
+    h1i = i4.w;
+    norm = prm_t<T>(P.normf, P.norm);
+    // grad W(h_i) = faci1 dw(q) / r * x_ij
+    faci1 = norm * (DIM == 2 ? h1i * h1i * h1i : (h1i * h1i) * (h1i * h1i));
+    rhoi = i1.y; irhoi = i1.z; omegai = i1.w;
+    ptoti = i2.x; AI = i2.y; vwi = i2.z; irho2i = i2.w;
+    ui = i3.x; vi = i3.y; wi = i3.z; epi = i3.w;
+    aui = i4.x; avi = i4.y; awi = i4.z;
+    bxi = i5.x; byi = i5.y; bzi = i5.z; p_i = i5.w;
+    bsxi = i6.x; bsyi = i6.y; bszi = i6.z; psii = i6.w;
+    pr2i = p_i * irho2i;
+    av = prm_t<T>(P.avf, P.av); ac = prm_t<T>(P.acf, P.ac); ar = prm_t<T>(P.arf, P.ar);
+    inv_mu0 = prm_t<T>(P.inv_mu0f, P.inv_mu0);
+    // neighbour test r^2 < (R max(h_i, h_j))^2: FP32 on the FP32 form, the
+    // exact FP64 rule of the oracle on the FP64 form
+    Rf = P.Rf;
+    rhi2f = (Rf * (float)pi.w) * (Rf * (float)pi.w);
+    rhi2 = rh2_exact(P.R, (double)pi.w);
+    dtc = 0;
   }
-  for (int k = 0; k < cnt; k++) {
-    const int j = jn;
-    V4<T> pj, j1, j2, j3, j4, j5, j6;
-    if constexpr (STAGED) {
-      jn = jn2;
-      if (k + 1 < cnt) fetch((k + 1) & 1, jn);
-      else cp_async_commit();  // an empty group keeps the wait below uniform
-      if (k + 2 < cnt) jn2 = row[(k + 2) * 32];
-      cp_async_wait_all_but_one();
-      if (j == i) {
-        dtc = fmax(dtc, vwi);  // the self pair, as below
-        continue;
-      }
-      const V4<T>* st = sb + ((k & 1) * kForcePlanes) * NT;
-      pj = st[0]; j1 = st[NT]; j2 = st[2 * NT]; j3 = st[3 * NT]; j4 = st[4 * NT]; j5 = st[5 * NT]; j6 = st[6 * NT];
-    } else {
-      if (k + 1 < cnt) jn = row[(k + 1) * 32];
-      if (j == i) {
-        // the self pair: every sum term carries a zero kernel gradient or a
-        // zero displacement; only the signal speed max(vw_i - 2 dot, 0) = vw_i
-        // enters dt_cfl
-        dtc = fmax(dtc, vwi);
-        continue;
-      }
-      pj = ld4(rec.q[0] + j); j1 = ld4(rec.q[1] + j); j2 = ld4(rec.q[2] + j); j3 = ld4(rec.q[3] + j);
-      j4 = ld4(rec.q[4] + j); j5 = ld4(rec.q[5] + j); j6 = ld4(rec.q[6] + j);
-    }
+
+  // the self pair: every sum term carries a zero kernel gradient or a zero
+  // displacement; only the signal speed max(vw_i - 2 dot, 0) = vw_i enters
+  // dt_cfl
+  __device__ __forceinline__ void self_pair() { dtc = fmax(dtc, vwi); }
+
+  // A candidate j: the neighbour test, then the pair terms.
+  __device__ __forceinline__ void pair(const Grid& G, const DevParams& P, const V4<T>& pj, const V4<T>& j1,
+                                       const V4<T>& j2, const V4<T>& j3, const V4<T>& j4, const V4<T>& j5,
+                                       const V4<T>& j6) {
+    const T two = (T)2, half = (T)0.5, zero = (T)0;
     T dx, dy, dz, r, inv_r;
     if constexpr (sizeof(T) == 4) {
       // FP32 geometry: one wrapped fixed-point difference per axis
@@ -363,7 +324,7 @@ __global__ void __launch_bounds__(kForceShapes[SHAPE][0], kForceShapes[SHAPE][1]
       dz = DIM == 3 ? fixed_delta(G, 2, __float_as_uint(pi.z), __float_as_uint(pj.z)) : 0.f;
       const float r2 = dx * dx + dy * dy + dz * dz;
       const float rhj = Rf * pj.w;
-      if (!(r2 < fmaxf(rhi2f, rhj * rhj))) continue;
+      if (!(r2 < fmaxf(rhi2f, rhj * rhj))) return;
       inv_r = r2 > 0.f ? rsqrtf(r2) : 0.f;
       r = r2 * inv_r;
     } else {
@@ -372,7 +333,7 @@ __global__ void __launch_bounds__(kForceShapes[SHAPE][0], kForceShapes[SHAPE][1]
       const double dyd = min_image((double)pi.y - pj.y, G.L[1], G.half[1], G.periodic[1]);
       const double dzd = DIM == 3 ? min_image((double)pi.z - pj.z, G.L[2], G.half[2], G.periodic[2]) : 0.0;
       const double r2d = r2_exact(dxd, dyd, dzd);
-      if (!(r2d < rhi2 || r2d < rh2_exact(P.R, pj.w))) continue;
+      if (!(r2d < rhi2 || r2d < rh2_exact(P.R, pj.w))) return;
       dx = dxd;
       dy = dyd;
       dz = dzd;
@@ -445,64 +406,231 @@ __global__ void __launch_bounds__(kForceShapes[SHAPE][0], kForceShapes[SHAPE][1]
     dbd.add(-mo * (xbi - xbj));
   }
 
-  // ---- per-particle epilogue in FP64
-  const double rhoi_d = o.rho[i], irho_d = 1.0 / rhoi_d;
-  const double hid = o.h[i], csi = o.cs[i];
-  cd_post<DIM, T>(M, i, P, o);
-  // MHDAccelerations.post_loop, SmoothingLengthRateFromForceDivergence
-  const double divi = -fdiv.get() * irho_d;
-  // MagneticStateRates.post_loop (src/equations.py:562-567)
-  const double vwid = sqrt(csi * csi + ((double)bxi * bxi + (double)byi * byi + (double)bzi * bzi) * P.inv_mu0 * irho_d);
-  const double chi = P.clean_speed * vwid;
-  const double psipi = o.psipred[i];
-  const double dbdv = dbd.get(), dbsv = dbs.get();
-  const double apsi = -chi * dbdv * irho_d - P.clean_damp * psipi * chi / hid - 0.5 * P.clean_active * psipi * divi;
-  double dtcd = dtc;
-  dtcd = fmax(dtcd, vwid);
-  dtcd = fmax(dtcd, chi);
-  // EnergyLimiter (src/equations.py:594-598)
-  double fed = fe.get();
-  const double epid = o.epred[i];
-  if (dtcd > 0.0) {
-    const double dtcour = P.c_cour * hid / dtcd;
-    if (epid + dtcour * fed < 0.0 && epid > 0.0) fed /= 1.0 - dtcour * fed / epid;
-  }
-  // DivBCorrection (src/equations.py:607-624)
-  double ax = fx.get(), ay = fy.get(), az = fz.get();
-  {
-    const double bxd = bxi, byd = byi, bzd = bzi;
-    const double b2 = bxd * bxd + byd * byd + bzd * bzd;
-    double frac = 0.0;
-    if (b2 > 0.0) {
-      const double betap = 2.0 * P.mu0 * o.p[i] / b2;
-      frac = fmax(0.0, fmin(1.0, (10.0 - betap) * 0.125));
+  // Post-loops in FP64: CullenDehnenAlphaDiagnostics (+ StrainDiagnostics),
+  // MHDAccelerations, SmoothingLengthRateFromForceDivergence,
+  // MagneticStateRates, EnergyLimiter, DivBCorrection, AdaptiveTimestep.
+  __device__ __forceinline__ void finish(int i, const DevParams& P, const ForceOut<T>& o) const {
+    const double rhoi_d = o.rho[i], irho_d = 1.0 / rhoi_d;
+    const double hid = o.h[i], csi = o.cs[i];
+    cd_post<DIM, T>(M, i, P, o);
+    // MHDAccelerations.post_loop, SmoothingLengthRateFromForceDivergence
+    const double divi = -fdiv.get() * irho_d;
+    // MagneticStateRates.post_loop (src/equations.py:562-567)
+    const double vwid =
+        sqrt(csi * csi + ((double)bxi * bxi + (double)byi * byi + (double)bzi * bzi) * P.inv_mu0 * irho_d);
+    const double chi = P.clean_speed * vwid;
+    const double psipi = o.psipred[i];
+    const double dbdv = dbd.get(), dbsv = dbs.get();
+    const double apsi = -chi * dbdv * irho_d - P.clean_damp * psipi * chi / hid - 0.5 * P.clean_active * psipi * divi;
+    double dtcd = dtc;
+    dtcd = fmax(dtcd, vwid);
+    dtcd = fmax(dtcd, chi);
+    // EnergyLimiter (src/equations.py:594-598)
+    double fed = fe.get();
+    const double epid = o.epred[i];
+    if (dtcd > 0.0) {
+      const double dtcour = P.c_cour * hid / dtcd;
+      if (epid + dtcour * fed < 0.0 && epid > 0.0) fed /= 1.0 - dtcour * fed / epid;
     }
-    const double cf = dbsv * frac * P.inv_mu0;
-    ax -= bxd * cf;
-    ay -= byd * cf;
-    az -= bzd * cf;
-  }
-  // AdaptiveTimestep (src/equations.py:578-585)
-  double dta = kBigNumber;
-  if (dtcd > 0.0) dta = P.c_cour * hid / dtcd;
-  const double f2 = ax * ax + ay * ay + az * az;
-  if (f2 > 0.0) dta = fmin(dta, P.c_force * sqrt(hid / sqrt(f2)));
+    // DivBCorrection (src/equations.py:607-624)
+    double ax = fx.get(), ay = fy.get(), az = fz.get();
+    {
+      const double bxd = bxi, byd = byi, bzd = bzi;
+      const double b2 = bxd * bxd + byd * byd + bzd * bzd;
+      double frac = 0.0;
+      if (b2 > 0.0) {
+        const double betap = 2.0 * P.mu0 * o.p[i] / b2;
+        frac = fmax(0.0, fmin(1.0, (10.0 - betap) * 0.125));
+      }
+      const double cf = dbsv * frac * P.inv_mu0;
+      ax -= bxd * cf;
+      ay -= byd * cf;
+      az -= bzd * cf;
+    }
+    // AdaptiveTimestep (src/equations.py:578-585)
+    double dta = kBigNumber;
+    if (dtcd > 0.0) dta = P.c_cour * hid / dtcd;
+    const double f2 = ax * ax + ay * ay + az * az;
+    if (f2 > 0.0) dta = fmin(dta, P.c_force * sqrt(hid / sqrt(f2)));
 
-  o.au[i] = ax;
-  o.av[i] = ay;
-  o.aw[i] = az;
-  o.ae[i] = fed;
-  o.ah[i] = hid * divi * (1.0 / (double)DIM);
-  o.div[i] = divi;
-  o.div_for_psi[i] = divi;
-  o.dt_cfl[i] = dtcd;
-  o.dt_adapt[i] = dta;
-  o.aBx[i] = bxr.get();
-  o.aBy[i] = byr.get();
-  o.aBz[i] = bzr.get();
-  o.apsi[i] = apsi;
-  o.divBsymm[i] = rhoi_d * dbsv;
-  o.divBdiff[i] = dbdv;
+    o.au[i] = ax;
+    o.av[i] = ay;
+    o.aw[i] = az;
+    o.ae[i] = fed;
+    o.ah[i] = hid * divi * (1.0 / (double)DIM);
+    o.div[i] = divi;
+    o.div_for_psi[i] = divi;
+    o.dt_cfl[i] = dtcd;
+    o.dt_adapt[i] = dta;
+    o.aBx[i] = bxr.get();
+    o.aBy[i] = byr.get();
+    o.aBz[i] = bzr.get();
+    o.apsi[i] = apsi;
+    o.divBsymm[i] = rhoi_d * dbsv;
+    o.divBdiff[i] = dbdv;
+  }
+};
+
+// List-driven pass: one thread per particle walks its compacted neighbour
+// list.  STAGED: each thread copies its next neighbour's record into its own
+// slot of a two-stage shared-memory buffer (cp.async) while it computes the
+// current pair, so a pair no longer waits on a gather from L1/L2.
+template <int K, int DIM, class T, int SHAPE, bool STAGED>
+__global__ void __launch_bounds__(kForceShapes[SHAPE][0], kForceShapes[SHAPE][1])
+    k_force_pass(int n, DevParams P, NbrList L, const Grid* __restrict__ grids, const int* __restrict__ inst,
+                 const ForceRec<T> rec, ForceOut<T> o) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const Grid& G = grid_of(grids, inst, i);
+  ForceParticle<K, DIM, T> F;
+  F.init(i, P, rec);
+
+  const int cnt = L.cnt[i];
+  const int* __restrict__ row = L.idx + (size_t)(i >> 5) * L.cap * 32 + (i & 31);
+  // Staged: slot [stage][plane][thread] of the dynamic shared buffer; the
+  // list entries run two pairs ahead of the computed pair, its record one.
+  // Register gather: the list entry is fetched one pair ahead and every
+  // record of a pair is requested before its neighbour test, so a pair waits
+  // on one memory round trip instead of three (entry, position, records).
+  constexpr int NT = kForceShapes[SHAPE][0];
+  extern __shared__ __align__(16) unsigned char force_smem[];
+  V4<T>* __restrict__ sb = reinterpret_cast<V4<T>*>(force_smem) + threadIdx.x;
+  auto fetch = [&](int stage, int jj) {
+#pragma unroll
+    for (int p = 0; p < kForcePlanes; p++) {
+      V4<T>* dst = sb + (stage * kForcePlanes + p) * NT;
+      const V4<T>* src = rec.q[p] + jj;
+#pragma unroll
+      for (int b = 0; b < (int)(sizeof(V4<T>) / 16); b++)
+        cp_async16(reinterpret_cast<char*>(dst) + 16 * b, reinterpret_cast<const char*>(src) + 16 * b);
+    }
+    cp_async_commit();
+  };
+  int jn = cnt > 0 ? row[0] : i;
+  int jn2 = i;
+  if constexpr (STAGED) {
+    fetch(0, jn);
+    jn2 = cnt > 1 ? row[32] : i;
+  }
+  for (int k = 0; k < cnt; k++) {
+    const int j = jn;
+    if constexpr (STAGED) {
+      jn = jn2;
+      if (k + 1 < cnt) fetch((k + 1) & 1, jn);
+      else cp_async_commit();  // an empty group keeps the wait below uniform
+      if (k + 2 < cnt) jn2 = row[(k + 2) * 32];
+      cp_async_wait_all_but_one();
+      if (j == i) {
+        F.self_pair();
+        continue;
+      }
+      const V4<T>* st = sb + ((k & 1) * kForcePlanes) * NT;
+      F.pair(G, P, st[0], st[NT], st[2 * NT], st[3 * NT], st[4 * NT], st[5 * NT], st[6 * NT]);
+    } else {
+      if (k + 1 < cnt) jn = row[(k + 1) * 32];
+      if (j == i) {
+        F.self_pair();
+        continue;
+      }
+      F.pair(G, P, ld4(rec.q[0] + j), ld4(rec.q[1] + j), ld4(rec.q[2] + j), ld4(rec.q[3] + j), ld4(rec.q[4] + j),
+             ld4(rec.q[5] + j), ld4(rec.q[6] + j));
+    }
+  }
+  F.finish(i, P, o);
+}
+
+// Cell-tile pass (FP32 form, an alternative kept for comparison): no
+// neighbour list.  Each warp takes 32 consecutive particles of the sorted
+// order, walks the union of their search stencils row by row (one
+// contiguous index range per row piece, as the list build does), stages 32
+// candidate records at a time in shared memory with coalesced 16-byte loads
+// (each record read from memory once per warp), and every lane tests every
+// staged candidate against its own particle and adds the pair terms of its
+// neighbours.  A big particle (h beyond what the grid's stencil covers) can
+// reach a particle from beyond that union; its pairs are then missed, so
+// this pass is exact only while no particle is big.
+constexpr int kTileThreads = 128;
+template <int K, int DIM>
+__global__ void __launch_bounds__(kTileThreads, 3)
+    k_force_tiles(int n, DevParams P, const Grid* __restrict__ grids, const int* __restrict__ inst,
+                  const int* __restrict__ cell_start, const int* __restrict__ cellc, const ForceRec<float> rec,
+                  ForceOut<float> o) {
+  using T = float;
+  __shared__ V4<T> tile[kTileThreads / 32][kForcePlanes][32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int i0 = (blockIdx.x * kTileThreads + threadIdx.x) & ~31;
+  if (i0 >= n) return;
+  const int i = i0 + lane;
+  const bool live = i < n;
+  const int ii = live ? i : i0;
+  const Grid& G = grid_of(grids, inst, ii);
+  ForceParticle<K, DIM, T> F;
+  F.init(ii, P, rec);
+  // the warp's cell extents (the warp's particles share one instance: a
+  // warp that straddles two instances takes the first one's grid, and the
+  // second instance's particles are taken whole by their own warps)
+  int cx, cy, cz;
+  unpack_cell<DIM>(cellc[ii], cx, cy, cz);
+  int lo[3] = {cx, cy, cz}, hi[3] = {cx, cy, cz};
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      lo[a] = min(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], off));
+      hi[a] = max(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], off));
+    }
+  const int sw = G.sw;
+  const int nc[3] = {G.nc[0], G.nc[1], DIM == 3 ? G.nc[2] : 1};
+  int a_lo[3], a_hi[3];
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const bool whole = a >= DIM || nc[a] < 2 * sw + 1 + (hi[a] - lo[a]);
+    a_lo[a] = whole ? 0 : lo[a] - sw;
+    a_hi[a] = whole ? nc[a] - 1 : hi[a] + sw;
+  }
+  V4<T>(*buf)[32] = tile[warp];
+  for (int zu = a_lo[2]; zu <= a_hi[2]; zu++) {
+    const int zc = zu < 0 ? zu + nc[2] : (zu >= nc[2] ? zu - nc[2] : zu);
+    if (!G.periodic[2] && zc != zu) continue;
+    for (int yu = a_lo[1]; yu <= a_hi[1]; yu++) {
+      const int yc = yu < 0 ? yu + nc[1] : (yu >= nc[1] ? yu - nc[1] : yu);
+      if (!G.periodic[1] && yc != yu) continue;
+      const int base = G.cell_base + (zc * nc[1] + yc) * nc[0];
+      // x pieces: below 0, inside, above nx - 1 (periodic wrap)
+      for (int piece = 0; piece < 3; piece++) {
+        int xl, xh;
+        if (piece == 0) { xl = a_lo[0]; xh = min(a_hi[0], -1); }
+        else if (piece == 1) { xl = max(a_lo[0], 0); xh = min(a_hi[0], nc[0] - 1); }
+        else { xl = max(a_lo[0], nc[0]); xh = a_hi[0]; }
+        if (xl > xh) continue;
+        if (piece != 1) {
+          if (!G.periodic[0]) continue;
+          const int s = piece == 0 ? nc[0] : -nc[0];
+          xl += s;
+          xh += s;
+        }
+        const int jb = cell_start[base + xl], je = cell_start[base + xh + 1];
+        for (int t0 = jb; t0 < je; t0 += 32) {
+          const int m = min(32, je - t0);
+          __syncwarp();
+          if (lane < m) {
+#pragma unroll
+            for (int p = 0; p < kForcePlanes; p++) buf[p][lane] = ld4(rec.q[p] + t0 + lane);
+          }
+          __syncwarp();
+          for (int c = 0; c < m; c++) {
+            const int j = t0 + c;
+            if (j == ii) {
+              F.self_pair();
+              continue;
+            }
+            F.pair(G, P, buf[0][c], buf[1][c], buf[2][c], buf[3][c], buf[4][c], buf[5][c], buf[6][c]);
+          }
+        }
+      }
+    }
+  }
+  if (live) F.finish(i, P, o);
 }
 
 // 2-D complement of the Cullen-Dehnen moments.  In a 2-D layout the force
@@ -627,6 +755,11 @@ static void force_launch_shape(Ctx* c, const ForceOut<T>& o, int n, cudaStream_t
 template <int K, int DIM, class T>
 static void force_launch_t(Ctx* c, const ForceOut<T>& o, int n, cudaStream_t st) {
   if constexpr (sizeof(T) == 4) {
+    if (c->force_tiles) {
+      k_force_tiles<K, DIM><<<(n + kTileThreads - 1) / kTileThreads, kTileThreads, 0, st>>>(
+          n, c->P, c->d_grids, c->inst, c->cell_start, c->cellc, records<T>(c), o);
+      return;
+    }
     if (c->force_staged) {
       force_launch_shape<K, DIM, T, true>(c, o, n, st);
       return;

@@ -100,6 +100,7 @@ struct Ctx {
   int stencil = 2;       // cells are >= list cut-off / stencil wide
   int force_shape = -1;  // launch-shape variant of the force pass (kForceShapes); -1 = per-precision default
   bool force_staged = true;  // force-pass records staged in shared memory (MHD_FORCE_STAGED=0: register gather)
+  bool force_tiles = false;  // FP32 force pass by cell tiles instead of lists (MHD_FORCE_TILES=1; no big particles)
   double list_cut = 0;   // R * h_max * (1 + list_margin) of the current grid
 
   // compacted neighbour lists (NbrList layout), built with every grid.  The

@@ -47,3 +47,27 @@ def test_fp32_form_close_to_fp64(name, steps):
     for k in ("rho", "u", "v", "Bx", "By"):
         assert errs[k] < 1e-5, f"{name} FP32 vs FP64 rel L2 {k} = {errs[k]:.2e} ({errs})"
     assert max(errs.values()) < 1e-4, errs
+
+
+@pytest.mark.parametrize("name", ["blast3d", "ot2d"])
+def test_cell_tile_force_pass_equals_list_pass(name, monkeypatch):
+    # The cell-tile force pass (MHD_FORCE_TILES=1, kept for comparison with
+    # the list-driven pass) visits the same pairs -- no particle is big in
+    # these warm-ups, whose h stays uniform -- in another order: FP32 sums
+    # agree to a few rounding errors of the pair terms.
+    from src.engine import Engine, params_from_dict
+    from src.particle_array import ParticleArray
+
+    ic, prm = {"blast3d": lambda: sc_.blast_3d(16, "cubic"), "ot2d": lambda: sc_.orszag_tang_2d(40, "quintic")}[name]()
+    names = ("au", "av", "ae", "aBevolx", "aBevoly", "apsi", "dt_adapt", "alphaloc", "divBsymm")
+    out = {}
+    for mode in ("0", "1"):
+        monkeypatch.setenv("MHD_FORCE_TILES", mode)
+        eng = Engine(params_from_dict(prm, "fp32"), ParticleArray("fluid", ic))
+        eng.warmup()
+        out[mode] = eng.pa.pull(*names, order="gid")
+        eng.close()
+    for k in names:
+        ref = out["0"][k]
+        err = float(np.max(np.abs(out["1"][k] - ref))) / max(float(np.max(np.abs(ref))), 1e-300)
+        assert err < 2e-5, (k, err)
