@@ -302,11 +302,12 @@ int mhd_ctx_tune(void* ctx, int32_t stencil, int32_t force_shape);
    the caller's parameters (seeded through the initial state and through
    alpha_max).  The context's parameters must have iterate = 0.  The step
    size is a plain value: the adaptive rule is not differentiated (frozen
-   dt).  Neighbours: all-pairs search with the exact rule, so
-   n <= MHD_TANGENT_MAX_N.  alpha_max: host array of 1 + MHD_TANGENT_DIRS
-   doubles (value and derivatives), or null for the context's value. */
+   dt).  Neighbours: a cell grid over each pass's positions and smoothing
+   lengths with the exact rule (any n <= the context's n_max; the
+   particles keep the caller's order).  alpha_max: host array of
+   1 + MHD_TANGENT_DIRS doubles (value and derivatives), or null for the
+   context's value. */
 #define MHD_TANGENT_DIRS 2
-#define MHD_TANGENT_MAX_N 65536
 int mhd_tangent_dirs(void);
 /* src/application.py:99-108: Bevol = B / rho, psi = 0, predicted copies. */
 int mhd_tangent_sync(void* ctx, MhdState* s, int64_t n, void* stream);
@@ -321,7 +322,7 @@ int mhd_tangent_magnetic_energy(void* ctx, const MhdState* s, int64_t n, double*
 /* ---- derivative form (reverse mode, checkpointed) ----
    No counterpart in the reference.  L = sum_i m_i |B_i|^2 / (2 mu0 rho_i)
    after `steps` literal PEC steps from the state in `s` (plain FP64 fields;
-   single density pass, n <= MHD_TANGENT_MAX_N), and its adjoint:
+   single density pass, n <= the context's n_max), and its adjoint:
    lambda0 = dL/dS_0 over the MHD_ADJOINT_FIELDS step-state fields
    (mhd_adjoint_field_name order, field-major, device, fields x n) and
    dL/d alpha_max through the steps.  The step sizes are frozen: on input

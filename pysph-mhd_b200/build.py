@@ -17,7 +17,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libmhd_b200.so")
 OBJ = os.path.join(HERE, "_build")
 SOURCES = ["mhd_abi.cu", "mhd_cells.cu", "mhd_pairs.cu", "mhd_force.cu", "mhd_integrate.cu", "mhd_noalloc.cu",
-           "mhd_tangent.cu", "mhd_adjoint.cu"]
+           "mhd_pairgrid.cu", "mhd_tangent.cu", "mhd_adjoint.cu"]
 # The derivative forms follow the reference's expression order: no FMA contraction.
 FILE_FLAGS = {"mhd_tangent.cu": ["--fmad=false"], "mhd_adjoint.cu": ["--fmad=false"]}
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

@@ -737,6 +737,7 @@ int mhd_ctx_destroy(void* ctx) {
   if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
   cudaFree(c->tan_work);
   cudaFree(c->adj_buf);
+  free_pair_grid(c->pgrid);
   delete c;
   return MHD_OK;
 }

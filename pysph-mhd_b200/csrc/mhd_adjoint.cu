@@ -15,7 +15,8 @@
 // per particle, pair terms per pair in gather form (a particle collects the
 // terms in which it is the i side and those in which it is the j side, so
 // there are no atomics).  The energy limiter's time scale (from dt_cfl) is
-// held at its value, like the step size.  Neighbours: all-pairs search with
+// held at its value, like the step size.  Neighbours: the cell grid of
+// mhd_pairgrid.cuh over each pass's positions and smoothing lengths, with
 // the exact rule.  Compiled with --fmad=false like the forward-mode file.
 #include <cuda_runtime.h>
 
@@ -24,6 +25,7 @@
 #include "mhd_common.cuh"
 #include "mhd_dual.cuh"
 #include "mhd_internal.h"
+#include "mhd_pairgrid.cuh"
 #include "mhd_step_fns.cuh"
 
 namespace mhd {
@@ -44,46 +46,6 @@ enum { T_S = 0, T_X = 24, T_VH = 27, T_VP = 30, T_EH = 33, T_EP = 34, T_HP = 35,
 enum { L_X = 0, L_VH = 3, L_VP = 6, L_EH = 9, L_EP = 10, L_HP = 11, L_A1 = 12, L_BH = 13, L_BP = 16, L_PSIH = 19,
        L_PSIP = 20, L_HN = 21, L_OM = 22, L_RHO = 23, L_P = 24, L_CS = 25, L_B = 26, M_D = 29, M_CD = 31, M_F = 58,
        L_RATES = 72, NL = 81 };  // L_RATES: au 3, ae, ah, ab 3, apsi
-
-// The pair search of every pass: all j (ascending) with r2 < (R h_i)^2 or
-// r2 < (R h_j)^2 for the positions x, y, z and smoothing lengths h, self
-// included, f(j, x_i - x_j min image), over one slice of the candidates.
-// The candidates are staged a block-wide tile at a time; the tiles within
-// reach of the warp (in ascending order) are dealt round robin to `slices`
-// slices and this call visits those of slice `slice`, so the pairs of a
-// warp spread evenly over the slices wherever its neighbours lie in the
-// index order.  Which tiles are within reach is warp-uniform (the box
-// reductions give every lane the same values).
-template <int DIM, class F>
-__device__ inline void pairs_in_slice(int n, const DevParams& P, int i, const double* x, const double* y,
-                                      const double* z, const double* h, int slice, int slices, F&& f) {
-  __shared__ double4 shr[kTile];
-  const bool active = i < n;
-  const double xi = active ? x[i] : 0.0, yi = active ? y[i] : 0.0, zi = active && DIM == 3 ? z[i] : 0.0;
-  const double rhi2 = active ? rh2_exact(P.R, h[i]) : 0.0;
-  const PairBox wb = warp_pair_box<DIM>(active, xi, yi, zi, active ? h[i] : 0.0);
-  int near = 0;  // tiles within reach of the warp so far
-  for (int base = 0; base < n; base += kTile) {
-    const int j = base + threadIdx.x;
-    if (j < n) shr[threadIdx.x] = make_double4(x[j], y[j], DIM == 3 ? z[j] : 0.0, h[j]);
-    __syncthreads();
-    const int m = n - base < kTile ? n - base : kTile;
-    // every lane takes part in the tile box's warp reductions
-    const PairBox tb = tile_pair_box<DIM, kTile>(shr, m);
-    const bool mine = !pair_boxes_apart<DIM>(wb, tb, P.R, P.L, P.periodic) && near++ % slices == slice;
-    if (active && mine) {
-      for (int t = 0; t < m; t++) {
-        const double4 q = shr[t];
-        const double dx = min_image(xi - q.x, P.L[0], P.half[0], P.periodic[0]);
-        const double dy = min_image(yi - q.y, P.L[1], P.half[1], P.periodic[1]);
-        const double dz = DIM == 3 ? min_image(zi - q.z, P.L[2], P.half[2], P.periodic[2]) : 0.0;
-        const double r2 = r2_exact(dx, dy, dz);
-        if (r2 < rhi2 || r2 < rh2_exact(P.R, q.w)) f(base + t, dx, dy, dz);
-      }
-    }
-    __syncthreads();
-  }
-}
 
 template <int N>
 __device__ inline Dual<N> seeded(double v, int k) {
@@ -109,9 +71,24 @@ struct Args {
   double* g_amax;          // reverse: per-particle dL/d alpha_max (accumulating over steps)
   const double* s_final;   // reverse, last step: S_K (loss terms)
   double* dta_out;         // forward: dt_adapt of the step (adaptive step sizes)
-  double* slices;          // reverse: per-slice partial sums of the force pair pass
+  double* slices;          // per-slice partial sums of the pair passes
   int dual_pairs;          // reverse: force and CD pair VJPs from dual Jacobians (check path) instead of by hand
+  // the neighbour search of the pair passes (mhd_pairgrid.cuh), rebuilt
+  // before each pass over its positions and smoothing lengths
+  const PairGrid* pg;
+  const int* cell_start;
+  const int* perm;
+  const double4* pos;
+  int nslices;
 };
+
+// f(j, dx, dy, dz) for every neighbour j of particle i (i < n) under the
+// exact rule, among the particles of this block's slice (grid y).
+template <int DIM, class F>
+__device__ inline void a_pairs(const Args& a, int i, F&& f) {
+  if (i >= a.n) return;
+  pair_grid_visit<DIM>(*a.pg, a.cell_start, a.perm, a.pos, a.P, i, (int)blockIdx.y, a.nslices, f);
+}
 
 #define TP(k, i) a.tape_w[(size_t)(k) * a.n + (i)]
 #define TR(k, i) a.tape[(size_t)(k) * a.n + (i)]
@@ -121,18 +98,17 @@ struct Args {
 #define LS(k, i) a.lam[(size_t)(k) * a.n + (i)]
 #define W(k, i) a.w[(size_t)(k) * a.n + (i)]
 
-// Pair passes split over kPairSlices slices of candidate tiles (grid y,
-// pairs_in_slice): each writes `width` partial sums per particle and slice,
-// value q of slice s at slices[(s * width + q) * n + i], and a per-particle
+// Pair passes split over a.nslices slices of the particles (grid y,
+// a_pairs): each writes `width` partial sums per particle and slice, value
+// q of slice s at slices[(s * width + q) * n + i], and a per-particle
 // kernel adds the slices in slice order (deterministic).
-constexpr int kPairSlices = 8;
 constexpr int kSliceWidth = 24;  // the widest partial record (the 24 CD moments)
 __device__ inline double& slice_part(const Args& a, int width, int q, int i) {
   return a.slices[((size_t)blockIdx.y * width + q) * a.n + i];
 }
 __device__ inline double slices_sum(const Args& a, int width, int q, int i) {
   double v = 0.0;
-  for (int s = 0; s < kPairSlices; s++) v += a.slices[((size_t)s * width + q) * a.n + i];
+  for (int s = 0; s < a.nslices; s++) v += a.slices[((size_t)s * width + q) * a.n + i];
   return v;
 }
 
@@ -276,12 +252,10 @@ template <int K, int DIM>
 __global__ void __launch_bounds__(kTile) k_f_density_pair(Args a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int n = a.n;
-  const double* X = a.tape_w + (size_t)T_X * n;
   const double* HP = a.tape_w + (size_t)T_HP * n;
   double rho = 0.0, dwdh = 0.0;
   const double hi = i < n ? HP[i] : 1.0;
-  pairs_in_slice<DIM>(n, a.P, i, X, X + n, X + 2 * n, HP, blockIdx.y, kPairSlices,
-                      [&](int j, double dx, double dy, double dz) {
+  a_pairs<DIM>(a, i, [&](int j, double dx, double dy, double dz) {
     const double xij[3] = {dx, dy, dz};
     f_density_pair<K, DIM>(a.P.norm, xij, hi, a.m[j], rho, dwdh);
   });
@@ -322,13 +296,11 @@ template <int K, int DIM>
 __global__ void __launch_bounds__(kTile) k_f_cd_pair(Args a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int n = a.n;
-  const double* X = a.tape_w + (size_t)T_X * n;
   const double* HN = a.tape_w + (size_t)T_HN * n;
   double r[6] = {}, vv[9] = {}, aa[9] = {};
   const int ii = i < n ? i : 0;
   const double hi = HN[ii];
-  pairs_in_slice<DIM>(n, a.P, i, X, X + n, X + 2 * n, HN, blockIdx.y, kPairSlices,
-                      [&](int j, double dx, double dy, double dz) {
+  a_pairs<DIM>(a, i, [&](int j, double dx, double dy, double dz) {
     const double xij[3] = {dx, dy, dz};
     double dv[3], da[3];
     for (int c = 0; c < 3; c++) {
@@ -372,13 +344,10 @@ template <int K, int DIM>
 __global__ void __launch_bounds__(kTile) k_f_force_pair(Args a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int n = a.n;
-  const double* X = a.tape_w + (size_t)T_X * n;
-  const double* HN = a.tape_w + (size_t)T_HN * n;
   const Side<double> I = side_values(a.tape_w, n, i < n ? i : 0);
   FSums<double> S;
   S.zero();
-  pairs_in_slice<DIM>(n, a.P, i, X, X + n, X + 2 * n, HN, blockIdx.y, kPairSlices,
-                      [&](int j, double dx, double dy, double dz) {
+  a_pairs<DIM>(a, i, [&](int j, double dx, double dy, double dz) {
     const double xij[3] = {dx, dy, dz};
     f_force_pair<K, DIM>(a.P, I, side_values(a.tape_w, n, j), a.m[j], xij, S);
   });
@@ -402,7 +371,7 @@ __global__ void __launch_bounds__(kTile) k_f_force(Args a) {
   S.zero();
   double* sp[kFSumDirs];
   fsum_ptrs(S, sp);
-  for (int sl = 0; sl < kPairSlices; sl++) {
+  for (int sl = 0; sl < a.nslices; sl++) {
     const double* part = a.slices + (size_t)sl * kFwdSums * n;
     for (int k = 0; k < kFSumDirs; k++) *sp[k] += part[(size_t)k * n + i];
     S.dtcfl = fmax(S.dtcfl, part[(size_t)kFSumDirs * n + i]);
@@ -581,10 +550,9 @@ __device__ inline void add_side(const Args& a, int i, const double* g, double si
 // through its j side and x_k.  The kSideDirs + 3 input directions are
 // evaluated a window of kForceWindow at a time, so the dual sums a thread
 // holds stay small (the same derivatives as one pass over all directions).
-// The candidate tiles within reach of a warp are dealt to kPairSlices
-// slices (grid y, pairs_in_slice), so that a small particle count still
-// fills the GPU; each slice writes its partial sums and k_r_force_pair_sum
-// adds them in slice order (deterministic).
+// The particles are dealt to a.nslices slices (grid y, a_pairs), so that a
+// small particle count still fills the GPU; each slice writes its partial
+// sums and k_r_force_pair_sum adds them in slice order (deterministic).
 constexpr int kForceWindow = 6;
 constexpr int kForceDirs = kSideDirs + 3;
 
@@ -594,14 +562,12 @@ __global__ void __launch_bounds__(kTile) k_r_force_pair(Args a) {
   using D = Dual<NW>;
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int n = a.n;
-  const double* X = a.tape + (size_t)T_X * n;
-  const double* HN = a.tape + (size_t)T_HN * n;
   const int kk = k < n ? k : 0;
   double gs[kSideDirs] = {}, gx[3] = {};
   if constexpr (!DUAL) {
     // hand-written VJP (vjp_force_pair)
     const Side<double> Kv = side_values(a.tape, n, kk);
-    pairs_in_slice<DIM>(n, a.P, k, X, X + n, X + 2 * n, HN, blockIdx.y, kPairSlices, [&](int j, double dx, double dy, double dz) {
+    a_pairs<DIM>(a, k, [&](int j, double dx, double dy, double dz) {
       const Side<double> Jv = side_values(a.tape, n, j);
       double w[kFSumDirs], gI[kSideDirs], gJ[kSideDirs], gxx[3];
       // (k, j): k is the i side
@@ -618,7 +584,7 @@ __global__ void __launch_bounds__(kTile) k_r_force_pair(Args a) {
       for (int c = 0; c < 3; c++) gx[c] -= gxx[c];
     });
   } else {
-  pairs_in_slice<DIM>(n, a.P, k, X, X + n, X + 2 * n, HN, blockIdx.y, kPairSlices, [&](int j, double dx, double dy, double dz) {
+  a_pairs<DIM>(a, k, [&](int j, double dx, double dy, double dz) {
     const Side<D> Jval = side_at<D>(a.tape, n, j, -1);
     for (int lo = 0; lo < ND; lo += NW) {
       const Side<D> Kseed = side_window<NW>(a.tape, n, kk, lo);
@@ -673,7 +639,7 @@ __global__ void __launch_bounds__(256) k_r_force_pair_sum(Args a) {
   double g[kForceDirs];
   for (int d = 0; d < kForceDirs; d++) {
     double v = 0.0;
-    for (int s = 0; s < kPairSlices; s++) v += a.slices[((size_t)s * kForceDirs + d) * n + k];
+    for (int s = 0; s < a.nslices; s++) v += a.slices[((size_t)s * kForceDirs + d) * n + k];
     g[d] = v;
   }
   add_side(a, k, g, 1.0, g + kSideDirs);
@@ -710,12 +676,10 @@ __global__ void __launch_bounds__(kTile) k_r_cd_pair(Args a) {
   using D = Dual<10>;  // x_ij 3, h_i, dv 3, da 3
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int n = a.n;
-  const double* X = a.tape + (size_t)T_X * n;
   const double* HN = a.tape + (size_t)T_HN * n;
   const int kk = k < n ? k : 0;
   double gx[3] = {}, gh = 0.0, gv[3] = {}, ga[3] = {};
-  pairs_in_slice<DIM>(n, a.P, k, X, X + n, X + 2 * n, HN, blockIdx.y, kPairSlices,
-                      [&](int j, double dx, double dy, double dz) {
+  a_pairs<DIM>(a, k, [&](int j, double dx, double dy, double dz) {
     for (int side = 0; side < 2; side++) {
       // side 0: pair (k, j); side 1: pair (j, k)
       const int ii = side ? j : kk, jj = side ? kk : j;
@@ -819,12 +783,10 @@ __global__ void __launch_bounds__(kTile) k_r_density_pair(Args a) {
   using D = Dual<4>;  // x_ij 3, h_i
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int n = a.n;
-  const double* X = a.tape + (size_t)T_X * n;
   const double* HP = a.tape + (size_t)T_HP * n;
   const int kk = k < n ? k : 0;
   double gx[3] = {}, gh = 0.0;
-  pairs_in_slice<DIM>(n, a.P, k, X, X + n, X + 2 * n, HP, blockIdx.y, kPairSlices,
-                      [&](int j, double dx, double dy, double dz) {
+  a_pairs<DIM>(a, k, [&](int j, double dx, double dy, double dz) {
     for (int side = 0; side < 2; side++) {
       const int ii = side ? j : kk, jj = side ? kk : j;
       const double sgn = side ? -1.0 : 1.0;
@@ -885,38 +847,67 @@ __global__ void __launch_bounds__(256) k_pack_state(int n, MhdState s, double* o
 #undef LS
 #undef W
 
+// {x, y, z, h} of a tape's positions and one of its smoothing lengths, for
+// the grid build.
+template <int DIM>
+__global__ void __launch_bounds__(256) k_pack_pos(int n, const double* __restrict__ X,
+                                                  const double* __restrict__ H, double4* __restrict__ pos) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  pos[i] = make_double4(X[i], X[n + i], DIM == 3 ? X[2 * n + i] : 0.0, H[i]);
+}
+
+// The grid of a tape's positions and the smoothing lengths at offset `h`.
+template <int DIM>
+static void grid_for(Ctx* c, Args& a, const double* tape, int h, cudaStream_t st) {
+  k_pack_pos<DIM><<<(a.n + 255) / 256, 256, 0, st>>>(a.n, tape + (size_t)T_X * a.n, tape + (size_t)h * a.n,
+                                                     c->pgrid.pos);
+  c->launches++;
+  build_pair_grid(c, c->pgrid, a.n, st);
+  a.pg = c->pgrid.grid;
+  a.cell_start = c->pgrid.cell_start;
+  a.perm = c->pgrid.perm;
+  a.pos = c->pgrid.pos;
+}
+
 template <int K, int DIM>
-static void forward_step(const Args& a, cudaStream_t st) {
+static void forward_step(Ctx* c, Args a, cudaStream_t st) {
   const int nb = (a.n + kTile - 1) / kTile, np = (a.n + 255) / 256;
+  const dim3 sliced(nb, a.nslices);
   k_f_predict<<<np, 256, 0, st>>>(a);
-  k_f_density_pair<K, DIM><<<dim3(nb, kPairSlices), kTile, 0, st>>>(a);
+  grid_for<DIM>(c, a, a.tape_w, T_HP, st);  // the density pass: predicted h
+  k_f_density_pair<K, DIM><<<sliced, kTile, 0, st>>>(a);
   k_f_density<DIM><<<np, 256, 0, st>>>(a);
   k_f_prologue<DIM><<<np, 256, 0, st>>>(a);
-  k_f_cd_pair<K, DIM><<<dim3(nb, kPairSlices), kTile, 0, st>>>(a);
+  grid_for<DIM>(c, a, a.tape_w, T_HN, st);  // the later groups: the new h
+  k_f_cd_pair<K, DIM><<<sliced, kTile, 0, st>>>(a);
   k_f_cd<<<np, 256, 0, st>>>(a);
-  k_f_force_pair<K, DIM><<<dim3(nb, kPairSlices), kTile, 0, st>>>(a);
+  k_f_force_pair<K, DIM><<<sliced, kTile, 0, st>>>(a);
   k_f_force<DIM><<<nb, kTile, 0, st>>>(a);
 }
 
 template <int K, int DIM>
-static void reverse_step(const Args& a, cudaStream_t st) {
+static void reverse_step(Ctx* c, Args a, cudaStream_t st) {
   const int nb = (a.n + kTile - 1) / kTile, np = (a.n + 255) / 256, n64 = (a.n + 63) / 64;
+  const dim3 sliced(nb, a.nslices);
   k_r_correct<<<np, 256, 0, st>>>(a);
   k_r_force_post<DIM><<<n64, 64, 0, st>>>(a);
+  grid_for<DIM>(c, a, a.tape, T_HN, st);
   if (a.dual_pairs)
-    k_r_force_pair<K, DIM, true><<<dim3(nb, kPairSlices), kTile, 0, st>>>(a);
+    k_r_force_pair<K, DIM, true><<<sliced, kTile, 0, st>>>(a);
   else
-    k_r_force_pair<K, DIM, false><<<dim3(nb, kPairSlices), kTile, 0, st>>>(a);
+    k_r_force_pair<K, DIM, false><<<sliced, kTile, 0, st>>>(a);
   k_r_force_pair_sum<<<np, 256, 0, st>>>(a);
   k_r_cd_post<<<n64, 64, 0, st>>>(a);
   if (a.dual_pairs)
-    k_r_cd_pair<K, DIM, true><<<dim3(nb, kPairSlices), kTile, 0, st>>>(a);
+    k_r_cd_pair<K, DIM, true><<<sliced, kTile, 0, st>>>(a);
   else
-    k_r_cd_pair<K, DIM, false><<<dim3(nb, kPairSlices), kTile, 0, st>>>(a);
+    k_r_cd_pair<K, DIM, false><<<sliced, kTile, 0, st>>>(a);
   k_r_cd_sum<<<np, 256, 0, st>>>(a);
   k_r_prologue<DIM><<<np, 256, 0, st>>>(a);
   k_r_density_post<DIM><<<np, 256, 0, st>>>(a);
-  k_r_density_pair<K, DIM><<<dim3(nb, kPairSlices), kTile, 0, st>>>(a);
+  grid_for<DIM>(c, a, a.tape, T_HP, st);
+  k_r_density_pair<K, DIM><<<sliced, kTile, 0, st>>>(a);
   k_r_density_sum<<<np, 256, 0, st>>>(a);
   k_r_predict<<<n64, 64, 0, st>>>(a);
 }
@@ -985,15 +976,14 @@ AdjLayout layout(int64_t n, int every) {
   L.dta = take(n);
   L.part = take(n / 256 + 64);
   static_assert(kFwdSums <= kSliceWidth && kForceDirs <= kSliceWidth, "slice records fit the buffer");
-  L.slices = take((size_t)kPairSlices * kSliceWidth * n);
+  L.slices = take((size_t)derivative_slices(n) * kSliceWidth * n);
   L.total = off;
   return L;
 }
 
 int check_adjoint(Ctx* c, const MhdState* s, int64_t n, int steps, const double* dts, int every, bool adaptive) {
   if (!s || !s->m || !s->itype) A_FAIL(MHD_ERR_INVALID, "state, m or itype is null");
-  if (n < 1 || n > c->n_max || n > MHD_TANGENT_MAX_N)
-    A_FAIL(MHD_ERR_INVALID, "n must be in [1, min(n_max, MHD_TANGENT_MAX_N)]");
+  if (n < 1 || n > c->n_max) A_FAIL(MHD_ERR_INVALID, "n must be in [1, n_max]");
   if (c->P.iterate) A_FAIL(MHD_ERR_INVALID, "the adjoint needs the single density pass (iterate = 0)");
   if (steps < 1 || !dts) A_FAIL(MHD_ERR_INVALID, "steps must be >= 1 and dts non-null");
   if (every < 1 || every > 256) A_FAIL(MHD_ERR_INVALID, "every must be in [1, 256]");
@@ -1009,6 +999,7 @@ int check_adjoint(Ctx* c, const MhdState* s, int64_t n, int steps, const double*
     A_CK(cudaMalloc(&c->adj_buf, sizeof(double) * L.total));
     c->adj_size = L.total;
   }
+  if (alloc_pair_grid(c->pgrid, c->n_max) != MHD_OK) A_FAIL(MHD_ERR_CUDA, "pair grid allocation failed");
   return MHD_OK;
 }
 
@@ -1020,6 +1011,7 @@ Args base_args(Ctx* c, const MhdState* s, int64_t n, double amax) {
   a.amax = amax;
   a.m = s->m;
   a.itype = s->itype;
+  a.nslices = derivative_slices(n);
   return a;
 }
 
@@ -1038,7 +1030,7 @@ double* run_segment(Ctx* c, Args a, const AdjLayout& L, const double* s0, int k0
     a.dt = dts[t];
     a.dta_out = buf + L.dta;
     a.slices = buf + L.slices;
-    MHD_A_DISPATCH(forward_step, a, st);
+    MHD_A_DISPATCH(forward_step, c, a, st);
     c->launches += 8;
     time += dts[t];
     if (t + 1 < steps && dts[t + 1] < 0.0) {
@@ -1139,7 +1131,7 @@ int mhd_adjoint_backward(void* ctx, const MhdState* s, int64_t n, int32_t steps,
         k_r_seed<<<np, 256, 0, st>>>(r);
         c->launches++;
       }
-      MHD_A_DISPATCH(reverse_step, r, st);
+      MHD_A_DISPATCH(reverse_step, c, r, st);
       c->launches += 12;
       double* tmp = lam_next;
       lam_next = lam;

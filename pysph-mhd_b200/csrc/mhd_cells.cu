@@ -471,8 +471,12 @@ void launch_sort_cells(Ctx* c, const MhdState* s, int n, cudaStream_t st) {
       k_cell_keys<2><<<nb, 256, 0, st>>>(n, c->d_grids, c->inst, s->x, s->y, s->z, c->keys[0], c->vals[0]);
     c->launches++;
   }
+  sort_keys_to_cells(c, n, c->key_cells, c->cell_start, st);
+}
+
+void sort_keys_to_cells(Ctx* c, int n, int64_t ncells, int* cell_start, cudaStream_t st) {
   int bits = 1;
-  while ((1LL << bits) < (int64_t)c->key_cells) bits++;
+  while ((1LL << bits) < ncells) bits++;
   const int passes = (bits + 7) / 8;
   const int sb = max_sort_blocks(n);
   int cur = 0;
@@ -487,8 +491,7 @@ void launch_sort_cells(Ctx* c, const MhdState* s, int n, cudaStream_t st) {
   }
   c->sorted_keys = c->keys[cur];
   c->perm = c->vals[cur];
-  k_cell_starts<<<ceil_div((int64_t)c->key_cells + 1, 256), 256, 0, st>>>(n, c->key_cells, c->sorted_keys,
-                                                                         c->cell_start);
+  k_cell_starts<<<ceil_div(ncells + 1, 256), 256, 0, st>>>(n, (int)ncells, c->sorted_keys, cell_start);
   c->launches++;
 }
 

@@ -190,7 +190,7 @@ __device__ __forceinline__ double pow_dim(double a) {
 }
 
 // Minimum-image displacement along one periodic axis.
-__device__ __forceinline__ double min_image(double d, double L, double half, int periodic) {
+__host__ __device__ __forceinline__ double min_image(double d, double L, double half, int periodic) {
   if (periodic) {
     if (d > half) d = d - L;
     if (d < -half) d = d + L;
@@ -198,101 +198,26 @@ __device__ __forceinline__ double min_image(double d, double L, double half, int
   return d;
 }
 
-// --------------------------------------------- all-pairs tile skipping
-// The all-pairs searches of the derivative forms stage blocks of candidates
-// in shared memory and test every (i, j).  A warp skips a staged tile when
-// no candidate can be within reach of any of its particles: per axis the
-// gap between the two bounding intervals, the smallest over the images -L,
-// 0, +L on a periodic axis, bounds |min_image(x_i - x_j)| from below, and
-// a gap beyond R max(h_i, h_j) on any axis fails r2 < (R h)^2 for every
-// pair.  The skip changes neither which pairs are visited nor their order.
-struct PairBox {
-  double lo[3], hi[3], h;
-};
-
-__device__ __forceinline__ double warp_min_d(double v) {
-  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
-  return v;
-}
-__device__ __forceinline__ double warp_max_d(double v) {
-  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-  return v;
-}
-
-// Bounding box of the active lanes' particles.  Every lane of the warp must
-// call it (warp reductions), active particle or not.
-template <int DIM>
-__device__ __forceinline__ PairBox warp_pair_box(bool active, double x, double y, double z, double h) {
-  const double inf = __longlong_as_double(0x7ff0000000000000LL);
-  PairBox b;
-  b.lo[0] = warp_min_d(active ? x : inf);
-  b.hi[0] = warp_max_d(active ? x : -inf);
-  b.lo[1] = warp_min_d(active ? y : inf);
-  b.hi[1] = warp_max_d(active ? y : -inf);
-  b.lo[2] = DIM == 3 ? warp_min_d(active ? z : inf) : 0.0;
-  b.hi[2] = DIM == 3 ? warp_max_d(active ? z : -inf) : 0.0;
-  b.h = warp_max_d(active ? h : -inf);
-  return b;
-}
-
-// Bounding box of the m staged candidates {x, y, z, h}.  Every lane of the
-// warp must call it (warp reductions), active particle or not.
-template <int DIM, int TILE>
-__device__ __forceinline__ PairBox tile_pair_box(const double4* sh, int m) {
-  const double inf = __longlong_as_double(0x7ff0000000000000LL);
-  const int lane = threadIdx.x & 31;
-  double lo[3] = {inf, inf, inf}, hi[3] = {-inf, -inf, -inf}, h = -inf;
-  for (int t = lane; t < m; t += 32) {
-    const double4 q = sh[t];
-    lo[0] = fmin(lo[0], q.x);
-    hi[0] = fmax(hi[0], q.x);
-    lo[1] = fmin(lo[1], q.y);
-    hi[1] = fmax(hi[1], q.y);
-    if (DIM == 3) {
-      lo[2] = fmin(lo[2], q.z);
-      hi[2] = fmax(hi[2], q.z);
-    }
-    h = fmax(h, q.w);
-  }
-  PairBox b;
-  for (int a = 0; a < DIM; a++) {
-    b.lo[a] = warp_min_d(lo[a]);
-    b.hi[a] = warp_max_d(hi[a]);
-  }
-  if (DIM == 2) b.lo[2] = b.hi[2] = 0.0;
-  b.h = warp_max_d(h);
-  return b;
-}
-
-// True when no pair of the two boxes can pass the neighbour test.  The
-// reach carries a relative slack of 1e-6 and an absolute one of a few ulp
-// of the coordinates, far above the rounding of the test itself.
-template <int DIM>
-__host__ __device__ __forceinline__ bool pair_boxes_apart(const PairBox& w, const PairBox& t, double R,
-                                                          const double* L, const int* periodic) {
-  const double reach = R * fmax(w.h, t.h) * (1.0 + 1e-6);
-  for (int a = 0; a < DIM; a++) {
-    double g = fmax(t.lo[a] - w.hi[a], w.lo[a] - t.hi[a]);
-    if (periodic[a]) {
-      g = fmin(g, fmax(t.lo[a] + L[a] - w.hi[a], w.lo[a] - t.hi[a] - L[a]));
-      g = fmin(g, fmax(t.lo[a] - L[a] - w.hi[a], w.lo[a] - t.hi[a] + L[a]));
-    }
-    const double ulps = 1e-14 * (fabs(w.lo[a]) + fabs(w.hi[a]) + fabs(t.lo[a]) + fabs(t.hi[a]) + fabs(L[a]));
-    if (g > reach + ulps) return true;
-  }
-  return false;
-}
-
 // Squared distance evaluated without FMA contraction, in the oracle's order
 // ((dx*dx + dy*dy) + dz*dz), so neighbour sets are bit-identical to it.
-__device__ __forceinline__ double r2_exact(double dx, double dy, double dz) {
+// (Host code: compiled without contraction, as the oracle is.)
+__host__ __device__ __forceinline__ double r2_exact(double dx, double dy, double dz) {
+#ifdef __CUDA_ARCH__
   return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+#else
+  return (dx * dx + dy * dy) + dz * dz;
+#endif
 }
 
 // (R*h)^2 without contraction.
-__device__ __forceinline__ double rh2_exact(double R, double h) {
+__host__ __device__ __forceinline__ double rh2_exact(double R, double h) {
+#ifdef __CUDA_ARCH__
   const double rh = __dmul_rn(R, h);
   return __dmul_rn(rh, rh);
+#else
+  const double rh = R * h;
+  return rh * rh;
+#endif
 }
 
 __device__ __forceinline__ unsigned long long dbl_order(double v) {

@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "mhd_common.cuh"
+#include "mhd_pairgrid.cuh"
 
 namespace mhd {
 
@@ -50,6 +51,7 @@ struct Ctx {
   int graph_passes = 8;           // density passes captured per right-hand side
   cudaStream_t cap_stream = nullptr;
   void* tan_work = nullptr;  // derivative form: new h / energy partials (dual records)
+  PairGridBufs pgrid;        // derivative forms: the cell grid of their pair passes
   void* adj_buf = nullptr;   // adjoint: states, tapes, reverse workspace (doubles)
   size_t adj_size = 0;
   struct GraphEntry {
@@ -193,6 +195,11 @@ int64_t scan_sums_needed(int64_t n_max);
 void launch_reduce_hbox(Ctx* c, const MhdState* s, int n, cudaStream_t st);
 void launch_sort_cells(Ctx* c, const MhdState* s, int n, cudaStream_t st);
 void launch_gather(Ctx* c, const GatherSet& gs, int n, cudaStream_t st);
+// Stable sort of (c->keys[0][i], c->vals[0][i]) by key for keys below
+// ncells, leaving the sorted keys in c->sorted_keys and the values (the
+// permutation) in c->perm, then cell_start[k] = first sorted slot with key
+// >= k for k in [0, ncells].
+void sort_keys_to_cells(Ctx* c, int n, int64_t ncells, int* cell_start, cudaStream_t st);
 
 void launch_reset_hbox(Ctx* c, cudaStream_t st);
 void launch_plan_grids(Ctx* c, cudaStream_t st);

@@ -7,12 +7,11 @@
 // (src/integrator.py:68-82) -- written once over a scalar type and run on
 // dual numbers: every state value carries its derivatives with respect to
 // MHD_TANGENT_DIRS parameters.  The step size is a plain value (frozen: the
-// adaptive rule's min() is not differentiated).  Neighbours come from a tiled
-// all-pairs search with the exact FP64 rule, in ascending index order, so the
-// primal values follow the oracle's summation order; the form is meant for
-// the small cases a gradient check uses (n <= MHD_TANGENT_MAX_N).
-// Compiled with --fmad=false: no contraction, the reference's expression
-// order throughout.
+// adaptive rule's min() is not differentiated).  Neighbours come from the
+// cell grid of mhd_pairgrid.cuh, built over each pass's positions and
+// smoothing lengths, with the exact FP64 rule.  Compiled with
+// --fmad=false: no contraction, the reference's expression order
+// throughout.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -22,6 +21,7 @@
 #include "mhd_common.cuh"
 #include "mhd_dual.cuh"
 #include "mhd_internal.h"
+#include "mhd_pairgrid.cuh"
 
 namespace mhd {
 
@@ -72,57 +72,44 @@ __device__ inline D pmax(const D& a, const D& b) { return b > a ? b : a; }
 template <class D>
 __device__ inline D pmin(const D& a, const D& b) { return b < a ? b : a; }
 
-// ------------------------------------------------------- all-pairs search
-// Calls f(j) for every j (ascending) with r2 < (R h_i)^2 or r2 < (R h_j)^2
-// on the minimum-image FP64 values, self included, within one slice of the
-// candidates.  The block (kTile threads) stages kTile positions at a time
-// in shared memory; every thread of the block must call it.  The tiles
-// within reach of a warp (bounding boxes) are dealt round robin to the
-// kTSlices slices (grid y), so that each slice has a share of every warp's
-// pairs; each pair kernel writes its partial sums per slice and a
+// ------------------------------------------------------- neighbour search
+// Calls f(j) for every j with r2 < (R h_i)^2 or r2 < (R h_j)^2 on the
+// minimum-image FP64 values, self included, among the particles of this
+// block's slice (grid y): the cell grid of mhd_pairgrid.cuh over the pass's
+// x and h.  Each pair kernel writes its partial sums per slice and a
 // per-particle kernel adds them in slice order (deterministic).
-constexpr int kTSlices = 8;
 constexpr int kTWidth = 24;  // partial records per particle and slice (the 24 CD moments at most)
+
+struct TGrid {
+  const PairGrid* g;
+  const int* cell_start;
+  const int* perm;
+  const double4* pos;
+  int slices;
+};
 
 __device__ inline TD& t_part(TD* part, int n, int q, int i) {
   return part[((size_t)blockIdx.y * kTWidth + q) * n + i];
 }
-__device__ inline TD t_slices_sum(const TD* part, int n, int q, int i) {
+__device__ inline TD t_slices_sum(const TD* part, int n, int q, int i, int slices) {
   TD v(0.0);
-  for (int sl = 0; sl < kTSlices; sl++) v = v + part[((size_t)sl * kTWidth + q) * n + i];
+  for (int sl = 0; sl < slices; sl++) v = v + part[((size_t)sl * kTWidth + q) * n + i];
   return v;
 }
 
 template <int DIM, class F>
-__device__ inline void all_pairs(int n, const DevParams& P, int i, const MhdState& s, F&& f) {
-  __shared__ double4 sh[kTile];
-  const bool active = i < n;
-  const TD *X = TF(x), *Y = TF(y), *Z = TF(z), *H = TF(h);
-  const double xi = active ? X[i].v : 0.0, yi = active ? Y[i].v : 0.0;
-  const double zi = active && DIM == 3 ? Z[i].v : 0.0;
-  const double rhi2 = active ? rh2_exact(P.R, H[i].v) : 0.0;
-  const PairBox wb = warp_pair_box<DIM>(active, xi, yi, zi, active ? H[i].v : 0.0);
-  int near = 0;  // tiles within reach of the warp so far
-  for (int base = 0; base < n; base += kTile) {
-    const int j = base + threadIdx.x;
-    if (j < n) sh[threadIdx.x] = make_double4(X[j].v, Y[j].v, DIM == 3 ? Z[j].v : 0.0, H[j].v);
-    __syncthreads();
-    const int m = n - base < kTile ? n - base : kTile;
-    // every lane takes part in the tile box's warp reductions
-    const PairBox tb = tile_pair_box<DIM, kTile>(sh, m);
-    const bool mine = !pair_boxes_apart<DIM>(wb, tb, P.R, P.L, P.periodic) && near++ % kTSlices == (int)blockIdx.y;
-    if (active && mine) {
-      for (int t = 0; t < m; t++) {
-        const double4 q = sh[t];
-        const double dx = min_image(xi - q.x, P.L[0], P.half[0], P.periodic[0]);
-        const double dy = min_image(yi - q.y, P.L[1], P.half[1], P.periodic[1]);
-        const double dz = DIM == 3 ? min_image(zi - q.z, P.L[2], P.half[2], P.periodic[2]) : 0.0;
-        const double r2 = r2_exact(dx, dy, dz);
-        if (r2 < rhi2 || r2 < rh2_exact(P.R, q.w)) f(base + t);
-      }
-    }
-    __syncthreads();
-  }
+__device__ inline void t_pairs(const TGrid& tg, const DevParams& P, int i, int n, F&& f) {
+  if (i >= n) return;
+  pair_grid_visit<DIM>(*tg.g, tg.cell_start, tg.perm, tg.pos, P, i, (int)blockIdx.y, tg.slices,
+                       [&](int j, double, double, double) { f(j); });
+}
+
+// {x, y, z, h} values of the current state for the grid build.
+template <int DIM>
+__global__ void __launch_bounds__(256) k_t_pack_pos(int n, MhdState s, double4* __restrict__ pos) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  pos[i] = make_double4(TF(x)[i].v, TF(y)[i].v, DIM == 3 ? TF(z)[i].v : 0.0, TF(h)[i].v);
 }
 
 // Minimum-image x_i - x_j along one axis as a dual number: the image shift
@@ -258,11 +245,11 @@ __global__ void __launch_bounds__(256) k_t_sync(int n, MhdState s) {
 // h_i, Omega from the old h, then h = hfact (m / rho)^(1/dim).  The new h goes
 // to h_new (other threads still read h).
 template <int K, int DIM>
-__global__ void __launch_bounds__(kTile) k_t_density_pair(int n, DevParams P, MhdState s, TD* __restrict__ part) {
+__global__ void __launch_bounds__(kTile) k_t_density_pair(int n, DevParams P, MhdState s, TD* __restrict__ part, TGrid tg) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   TD rho(0.0), dwdh(0.0);
   const TD hi = i < n ? TF(h)[i] : TD(1.0);
-  all_pairs<DIM>(n, P, i, s, [&](int j) {
+  t_pairs<DIM>(tg, P, i, n, [&](int j) {
     TD xij[3], rij;
     pair_geometry<DIM>(P, s, i, j, xij, rij);
     const TD mj = TF(m)[j];
@@ -276,11 +263,11 @@ __global__ void __launch_bounds__(kTile) k_t_density_pair(int n, DevParams P, Mh
 
 template <int DIM>
 __global__ void __launch_bounds__(256) k_t_density(int n, DevParams P, MhdState s, const TD* __restrict__ part,
-                                                   TD* __restrict__ h_new) {
+                                                   TD* __restrict__ h_new, int slices) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const TD hi = TF(h)[i];
-  const TD rho = t_slices_sum(part, n, 0, i), dwdh = t_slices_sum(part, n, 1, i);
+  const TD rho = t_slices_sum(part, n, 0, i, slices), dwdh = t_slices_sum(part, n, 1, i, slices);
   TF(rho_sum)[i] = rho;
   if (TF(converged)[i].v == 1.0) {
     // already finalised in this group evaluation (the warm-up's second and
@@ -322,14 +309,14 @@ __global__ void __launch_bounds__(256) k_t_prologue(int n, DevParams P, MhdState
 // src/equations.py:318-429 with the previous step's accelerations; the
 // alpha clip [alpha_min, alpha_max] with alpha_max a dual number.
 template <int K, int DIM>
-__global__ void __launch_bounds__(kTile) k_t_cd_pair(int n, DevParams P, MhdState s, TD* __restrict__ part) {
+__global__ void __launch_bounds__(kTile) k_t_cd_pair(int n, DevParams P, MhdState s, TD* __restrict__ part, TGrid tg) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   TD r[6], vv[9], aa[9];
   for (int k = 0; k < 6; k++) r[k] = TD(0.0);
   for (int k = 0; k < 9; k++) vv[k] = aa[k] = TD(0.0);
   const bool act = i < n;
   const TD hi = act ? TF(h)[i] : TD(1.0);
-  all_pairs<DIM>(n, P, i, s, [&](int j) {
+  t_pairs<DIM>(tg, P, i, n, [&](int j) {
     TD xij[3], rij, dwi[3];
     pair_geometry<DIM>(P, s, i, j, xij, rij);
     t_kern_grad<K, DIM>(P.norm, xij, rij, hi, dwi);
@@ -358,15 +345,15 @@ __global__ void __launch_bounds__(kTile) k_t_cd_pair(int n, DevParams P, MhdStat
 }
 
 __global__ void __launch_bounds__(256) k_t_cd(int n, DevParams P, MhdState s, const TD* __restrict__ part,
-                                              TD alpha_max) {
+                                              TD alpha_max, int slices) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const TD hi = TF(h)[i];
   TD r[6], vv[9], aa[9];
-  for (int k = 0; k < 6; k++) r[k] = t_slices_sum(part, n, k, i);
+  for (int k = 0; k < 6; k++) r[k] = t_slices_sum(part, n, k, i, slices);
   for (int k = 0; k < 9; k++) {
-    vv[k] = t_slices_sum(part, n, 6 + k, i);
-    aa[k] = t_slices_sum(part, n, 15 + k, i);
+    vv[k] = t_slices_sum(part, n, 6 + k, i, slices);
+    aa[k] = t_slices_sum(part, n, 15 + k, i, slices);
   }
   const TD rxx = r[0], rxy = r[1], rxz = r[2], ryy = r[3], ryz = r[4], rzz = r[5];
   const TD denom = rxx * ryy * rzz + 2.0 * rxy * rxz * ryz - rxx * ryz * ryz - ryy * rxz * rxz - rzz * rxy * rxy;
@@ -434,7 +421,7 @@ enum { TF_A6 = 0, TF_A8 = 3, TF_AE6 = 6, TF_AE9 = 7, TF_DIV = 8, TF_AB = 9, TF_D
        TF_DTCFL = 14, TF_JMAX = 15 };
 
 template <int K, int DIM>
-__global__ void __launch_bounds__(kTile) k_t_force_pair(int n, DevParams P, MhdState s, TD* __restrict__ part) {
+__global__ void __launch_bounds__(kTile) k_t_force_pair(int n, DevParams P, MhdState s, TD* __restrict__ part, TGrid tg) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const bool act = i < n;
   TD a6[3] = {TD(0.0), TD(0.0), TD(0.0)}, a8[3] = {TD(0.0), TD(0.0), TD(0.0)};
@@ -442,7 +429,7 @@ __global__ void __launch_bounds__(kTile) k_t_force_pair(int n, DevParams P, MhdS
   int jmax = INT_MAX;
   const int ii = act ? i : 0;
   T_FORCE_SIDE_I
-  all_pairs<DIM>(n, P, i, s, [&](int j) {
+  t_pairs<DIM>(tg, P, i, n, [&](int j) {
     TD xij[3], rij, dwi[3], dwj[3];
     pair_geometry<DIM>(P, s, i, j, xij, rij);
     t_kern_grad<K, DIM>(P.norm, xij, rij, hi, dwi);
@@ -473,7 +460,7 @@ __global__ void __launch_bounds__(kTile) k_t_force_pair(int n, DevParams P, MhdS
       TD c = vwave_i - beta * dot;
       c = pmax(c, vwave_j - beta * dot);
       c = pmax(c, TD(0.0));
-      if (c > dtcfl) {  // pmax(dtcfl, c), keeping the pair that set it
+      if (c > dtcfl || (c.v == dtcfl.v && j < jmax && jmax != INT_MAX)) {  // pmax, keeping the smallest j at the max
         dtcfl = c;
         jmax = j;
       }
@@ -559,7 +546,8 @@ __global__ void __launch_bounds__(kTile) k_t_force_pair(int n, DevParams P, MhdS
 }
 
 template <int DIM>
-__global__ void __launch_bounds__(256) k_t_force(int n, DevParams P, MhdState s, const TD* __restrict__ part) {
+__global__ void __launch_bounds__(256) k_t_force(int n, DevParams P, MhdState s, const TD* __restrict__ part,
+                                                 int slices) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int ii = i;
@@ -572,17 +560,17 @@ __global__ void __launch_bounds__(256) k_t_force(int n, DevParams P, MhdState s,
   (void)rho_i2_inv;
   TD a6[3], a8[3], ab[3];
   for (int a = 0; a < 3; a++) {
-    a6[a] = t_slices_sum(part, n, TF_A6 + a, i);
-    a8[a] = t_slices_sum(part, n, TF_A8 + a, i);
-    ab[a] = t_slices_sum(part, n, TF_AB + a, i);
+    a6[a] = t_slices_sum(part, n, TF_A6 + a, i, slices);
+    a8[a] = t_slices_sum(part, n, TF_A8 + a, i, slices);
+    ab[a] = t_slices_sum(part, n, TF_AB + a, i, slices);
   }
-  const TD ae6 = t_slices_sum(part, n, TF_AE6, i), ae9 = t_slices_sum(part, n, TF_AE9, i);
-  const TD div = t_slices_sum(part, n, TF_DIV, i);
-  const TD divbs = t_slices_sum(part, n, TF_DIVBS, i), divbd = t_slices_sum(part, n, TF_DIVBD, i);
+  const TD ae6 = t_slices_sum(part, n, TF_AE6, i, slices), ae9 = t_slices_sum(part, n, TF_AE9, i, slices);
+  const TD div = t_slices_sum(part, n, TF_DIV, i, slices);
+  const TD divbs = t_slices_sum(part, n, TF_DIVBS, i, slices), divbd = t_slices_sum(part, n, TF_DIVBD, i, slices);
   // the largest slice maximum; on a tie the one set by the smaller j
   TD dtcfl(0.0);
   double jbest = (double)INT_MAX;
-  for (int sl = 0; sl < kTSlices; sl++) {
+  for (int sl = 0; sl < slices; sl++) {
     const TD v = part[((size_t)sl * kTWidth + TF_DTCFL) * n + i];
     const double jv = part[((size_t)sl * kTWidth + TF_JMAX) * n + i].v;
     if (v > dtcfl || (v.v == dtcfl.v && jv < jbest)) {
@@ -667,19 +655,30 @@ __global__ void k_t_energy_final(int nb, const TD* __restrict__ part, TD* __rest
 #undef TF
 
 // ------------------------------------------------------------- launchers
+// The grid of the current x and h for the next pair passes.
+template <int DIM>
+static TGrid t_grid(Ctx* c, MhdState* s, int n, cudaStream_t st) {
+  k_t_pack_pos<DIM><<<(n + 255) / 256, 256, 0, st>>>(n, *s, c->pgrid.pos);
+  c->launches++;
+  build_pair_grid(c, c->pgrid, n, st);
+  return TGrid{c->pgrid.grid, c->pgrid.cell_start, c->pgrid.perm, c->pgrid.pos, derivative_slices(n)};
+}
+
 template <int K, int DIM>
 static void t_rhs_launch(Ctx* c, MhdState* s, int n, TD amax, cudaStream_t st) {
   const int nb = (n + kTile - 1) / kTile, np = (n + 255) / 256;
   TD* h_new = reinterpret_cast<TD*>(c->tan_work);
-  TD* part = h_new + c->n_max + 1024;  // kTSlices * kTWidth records per particle
-  const dim3 sliced(nb, kTSlices);
-  k_t_density_pair<K, DIM><<<sliced, kTile, 0, st>>>(n, c->P, *s, part);
-  k_t_density<DIM><<<np, 256, 0, st>>>(n, c->P, *s, part, h_new);
+  TD* part = h_new + c->n_max + 1024;  // slices * kTWidth records per particle
+  TGrid tg = t_grid<DIM>(c, s, n, st);  // density pass: the h before it
+  const dim3 sliced(nb, tg.slices);
+  k_t_density_pair<K, DIM><<<sliced, kTile, 0, st>>>(n, c->P, *s, part, tg);
+  k_t_density<DIM><<<np, 256, 0, st>>>(n, c->P, *s, part, h_new, tg.slices);
   k_t_prologue<DIM><<<np, 256, 0, st>>>(n, c->P, *s, h_new);
-  k_t_cd_pair<K, DIM><<<sliced, kTile, 0, st>>>(n, c->P, *s, part);
-  k_t_cd<<<np, 256, 0, st>>>(n, c->P, *s, part, amax);
-  k_t_force_pair<K, DIM><<<sliced, kTile, 0, st>>>(n, c->P, *s, part);
-  k_t_force<DIM><<<np, 256, 0, st>>>(n, c->P, *s, part);
+  tg = t_grid<DIM>(c, s, n, st);  // the later groups: the new h
+  k_t_cd_pair<K, DIM><<<sliced, kTile, 0, st>>>(n, c->P, *s, part, tg);
+  k_t_cd<<<np, 256, 0, st>>>(n, c->P, *s, part, amax, tg.slices);
+  k_t_force_pair<K, DIM><<<sliced, kTile, 0, st>>>(n, c->P, *s, part, tg);
+  k_t_force<DIM><<<np, 256, 0, st>>>(n, c->P, *s, part, tg.slices);
   c->launches += 7;
 }
 
@@ -725,8 +724,7 @@ const char* const kTangentFields[] = {
 
 int check_tangent(Ctx* c, const MhdState* s, int64_t n) {
   if (!s) T_FAIL(MHD_ERR_INVALID, "state is null");
-  if (n < 1 || n > c->n_max || n > MHD_TANGENT_MAX_N)
-    T_FAIL(MHD_ERR_INVALID, "n must be in [1, min(n_max, MHD_TANGENT_MAX_N)]");
+  if (n < 1 || n > c->n_max) T_FAIL(MHD_ERR_INVALID, "n must be in [1, n_max]");
   if (c->P.iterate) T_FAIL(MHD_ERR_INVALID, "the derivative form needs the single density pass (iterate = 0)");
   const double* const* f = reinterpret_cast<const double* const*>(s);
   for (const char* name : kTangentFields) {
@@ -737,9 +735,10 @@ int check_tangent(Ctx* c, const MhdState* s, int64_t n) {
   if (!s->itype) T_FAIL(MHD_ERR_INVALID, "itype is null");
   if (!c->tan_work) {
     // new h (n_max + 1024 records), then the pair kernels' partial sums
-    const size_t nt = (size_t)std::min<int64_t>(c->n_max, MHD_TANGENT_MAX_N);
-    T_CK(cudaMalloc(&c->tan_work, sizeof(TD) * ((size_t)c->n_max + 1024 + (size_t)kTSlices * kTWidth * nt)));
+    T_CK(cudaMalloc(&c->tan_work,
+                    sizeof(TD) * ((size_t)c->n_max + 1024 + derivative_slice_records(c->n_max) * kTWidth)));
   }
+  if (alloc_pair_grid(c->pgrid, c->n_max) != MHD_OK) T_FAIL(MHD_ERR_CUDA, "pair grid allocation failed");
   return MHD_OK;
 }
 

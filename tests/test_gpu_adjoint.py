@@ -120,3 +120,15 @@ def test_hand_written_pair_vjp_equals_dual_jacobian(monkeypatch):
         scale = max(float(torch.linalg.norm(b[f])), 1e-300)
         assert float(torch.linalg.norm(a[f] - b[f])) <= 1e-11 * max(scale, 1e-12 * float(torch.linalg.norm(b))), f
     assert abs(out["0"][1] - out["1"][1]) <= 1e-11 * max(abs(out["1"][1]), 1e-300)
+
+
+def test_adjoint_beyond_small_cases():
+    # 256 x 512 = 131,072 particles: the grid search has no size limit, and
+    # above 65,536 particles the pair passes run as one slice
+    from src.derivative import alfven_case
+
+    ic, seed, prm = alfven_case(_alfven_config(256), 0.1, 1.0)
+    assert len(ic["x"]) == 131072
+    (la, ga), (lt, gt), _ = _both(ic, prm, seed, 4, 2)
+    assert abs(la - lt) <= 1e-12 * abs(lt)
+    assert abs(ga[0] - gt[0]) <= 1e-9 * abs(gt[0]), (ga, gt)
