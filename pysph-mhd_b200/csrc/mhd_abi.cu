@@ -652,6 +652,7 @@ int mhd_ctx_create(const MhdParams* params, int64_t n_max, void** out) {
          dev_alloc(c, &c->cellc, c->n_pad) == MHD_OK;
     ok = ok && dev_alloc(c, &c->nbr_hlim, c->n_pad) == MHD_OK && dev_alloc(c, &c->big_idx, c->n_pad) == MHD_OK &&
          dev_alloc(c, &c->app_idx, c->n_pad) == MHD_OK &&
+         dev_alloc(c, &c->reb_idx, c->n_pad) == MHD_OK &&
          dev_alloc(c, &c->new_of_old, c->n_pad) == MHD_OK && dev_alloc(c, &c->nbr_mark, c->n_pad) == MHD_OK;
     for (Ctx::ListSlot& S : c->slots)
       ok = ok && dev_alloc(c, &S.cnt, c->n_pad) == MHD_OK && dev_alloc(c, &S.gcnt, c->n_pad) == MHD_OK &&
@@ -719,6 +720,7 @@ int mhd_ctx_destroy(void* ctx) {
   for (unsigned* p : c->cell_scr) cudaFree(p);
   cudaFree(c->big_idx);
   cudaFree(c->app_idx);
+  cudaFree(c->reb_idx);
   cudaFree(c->nbr_hlim);
   for (double* p : c->spare) cudaFree(p);
   for (auto& e : c->events) {

@@ -97,6 +97,7 @@ struct DevScalars {
   int events;                       // captured runs: bit 0 = density passes ran out before the group stopped
   int n_big;                        // big particles met by the last list build
   int n_app;                        // particles the last build's scatter pass appended entries to
+  int n_reb;                        // particles whose lists the last build rebuilds (carried builds)
   unsigned long long n_pairs;       // force-pass neighbour pairs (accumulating)
   unsigned long long n_candidates;  // force-pass distance tests (accumulating)
   int n_unconverged[256 + 8];       // per density pass

@@ -118,6 +118,7 @@ struct Ctx {
   int* nbr_gcnt = nullptr;  // entries of the gather pass (the rest were scattered)
   int* big_idx = nullptr;   // big particles of the last build (DevScalars::n_big of them)
   int* app_idx = nullptr;   // particles given scattered entries by the last build (DevScalars::n_app)
+  int* reb_idx = nullptr;   // particles whose lists a carried build rebuilds (DevScalars::n_reb)
   double* nbr_hlim = nullptr;
 
   // Lists persist across sorts in two slots, one per state buffer the caller

@@ -356,10 +356,12 @@ __global__ void __launch_bounds__(128) k_build_lists(int n, DevParams P, const G
                                                      float grow, int cap, int* __restrict__ idx,
                                                      int* __restrict__ cnt_out, int* __restrict__ gcnt_out,
                                                      double* __restrict__ hlim, int* __restrict__ big_idx,
-                                                     const int* __restrict__ mark, DevScalars* sc) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  if (mark && !mark[i]) return;  // list carried over
+                                                     const int* __restrict__ reb_idx, DevScalars* sc) {
+  // a carried build lists the rebuilt particles only (reb_idx, in sorted
+  // order within each warp's share), a full one every particle
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (reb_idx ? sc->n_reb : n)) return;
+  const int i = reb_idx ? reb_idx[t] : t;
   const Grid& G = grid_of(grids, inst, i);
   const float4 pi = posf[i];
   const int ci = cellc[i];
@@ -767,7 +769,8 @@ __global__ void __launch_bounds__(256) k_remap(int n, int cap, const int* __rest
                                                float* __restrict__ md_new, int64_t pad,
                                                const int* __restrict__ idx_old, const int* __restrict__ cnt_old,
                                                int* __restrict__ idx_new, int* __restrict__ cnt_new,
-                                               int* __restrict__ gcnt_new, DevScalars* sc) {
+                                               int* __restrict__ gcnt_new, int* __restrict__ reb_idx,
+                                               DevScalars* sc) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   bool rebuild = false;
   if (k < n) {
@@ -781,6 +784,16 @@ __global__ void __launch_bounds__(256) k_remap(int n, int cap, const int* __rest
     }
     rebuild = dirty || cell_dirty[keys[k]] != 0u;
     mark[k] = rebuild ? 1 : 0;
+  }
+  {
+    // the gather pass runs over the rebuilt particles only: each warp enrols
+    // its rebuilt lanes in lane order with one atomic
+    const unsigned b = __ballot_sync(0xffffffffu, rebuild);
+    const int lane = threadIdx.x & 31;
+    int base = 0;
+    if (lane == 0 && b) base = atomicAdd(&sc->n_reb, __popc(b));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (rebuild) reb_idx[base + __popc(b & ((1u << lane) - 1u))] = k;
   }
   const int nr = __syncthreads_count(rebuild);
   if (threadIdx.x == 0 && nr) atomicAdd(&sc->n_rebuilt, (unsigned long long)nr);
@@ -918,13 +931,13 @@ static void build_lists_dim(Ctx* c, const MhdState* s, int n, cudaStream_t st, c
     unsigned* dirty_dil = dilate_cells(c, flags, md_dil, st);
     k_remap<<<nb256, 256, 0, st>>>(n, c->list_cap, c->perm, c->sorted_keys, c->new_of_old, dirty_dil, c->nbr_mark,
                                    s->x, s->y, s->z, s->h, S.xr, S.hm, S.md, pad, O->idx, O->cnt, S.idx, S.cnt,
-                                   S.gcnt, c->d_sc);
+                                   S.gcnt, c->reb_idx, c->d_sc);
     c->launches += 2;
     mark = c->nbr_mark;
   }
   k_build_lists<DIM><<<nb, 128, 0, st>>>(n, c->P, c->d_grids, c->inst, c->cell_start, s->x, s->y, s->z, s->h,
                                          c->posf, c->cellc, grow, c->list_cap, S.idx, S.cnt, S.gcnt, c->nbr_hlim,
-                                         c->big_idx, mark, c->d_sc);
+                                         c->big_idx, mark ? c->reb_idx : nullptr, c->d_sc);
   k_build_lists_big<DIM><<<big_blocks(c, n), 128, 0, st>>>(c->P, c->d_grids, c->inst, c->cell_start, s->x, s->y,
                                                          s->z, s->h, c->posf, c->cellc, grow, c->list_cap, S.idx,
                                                          S.cnt, S.gcnt, c->nbr_hlim, c->big_idx, c->d_sc);
@@ -951,7 +964,7 @@ void launch_build_lists(Ctx* c, const MhdState* s, int n, cudaStream_t st, const
   c->nbr_idx = S.idx;
   c->nbr_cnt = S.cnt;
   c->nbr_gcnt = S.gcnt;
-  cudaMemsetAsync(&c->d_sc->n_big, 0, 2 * sizeof(int), st);  // n_big and n_app
+  cudaMemsetAsync(&c->d_sc->n_big, 0, 3 * sizeof(int), st);  // n_big, n_app and n_reb
   if (c->P.dim == 3)
     build_lists_dim<3>(c, s, n, st, carry ? &c->slots[od] : nullptr, S);
   else
