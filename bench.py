@@ -610,6 +610,56 @@ def _app_case(name, nx=None, precision=None):
     return ic, prm, cfg
 
 
+def _morton(cx, cy, cz, bits):
+    """Interleaved bits of three cell coordinates (x lowest)."""
+    key = np.zeros(cx.shape, dtype=np.int64)
+    for b in range(bits):
+        key |= ((cx >> b) & 1) << (3 * b)
+        key |= ((cy >> b) & 1) << (3 * b + 1)
+        key |= ((cz >> b) & 1) << (3 * b + 2)
+    return key
+
+
+def cell_order_locality(n: int, seed: int = 0):
+    """How far apart in memory the neighbours of a warp's 32 consecutive
+    particles lie under the linear cell order the sort uses (x fastest, then
+    y, then z) and under a Morton (Z-curve) order of the same cells: per warp,
+    the distinct neighbour records its list entries name (each a record load
+    that L1 can serve to the other lanes) and the distinct 128-byte lines of
+    one 16-byte record plane they touch.  On the blast lattice (n^3, 0.1 %
+    jitter, cubic kernel, h = 1.2 dx, the grid's cells of the list cut-off /
+    2), neighbours by the reach R h (1 + 2 %) of the list build.  CPU only."""
+    from scipy.spatial import cKDTree
+
+    rng = np.random.default_rng(seed)
+    dx = 1.0 / n
+    ax = (np.arange(n) + 0.5) * dx
+    pos = np.stack(np.meshgrid(ax, ax, ax, indexing="ij"), -1).reshape(-1, 3)
+    pos = (pos + 0.001 * dx * rng.uniform(-1, 1, pos.shape)) % 1.0
+    reach = 2.0 * 1.2 * dx * 1.02
+    nc = int(np.floor(1.0 / (reach / 2)))
+    c = np.minimum((pos * nc).astype(np.int64), nc - 1)
+    keys = {"linear": (c[:, 2] * nc + c[:, 1]) * nc + c[:, 0],
+            "morton": _morton(c[:, 0], c[:, 1], c[:, 2], int(np.ceil(np.log2(nc))))}
+    pairs = cKDTree(pos, boxsize=1.0).query_pairs(reach, output_type="ndarray")
+    i = np.concatenate([pairs[:, 0], pairs[:, 1], np.arange(len(pos))])
+    j = np.concatenate([pairs[:, 1], pairs[:, 0], np.arange(len(pos))])
+    out = {"workload": f"blast lattice {n}^3 = {len(pos)} particles, {nc}^3 cells, "
+                       f"{len(i) / len(pos):.1f} neighbours per particle (self included)"}
+    for name, key in keys.items():
+        order = np.argsort(key, kind="stable")
+        rank = np.empty_like(order)
+        rank[order] = np.arange(len(order))
+        wi, wj = rank[i] // 32, rank[j]  # warp of i, new index of j
+        recs = np.unique(wi * len(pos) + wj)
+        lines = np.unique(wi * len(pos) + wj // 8)
+        warps = (len(pos) + 31) // 32
+        out[name] = {"records_per_warp": len(recs) / warps, "lines_per_warp": len(lines) / warps,
+                     "list_entries_per_warp": len(i) / warps,
+                     "mean_abs_index_distance": float(np.mean(np.abs(rank[i] - rank[j])))}
+    return out
+
+
 def run_workload(args):
     """The other measured configurations, one JSON line each:
     ot128  -- 2-D Orszag-Tang 128^2, quintic, 50 steps: FP64 on the GPU and the
@@ -938,13 +988,17 @@ def main():
     ap.add_argument("--batch-steps", type=int, default=100)
     ap.add_argument("--batch-loop-steps", type=int, default=10, help="steps per instance of the FP64 loop")
     ap.add_argument("--derivative-steps", type=int, default=200, help="derivative form steps (0 skips it)")
-    ap.add_argument("--workload", default="blast", choices=("blast", "ot128", "briowu"),
-                    help="blast: the benchmark line; ot128 / briowu: the other measured configurations")
+    ap.add_argument("--workload", default="blast", choices=("blast", "ot128", "briowu", "cell_order"),
+                    help="blast: the benchmark line; ot128 / briowu: the other measured configurations; "
+                         "cell_order: memory locality of neighbour gathers, linear vs Morton cell order (CPU)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
-    if args.workload != "blast":
+    if args.workload == "cell_order":
+        if rank == 0:
+            print(json.dumps(cell_order_locality(args.n if args.n != 128 else 64)))
+    elif args.workload != "blast":
         if rank == 0:
             run_workload(args)
     elif args.impl == "reference":
