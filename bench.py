@@ -325,8 +325,11 @@ def _batched(args, dev, rank=0, world=1):
     (src.parallel.shard_instances); each rank runs its share in FP32, the
     value is all particle-steps over the slowest rank's time, and the ranks'
     per-instance checksums are gathered."""
+    import ctypes
+
     import torch
 
+    from src import _abi
     from src.parallel import checksum, gather_instances, max_over_ranks, shard_instances
 
     from src.batch import BatchEngine
@@ -369,6 +372,22 @@ def _batched(args, dev, rank=0, world=1):
         if world > 1:
             sums = gather_instances({k: checksum(eng.pull_instance(i, "rho", "u", "v", "Bx", "By"))
                                      for i, k in enumerate(share)}, n_all)
+        # where the captured run's time goes: the same kernels run uncaptured
+        # for a few steps with CUDA events around each family (the density
+        # iteration host-checked there, so its passes are the needed ones)
+        lib = _abi.load()
+        ms_k = (ctypes.c_double * len(_abi.TIMING_KINDS))()
+        cnt_k = (ctypes.c_int64 * len(_abi.TIMING_KINDS))()
+        lib.mhd_timing_enable(eng.ctx, 1)
+        lib.mhd_timing_read(eng.ctx, ms_k, cnt_k)
+        k_unc = 5
+        eng.restore(snap)
+        eng.advance(k_unc, finish=False, capture=False)
+        lib.mhd_timing_read(eng.ctx, ms_k, cnt_k)
+        lib.mhd_timing_enable(eng.ctx, 0)
+        out[prec]["kernels_ms_per_step"] = {k: ms_k[i] / k_unc for i, k in enumerate(_abi.TIMING_KINDS)}
+        out[prec]["captured_ms_per_step"] = ms / steps
+        out[prec]["launches_per_step"] = out[prec]["gpu_launches"] / steps
         eng.close()
     if world > 1:
         return {"workload": f"{n_all} x 2-D Orszag-Tang (seed 0), {total} particles, {steps} steps, instances "
