@@ -278,12 +278,13 @@ int mhd_clock_get_all(void* ctx, double* t, double* dt, void* stream);
    and list rebuilds of mhd_rhs.  capture = 1 (after mhd_ctx_set_instances)
    captures the steps once into a CUDA graph -- cached per buffers, step
    count and context configuration -- and launches them as one graph: each
-   density iteration runs min(max_iter, 8) passes with the on-device stop
-   test, and nothing synchronises until the run ends.  A captured run whose
-   lists stopped covering an h (or overflowed), or whose density iteration
-   had not stopped after its captured passes, returns MHD_ERR_RELIST: its
-   state is invalid; restore the input state and clocks and replay the run
-   with capture = 0. */
+   density iteration runs its first min_iter passes, then a conditional
+   while node repeats one pass until the group stops (the on-device stop
+   test) or 256 passes ran, and nothing synchronises until the run ends.  A
+   captured run whose lists stopped covering an h (or overflowed), or whose
+   density iteration had not stopped after its captured passes, returns
+   MHD_ERR_RELIST: its state is invalid; restore the input state and clocks
+   and replay the run with capture = 0. */
 int mhd_advance(void* ctx, MhdState* a, MhdState* b, int64_t n, int32_t steps, int32_t finish, int32_t capture,
                 void* stream);
 

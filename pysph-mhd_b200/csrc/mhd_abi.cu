@@ -493,11 +493,55 @@ int read_status(Ctx* c, cudaStream_t st) {
   return MHD_OK;
 }
 
+// The rest of a captured density iteration as a conditional while node:
+// an arming kernel sets the loop's condition after passes [0, first), and
+// the body -- one density pass whose index and h buffers come from the
+// device, then the control kernel that advances the index and sets the
+// condition again -- repeats until the group stops, a list needs
+// rebuilding, or the passes reach min(max_iter, kDensityLoopCap).  The
+// index rises by one per iteration, so the loop ends after at most
+// kDensityLoopCap - first iterations whatever the particles do.
+int capture_density_loop(Ctx* c, MhdState* dst, int n, int first, cudaStream_t st) {
+  cudaStreamCaptureStatus status;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  CK(cudaStreamGetCaptureInfo(st, &status, nullptr, &g, &deps, &nd));
+  if (status != cudaStreamCaptureStatusActive) FAIL(MHD_ERR_INVALID, "the density loop needs an active capture");
+  cudaGraphConditionalHandle h;
+  CK(cudaGraphConditionalHandleCreate(&h, g, 0, 0));
+  launch_density_loop_control(c, h, first, st);
+  CK(cudaStreamGetCaptureInfo(st, &status, nullptr, &g, &deps, &nd));
+  cudaGraphNodeParams np = {cudaGraphNodeTypeConditional};
+  np.conditional.handle = h;
+  np.conditional.type = cudaGraphCondTypeWhile;
+  np.conditional.size = 1;
+  cudaGraphNode_t node;
+  CK(cudaGraphAddNode(&node, g, deps, nd, &np));
+  cudaGraph_t body = np.conditional.phGraph_out[0];
+  if (!c->cap_stream2) CK(cudaStreamCreateWithFlags(&c->cap_stream2, cudaStreamNonBlocking));
+  CK(cudaStreamBeginCaptureToGraph(c->cap_stream2, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  launch_density_pass(c, dst, n, -1, dst->h, c->h_alt, c->cap_stream2);
+  launch_density_loop_control(c, h, -1, c->cap_stream2);
+  // the body's launches are counted when they run (DevScalars::loop_iters)
+  c->launches -= 2;
+  cudaGraph_t captured = nullptr;
+  const cudaError_t le = cudaGetLastError();
+  const cudaError_t ee = cudaStreamEndCapture(c->cap_stream2, &captured);
+  if (le != cudaSuccess || ee != cudaSuccess)
+    FAIL(MHD_ERR_CUDA, std::string("density loop body capture failed: ") +
+                           cudaGetErrorString(le != cudaSuccess ? le : ee));
+  CK(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+  return MHD_OK;
+}
+
 // Right-hand side with nothing that synchronises (batched contexts): device
-// planning, sort and lists, a fixed number of density passes with their
-// on-device stop test, the force pass.  Lists that stop covering an h, or a
-// group that has not stopped after the captured passes, raise relist or an
-// event that the caller reads after the run.
+// planning, sort and lists, the density iteration with its on-device stop
+// test (its first min_iter passes as plain launches, the rest as a
+// conditional while node; with MHD_GRAPH_LOOP=0 or diagnostic outputs, a
+// fixed number of passes), the force pass.  Lists that stop covering an h,
+// or a group that has not stopped after the captured passes, raise relist
+// or an event that the caller reads after the run.
 int rhs_captured(Ctx* c, const MhdState* src, MhdState* dst, int n, cudaStream_t st) {
   int rc = plan_grid(c, src, n, st);
   if (rc != MHD_OK) return rc;
@@ -506,9 +550,19 @@ int rhs_captured(Ctx* c, const MhdState* src, MhdState* dst, int n, cudaStream_t
   CK(cudaMemsetAsync(&c->d_sc->n_unconverged[0], 0, sizeof(c->d_sc->n_unconverged), st));
   CK(cudaMemsetAsync(&c->d_sc->passes_done, 0, sizeof(int), st));
   double* buf[2] = {dst->h, c->h_alt};
-  const int passes = std::min(c->P.max_iter, c->graph_passes);
-  for (int k = 0; k < passes; k++) launch_density_pass(c, dst, n, k, buf[k & 1], buf[(k + 1) & 1], st);
-  launch_finish_density(c, dst, n, passes, st);
+  const bool diag = dst->arho || dst->grhox || dst->grhoy || dst->grhoz || dst->dwdh;
+  const int cap = std::min(c->P.max_iter, kDensityLoopCap);
+  const int first = std::min(cap, std::max(c->P.min_iter, 1));
+  if (c->graph_loop && !diag && c->P.iterate && cap > first) {
+    for (int k = 0; k < first; k++) launch_density_pass(c, dst, n, k, buf[k & 1], buf[(k + 1) & 1], st);
+    rc = capture_density_loop(c, dst, n, first, st);
+    if (rc != MHD_OK) return rc;
+    launch_finish_density(c, dst, n, cap, st);
+  } else {
+    const int passes = std::min(c->P.max_iter, c->graph_passes);
+    for (int k = 0; k < passes; k++) launch_density_pass(c, dst, n, k, buf[k & 1], buf[(k + 1) & 1], st);
+    launch_finish_density(c, dst, n, passes, st);
+  }
   launch_force_prologue(c, dst, n, st);
   launch_force_pass(c, dst, n, st);
   CK(cudaGetLastError());
@@ -680,6 +734,7 @@ int mhd_ctx_create(const MhdParams* params, int64_t n_max, void** out) {
   if (const char* m = getenv("MHD_FORCE_SHAPE")) c->force_shape = std::max(0, std::min(3, atoi(m)));
   if (const char* m = getenv("MHD_STENCIL")) c->stencil = std::max(1, std::min(3, atoi(m)));
   if (const char* m = getenv("MHD_GRAPH_PASSES")) c->graph_passes = std::max(1, std::min(256, atoi(m)));
+  if (const char* m = getenv("MHD_GRAPH_LOOP")) c->graph_loop = atoi(m) != 0;
   if (const char* m = getenv("MHD_CELL_KAPPA")) c->cell_kappa = std::max(1.0, atof(m));
   if (const char* m = getenv("MHD_LIST_MARGIN")) c->list_margin = std::max(0.005, std::min(0.5, atof(m)));
   if (const char* m = getenv("MHD_LIST_REUSE")) c->list_reuse = atoi(m) != 0;
@@ -737,6 +792,7 @@ int mhd_ctx_destroy(void* ctx) {
   cudaFree(c->d_stage);
   drop_graphs(c);
   if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
+  if (c->cap_stream2) cudaStreamDestroy(c->cap_stream2);
   cudaFree(c->tan_work);
   cudaFree(c->adj_buf);
   free_pair_grid(c->pgrid);
@@ -1135,10 +1191,12 @@ int mhd_advance(void* ctx, MhdState* a, MhdState* b, int64_t n, int32_t steps, i
     c->graphs.push_back(e);
     hit = &c->graphs.back();
   }
+  const unsigned long long iters0 = c->h_sc->loop_iters;
   CK(cudaGraphLaunch(hit->exec, st));
   c->launches += hit->launches;
   CK(cudaMemcpyAsync(c->h_sc, c->d_sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
+  c->launches += 2 * (int64_t)(c->h_sc->loop_iters - iters0);
   const int rc = read_status(c, st);
   if (rc != MHD_OK) return rc;
   if (c->h_sc->relist || c->h_sc->events) {

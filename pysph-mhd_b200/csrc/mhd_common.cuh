@@ -93,6 +93,8 @@ struct DevScalars {
   int relist;       // an h outgrew its neighbour list, or a list overflowed
   int list_max;     // longest neighbour list met by the last build
   int passes_done;  // density passes executed in the current group evaluation
+  int loop_pass;    // captured runs: the pass the density loop's body runs next
+  unsigned long long loop_iters;  // density-loop body iterations run (accumulating; each runs 2 kernels)
   unsigned int ticket;              // last-block counter of the dt reduction
   int events;                       // captured runs: bit 0 = density passes ran out before the group stopped
   int n_big;                        // big particles met by the last list build

@@ -50,6 +50,8 @@ struct Ctx {
   int64_t generation = 0;         // bumped when a buffer captured by a graph is reallocated
   int graph_passes = 8;           // density passes captured per right-hand side
   cudaStream_t cap_stream = nullptr;
+  cudaStream_t cap_stream2 = nullptr;  // captures the density loop's body graph
+  bool graph_loop = true;  // captured density iteration as a conditional while node (MHD_GRAPH_LOOP=0: fixed passes)
   void* tan_work = nullptr;  // derivative form: new h / energy partials (dual records)
   PairGridBufs pgrid;        // derivative forms: the cell grid of their pair passes
   void* adj_buf = nullptr;   // adjoint: states, tapes, reverse workspace (doubles)
@@ -216,6 +218,12 @@ void launch_pair_stats(Ctx* c, const MhdState* s, int n, cudaStream_t st);
 // density pass `pass` (0-based) reading h_in, writing h_out
 void launch_density_pass(Ctx* c, MhdState* s, int n, int pass, const double* h_in, double* h_out, cudaStream_t st);
 void launch_finish_density(Ctx* c, MhdState* s, int n, int passes, cudaStream_t st);
+// The captured density loop's control (one thread): with first >= 0 it arms
+// the loop (the next pass is `first`), otherwise it advances it; then it
+// sets the loop condition: the group has not stopped, no list needs
+// rebuilding, and the next pass is below min(max_iter, kDensityLoopCap).
+constexpr int kDensityLoopCap = 256;
+void launch_density_loop_control(Ctx* c, cudaGraphConditionalHandle h, int first, cudaStream_t st);
 // Raises the dynamic shared-memory limit of the staged force passes for the
 // context's kernel, dimension and precision (set-up only).
 cudaError_t configure_force_pass(Ctx* c);

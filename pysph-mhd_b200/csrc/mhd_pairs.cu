@@ -157,6 +157,16 @@ __global__ void __launch_bounds__(128) k_density_pass(int n, int pass, DevParams
                                                       double* __restrict__ omega, double* __restrict__ converged,
                                                       const Grid* __restrict__ grids, const int* __restrict__ inst,
                                                       const uint4* __restrict__ posq, DevScalars* sc) {
+  // pass < 0: the body of the captured density loop -- the pass index comes
+  // from the device, and the h buffers alternate with its parity
+  if (pass < 0) {
+    pass = sc->loop_pass;
+    if (pass & 1) {
+      double* a = const_cast<double*>(h_in);
+      h_in = h_out;
+      h_out = a;
+    }
+  }
   // Stop when the iterated group already stopped after pass `pass` (1-based
   // count), or when the neighbour lists no longer cover the current h.
   if (sc->relist) return;
@@ -1036,6 +1046,24 @@ __global__ void __launch_bounds__(256) k_finish_density(int n, DevParams P, int 
     if (!stopped && done >= passes) atomicOr(&sc->events, 1);
   }
   if (i < n && (done & 1)) h[i] = h_alt[i];
+}
+
+__global__ void __launch_bounds__(32) k_density_loop_control(DevParams P, DevScalars* sc,
+                                                              cudaGraphConditionalHandle h, int first) {
+  if (threadIdx.x != 0) return;
+  const int next = first >= 0 ? first : sc->loop_pass + 1;
+  sc->loop_pass = next;
+  if (first < 0) sc->loop_iters++;
+  const int done = sc->passes_done;
+  const bool stopped = done >= P.max_iter || !P.iterate ||
+                       (done >= P.min_iter && done > 0 && sc->n_unconverged[done - 1] == 0);
+  const int cap = P.max_iter < kDensityLoopCap ? P.max_iter : kDensityLoopCap;
+  cudaGraphSetConditional(h, (!stopped && !sc->relist && next < cap) ? 1u : 0u);
+}
+
+void launch_density_loop_control(Ctx* c, cudaGraphConditionalHandle h, int first, cudaStream_t st) {
+  k_density_loop_control<<<1, 32, 0, st>>>(c->P, c->d_sc, h, first);
+  c->launches++;
 }
 
 void launch_finish_density(Ctx* c, MhdState* s, int n, int passes, cudaStream_t st) {

@@ -100,8 +100,10 @@ def test_graph_is_reused_and_runs_continue():
 
 
 def test_unfinished_captured_iteration_replays(monkeypatch):
-    # One captured density pass cannot satisfy min_iter = 2: every captured
+    # With the density iteration captured as fixed launches (no conditional
+    # loop), one captured pass cannot satisfy min_iter = 2: every captured
     # run raises the event and is replayed uncaptured from its snapshot.
+    monkeypatch.setenv("MHD_GRAPH_LOOP", "0")
     monkeypatch.setenv("MHD_GRAPH_PASSES", "1")
     ics, prm = _instances(sizes=(12, 15), seed=7)
     a = _batch(ics, prm, "fp64", 3, capture=True)
@@ -178,3 +180,30 @@ def test_instance_declaration_is_validated():
     assert rc == -1 and "set_instances" in e2.lib.mhd_last_error(e2.ctx).decode()
     assert _abi.ERRORS[-7] == "MHD_ERR_RELIST"
     e2.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_captured_density_loop_equals_fixed_passes(precision, monkeypatch):
+    # A captured run iterates the density group past its first min_iter
+    # passes in a conditional while node (MHD_GRAPH_LOOP=1, the default) or
+    # as a fixed number of launches that return at once after the group
+    # stopped (MHD_GRAPH_LOOP=0): the same passes run, so the results agree
+    # bit for bit, and the loop needs fewer launches per step.  With only
+    # two fixed passes captured the fixed form must replay any step that
+    # needs a third one uncaptured; the loop runs it inside the graph.
+    ics, prm = _instances(sizes=(14, 19), scales=(1.0, 1.1), seed=11)
+    out, launches, replays = {}, {}, {}
+    for loop, passes in (("1", "2"), ("0", "8"), ("0", "2")):
+        monkeypatch.setenv("MHD_GRAPH_LOOP", loop)
+        monkeypatch.setenv("MHD_GRAPH_PASSES", passes)
+        eng = _batch(ics, prm, precision, 6)
+        key = loop + passes
+        out[key] = eng.pa.pull(*FIELDS, "gid", order="gid")
+        launches[key] = eng.launches()
+        replays[key] = eng.replays
+        eng.close()
+    for k in FIELDS:
+        np.testing.assert_array_equal(out["12"][k], out["08"][k], err_msg=k)
+        np.testing.assert_array_equal(out["12"][k], out["02"][k], err_msg=k)
+    assert replays["12"] == 0
+    assert launches["12"] < launches["08"]
