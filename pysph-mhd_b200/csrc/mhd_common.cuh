@@ -611,4 +611,169 @@ __device__ __forceinline__ void for_each_row_trimmed(const Grid& G, int sw, cons
   }
 }
 
+// The rows of for_each_row_trimmed's walk, restated one row at a time so
+// that a warp can take one row per lane (warp_rows): rows yu in
+// [ylo, yhi] (and zu in [zlo, zhi] in 3-D), each over the unwrapped x-range
+// [xl0, xh0], trimmed per row when xtrim.
+struct RowPlan {
+  int ylo, yhi, zlo, zhi, xl0, xh0;
+  bool xtrim, ys, zs;
+  double cut2;
+};
+
+template <int DIM>
+__device__ __forceinline__ RowPlan row_plan(const Grid& G, int sw, double xi, double yi, double zi, double cut) {
+  RowPlan R;
+  const int whole = 2 * sw + 1;
+  const int nx = G.nc[0], ny = G.nc[1], nz = G.nc[2];
+  const int cy = cell_coord(G, 1, yi);
+  const int cz = DIM == 3 ? cell_coord(G, 2, zi) : 0;
+  R.xtrim = false;
+  if (nx < whole) {
+    R.xl0 = 0;
+    R.xh0 = nx - 1;
+  } else {
+    R.xl0 = (int)floor((xi - cut - G.lo[0]) * G.inv_cs[0]);
+    R.xh0 = (int)floor((xi + cut - G.lo[0]) * G.inv_cs[0]);
+    if (!G.periodic[0]) {
+      R.xl0 = R.xl0 < 0 ? 0 : R.xl0;
+      R.xh0 = R.xh0 >= nx ? nx - 1 : R.xh0;
+    }
+    if (R.xh0 - R.xl0 >= nx) R.xh0 = R.xl0 + nx - 1;
+    else R.xtrim = true;
+  }
+  R.cut2 = cut * cut;
+  R.zs = DIM == 3 && nz >= whole;
+  R.ys = ny >= whole;
+  R.zlo = DIM == 3 ? (R.zs ? cz - sw : 0) : 0;
+  R.zhi = DIM == 3 ? (R.zs ? cz + sw : nz - 1) : 0;
+  R.ylo = R.ys ? cy - sw : 0;
+  R.yhi = R.ys ? cy + sw : ny - 1;
+  return R;
+}
+
+// The pieces of row (yu, zu): [jb[p], je[p]) holds the particles of its
+// cells below 0 (p = 0, x offset -nx), inside the grid (p = 1, offset 0) and
+// above nx - 1 (p = 2, offset +nx); an absent piece is empty.  The cells and
+// their order are for_each_row_trimmed's.
+template <int DIM>
+__device__ __forceinline__ void row_pieces(const Grid& G, const RowPlan& R, const int* __restrict__ cell_start,
+                                           double xi, double yi, double zi, int yu, int zu, int (&jb)[3],
+                                           int (&je)[3]) {
+  jb[0] = je[0] = jb[1] = je[1] = jb[2] = je[2] = 0;
+  const int nx = G.nc[0], ny = G.nc[1], nz = G.nc[2];
+  int zc = zu;
+  double dzm = 0.0;
+  if (R.zs) {
+    const double c_lo = G.lo[2] + zu * G.cs[2], c_hi = c_lo + G.cs[2];
+    dzm = zi < c_lo ? c_lo - zi : (zi > c_hi ? zi - c_hi : 0.0);
+    if (dzm * dzm >= R.cut2) return;
+    if (zc < 0 || zc >= nz) {
+      if (!G.periodic[2]) return;
+      zc = zc < 0 ? zc + nz : zc - nz;
+    }
+  }
+  int yc = yu;
+  double dym = 0.0;
+  if (R.ys) {
+    const double c_lo = G.lo[1] + yu * G.cs[1], c_hi = c_lo + G.cs[1];
+    dym = yi < c_lo ? c_lo - yi : (yi > c_hi ? yi - c_hi : 0.0);
+    if (dym * dym + dzm * dzm >= R.cut2) return;
+    if (yc < 0 || yc >= ny) {
+      if (!G.periodic[1]) return;
+      yc = yc < 0 ? yc + ny : yc - ny;
+    }
+  }
+  const int base = G.cell_base + (zc * ny + yc) * nx;
+  int xl = R.xl0, xh = R.xh0;
+  if (R.xtrim) {
+    const double wx = sqrt(R.cut2 - (dym * dym + dzm * dzm));
+    const int a = (int)floor((xi - wx - G.lo[0]) * G.inv_cs[0]);
+    const int b = (int)floor((xi + wx - G.lo[0]) * G.inv_cs[0]);
+    xl = a > xl ? a : xl;
+    xh = b < xh ? b : xh;
+    if (xl > xh) return;
+  }
+  if (xl < 0) {
+    const int a = xl + nx, b = (xh < 0 ? xh : -1) + nx;
+    jb[0] = cell_start[base + a];
+    je[0] = cell_start[base + b + 1];
+  }
+  if (xh >= 0 && xl < nx) {
+    const int a = xl < 0 ? 0 : xl, b = xh >= nx ? nx - 1 : xh;
+    jb[1] = cell_start[base + a];
+    je[1] = cell_start[base + b + 1];
+  }
+  if (xh >= nx) {
+    const int a = (xl >= nx ? xl : nx) - nx, b = xh - nx;
+    jb[2] = cell_start[base + a];
+    je[2] = cell_start[base + b + 1];
+  }
+}
+
+// for_each_row_trimmed's walk for a whole warp searching from one point:
+// the lanes look up 32 rows' pieces side by side (one row each, instead of
+// every row in turn), a warp prefix sum lays the rows' particles end to
+// end, and f(j, yu, zu, xoff) is called by every lane for 32 consecutive
+// candidates at a time, in for_each_row_trimmed's order (j < 0 past the
+// end; yu, zu the candidate's row and xoff its piece's offset, as
+// for_each_row_trimmed passes them).  Must be called by all 32 lanes with
+// the same arguments; f may use warp-wide operations.
+template <int DIM, class F>
+__device__ __forceinline__ void warp_rows(const Grid& G, int sw, const int* __restrict__ cell_start, double xi,
+                                          double yi, double zi, double cut, F&& f) {
+  constexpr unsigned kFull = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const RowPlan R = row_plan<DIM>(G, sw, xi, yi, zi, cut);
+  const int nyr = R.yhi - R.ylo + 1, nrows = nyr * (R.zhi - R.zlo + 1);
+  const int nx = G.nc[0];
+  for (int r0 = 0; r0 < nrows; r0 += 32) {
+    const int r = r0 + lane;
+    int jb[3] = {0, 0, 0}, je[3] = {0, 0, 0}, yu = 0, zu = 0;
+    if (r < nrows) {
+      zu = R.zlo + r / nyr;
+      yu = R.ylo + r % nyr;
+      row_pieces<DIM>(G, R, cell_start, xi, yi, zi, yu, zu, jb, je);
+    }
+    const int l0 = je[0] - jb[0], l1 = je[1] - jb[1], m = l0 + l1 + (je[2] - jb[2]);
+    int incl = m;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const int v = __shfl_up_sync(kFull, incl, off);
+      if (lane >= off) incl += v;
+    }
+    const int excl = incl - m;
+    const int total = __shfl_sync(kFull, incl, 31);
+    for (int c0 = 0; c0 < total; c0 += 32) {
+      const int c = c0 + lane;
+      // the row lane owning candidate c: the last lane whose range starts at
+      // or before c (a lane with no candidates never is)
+      int L = 0;
+#pragma unroll
+      for (int step = 16; step > 0; step >>= 1) {
+        const int e = __shfl_sync(kFull, excl, L + step);
+        if (e <= c) L += step;
+      }
+      const int k = c - __shfl_sync(kFull, excl, L);
+      const int a0 = __shfl_sync(kFull, l0, L), a1 = __shfl_sync(kFull, l1, L);
+      const int b0 = __shfl_sync(kFull, jb[0], L), b1 = __shfl_sync(kFull, jb[1], L),
+                b2 = __shfl_sync(kFull, jb[2], L);
+      const int yr = __shfl_sync(kFull, yu, L), zr = __shfl_sync(kFull, zu, L);
+      int j = -1, xoff = 0;
+      if (c < total) {
+        if (k < a0) {
+          j = b0 + k;
+          xoff = -nx;
+        } else if (k < a0 + a1) {
+          j = b1 + (k - a0);
+        } else {
+          j = b2 + (k - a0 - a1);
+          xoff = nx;
+        }
+      }
+      f(j, yr, zr, xoff);
+    }
+  }
+}
+
 }  // namespace mhd

@@ -469,32 +469,31 @@ __global__ void __launch_bounds__(128) k_scatter_big(DevParams P, const Grid* __
     int sw;
     double cut;
     search_extent(G, DIM, Rg, pj.w, true, sw, cut);
-    for_each_row_trimmed<DIM>(G, sw, cell_start, x[j], y[j], DIM == 3 ? z[j] : 0.0, cut,
-                              [&](int, int, int ib, int ie, int) {
-      for (int i = ib + lane; i < ie; i += 32) {
-        if (i == j) continue;
-        const float4 pi = __ldg(posf + i);
-        const float r2 = sym_r2<DIM>(G, pi, __ldg(cellc + i), pj, cj);
-        if (!(r2 < reach_j)) continue;
-        if (pi.w > hbig && r2 < reach2(Rg, pi.w, slack)) continue;  // i kept j itself
-        int* __restrict__ irow = idx + (size_t)(i >> 5) * cap * 32 + (i & 31);
-        if (mark && !mark[i]) {
-          // a carried-over list may hold j already (its appended entries
-          // of this build start after gcnt)
-          const int g = gcnt[i];
-          bool held = false;
-          for (int e = 0; e < g && !held; e++) held = irow[(size_t)e * 32] == j;
-          if (held) continue;
-        }
-        const int slot = atomicAdd(cnt + i, 1);
-        // the first entry appended to i's list enrols i for the ordering pass
-        if (slot == __ldg(gcnt + i)) app_idx[atomicAdd(&sc->n_app, 1)] = i;
-        if (slot < cap) {
-          irow[(size_t)slot * 32] = j;
-        } else {
-          atomicMax(&sc->list_max, slot + 1);
-          atomicExch(&sc->relist, 1);
-        }
+    // the extended stencil's rows looked up 32 at a time, candidates 32 at
+    // a time (the appends land in atomic order; the ordering pass sorts them)
+    warp_rows<DIM>(G, sw, cell_start, x[j], y[j], DIM == 3 ? z[j] : 0.0, cut, [&](int i, int, int, int) {
+      if (i < 0 || i == j) return;
+      const float4 pi = __ldg(posf + i);
+      const float r2 = sym_r2<DIM>(G, pi, __ldg(cellc + i), pj, cj);
+      if (!(r2 < reach_j)) return;
+      if (pi.w > hbig && r2 < reach2(Rg, pi.w, slack)) return;  // i kept j itself
+      int* __restrict__ irow = idx + (size_t)(i >> 5) * cap * 32 + (i & 31);
+      if (mark && !mark[i]) {
+        // a carried-over list may hold j already (its appended entries of
+        // this build start after gcnt)
+        const int g = gcnt[i];
+        bool held = false;
+        for (int e = 0; e < g && !held; e++) held = irow[(size_t)e * 32] == j;
+        if (held) return;
+      }
+      const int slot = atomicAdd(cnt + i, 1);
+      // the first entry appended to i's list enrols i for the ordering pass
+      if (slot == __ldg(gcnt + i)) app_idx[atomicAdd(&sc->n_app, 1)] = i;
+      if (slot < cap) {
+        irow[(size_t)slot * 32] = j;
+      } else {
+        atomicMax(&sc->list_max, slot + 1);
+        atomicExch(&sc->relist, 1);
       }
     });
   }
@@ -539,37 +538,35 @@ __global__ void __launch_bounds__(128) k_build_lists_big(DevParams P, const Grid
     const float csx = G.csf[0], csy = G.csf[1], csz = G.csf[2];
     int* __restrict__ row = idx + (size_t)(i >> 5) * cap * 32 + (i & 31);
     int cnt = 0;
-    for_each_row_trimmed<DIM>(G, sw, cell_start, x[i], y[i], DIM == 3 ? z[i] : 0.0, cut,
-                              [&](int cyu, int czu, int jb, int je, int xoff) {
-      const float sy = pi.y + (float)(cyi - cyu) * csy;
-      const float sz = DIM == 3 ? pi.z + (float)(czi - czu) * csz : 0.f;
-      const int cxo = cxi - xoff;
-      for (int t0 = jb; t0 < je; t0 += 32) {
-        const int j = t0 + lane;
-        bool keep = false;
-        if (j < je) {
-          const float4 pj = __ldg(posf + j);
-          const int cjj = __ldg(cellc + j);
-          if (pj.w > hbig) {
-            keep = sym_r2<DIM>(G, pi, ci, pj, cjj) < own2;
-          } else {
-            const float sx = pi.x + (float)(cxo - (cjj & xmask)) * csx;
-            float dx = sx - pj.x, dy = sy - pj.y, dz = DIM == 3 ? sz - pj.z : 0.f;
-            if (mx) dx = dx > 0.5f * Lx ? dx - Lx : (dx < -0.5f * Lx ? dx + Lx : dx);
-            if (my) dy = dy > 0.5f * Ly ? dy - Ly : (dy < -0.5f * Ly ? dy + Ly : dy);
-            if (mz) dz = dz > 0.5f * Lz ? dz - Lz : (dz < -0.5f * Lz ? dz + Lz : dz);
-            const float r2 = dx * dx + dy * dy + dz * dz;
-            const float rhj = Rg * pj.w;
-            keep = r2 < fmaxf(rhi2, rhj * rhj) * slack;
-          }
+    // the extended stencil's rows looked up 32 at a time (a big particle's
+    // search has up to (2 sw + 1)^2 rows), candidates 32 at a time
+    warp_rows<DIM>(G, sw, cell_start, x[i], y[i], DIM == 3 ? z[i] : 0.0, cut, [&](int j, int cyu, int czu, int xoff) {
+      bool keep = false;
+      if (j >= 0) {
+        const float4 pj = __ldg(posf + j);
+        const int cjj = __ldg(cellc + j);
+        if (pj.w > hbig) {
+          keep = sym_r2<DIM>(G, pi, ci, pj, cjj) < own2;
+        } else {
+          const float sy = pi.y + (float)(cyi - cyu) * csy;
+          const float sz = DIM == 3 ? pi.z + (float)(czi - czu) * csz : 0.f;
+          const int cxo = cxi - xoff;
+          const float sx = pi.x + (float)(cxo - (cjj & xmask)) * csx;
+          float dx = sx - pj.x, dy = sy - pj.y, dz = DIM == 3 ? sz - pj.z : 0.f;
+          if (mx) dx = dx > 0.5f * Lx ? dx - Lx : (dx < -0.5f * Lx ? dx + Lx : dx);
+          if (my) dy = dy > 0.5f * Ly ? dy - Ly : (dy < -0.5f * Ly ? dy + Ly : dy);
+          if (mz) dz = dz > 0.5f * Lz ? dz - Lz : (dz < -0.5f * Lz ? dz + Lz : dz);
+          const float r2 = dx * dx + dy * dy + dz * dz;
+          const float rhj = Rg * pj.w;
+          keep = r2 < fmaxf(rhi2, rhj * rhj) * slack;
         }
-        const unsigned bal = __ballot_sync(0xffffffffu, keep);
-        if (keep) {
-          const int pos = cnt + __popc(bal & ((1u << lane) - 1u));
-          if (pos < cap) row[pos * 32] = j;
-        }
-        cnt += __popc(bal);
       }
+      const unsigned bal = __ballot_sync(0xffffffffu, keep);
+      if (keep) {
+        const int pos = cnt + __popc(bal & ((1u << lane) - 1u));
+        if (pos < cap) row[pos * 32] = j;
+      }
+      cnt += __popc(bal);
     });
     if (lane == 0) {
       const int stored = cnt < cap ? cnt : cap;
