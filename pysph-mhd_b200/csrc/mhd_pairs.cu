@@ -357,8 +357,12 @@ __device__ __forceinline__ void search_extent(const Grid& G, int dim, float Rg, 
 // position is shifted by the cell offset, so a candidate costs one float4
 // load.  Counts beyond `cap` are recorded, not stored, and flag a rebuild
 // with a larger capacity.
+constexpr int kGatherUnroll = 4;
+// (a carried build runs this over a few percent of the particles: few blocks
+// have work, so the registers the unrolled loads take cost no occupancy that
+// matters)
 template <int DIM>
-__global__ void __launch_bounds__(128) k_build_lists(int n, DevParams P, const Grid* __restrict__ grids,
+__global__ void __launch_bounds__(128, 2) k_build_lists(int n, DevParams P, const Grid* __restrict__ grids,
                                                      const int* __restrict__ inst, const int* __restrict__ cell_start,
                                                      const double* __restrict__ x, const double* __restrict__ y,
                                                      const double* __restrict__ z, const double* __restrict__ h,
@@ -406,14 +410,13 @@ __global__ void __launch_bounds__(128) k_build_lists(int n, DevParams P, const G
     const float sy = pi.y + (float)(cyi - cyu) * csy;
     const float sz = DIM == 3 ? pi.z + (float)(czi - czu) * csz : 0.f;
     const int cxo = cxi - xoff;
-    for (int j = jb; j < je; j++) {
-      const float4 pj = __ldg(posf + j);
-      const float sx = pi.x + (float)(cxo - (__ldg(cellc + j) & xmask)) * csx;
+    auto test = [&](int j, const float4& pj, int cj) {
+      const float sx = pi.x + (float)(cxo - (cj & xmask)) * csx;
       bool keep;
       if (pj.w > hbig) {
         // big j: kept here only by a big i, within i's own reach (the
         // scatter pass adds it everywhere else)
-        keep = big_i && sym_r2<DIM>(G, pi, ci, pj, __ldg(cellc + j)) < own2;
+        keep = big_i && sym_r2<DIM>(G, pi, ci, pj, cj) < own2;
       } else {
         float dx = sx - pj.x, dy = sy - pj.y, dz = DIM == 3 ? sz - pj.z : 0.f;
         if (mx) dx = dx > 0.5f * Lx ? dx - Lx : (dx < -0.5f * Lx ? dx + Lx : dx);
@@ -427,7 +430,23 @@ __global__ void __launch_bounds__(128) k_build_lists(int n, DevParams P, const G
         if (cnt < cap) row[cnt * 32] = j;
         cnt++;
       }
+    };
+    // kGatherUnroll candidates at a time, every record of a group requested
+    // before the first test (a thread's candidates are a chain of L1/L2 round
+    // trips otherwise)
+    int j = jb;
+    for (; j + kGatherUnroll <= je; j += kGatherUnroll) {
+      float4 pq[kGatherUnroll];
+      int cq[kGatherUnroll];
+#pragma unroll
+      for (int u = 0; u < kGatherUnroll; u++) {
+        pq[u] = __ldg(posf + j + u);
+        cq[u] = __ldg(cellc + j + u);
+      }
+#pragma unroll
+      for (int u = 0; u < kGatherUnroll; u++) test(j + u, pq[u], cq[u]);
     }
+    for (; j < je; j++) test(j, __ldg(posf + j), __ldg(cellc + j));
   });
   const int stored = cnt < cap ? cnt : cap;
   cnt_out[i] = stored;
