@@ -604,7 +604,10 @@ __global__ void __launch_bounds__(128) k_build_lists_big(DevParams P, const Grid
 // appends them in whatever order its atomics resolve) and cap the counts.
 // One warp per particle the scatter pass enrolled: up to 32 appended entries
 // are sorted across the lanes by a bitonic network (one entry per lane,
-// padded with INT_MAX); longer runs, rare, by one lane's insertion sort.
+// padded with INT_MAX), up to 32 kRankRegs by rank (each entry's position is
+// the count of smaller entries), longer runs, rare, by one lane's insertion
+// sort.
+constexpr int kRankRegs = 8;
 __global__ void __launch_bounds__(128) k_sort_appended(int cap, int* __restrict__ idx, int* __restrict__ cnt,
                                                        const int* __restrict__ gcnt,
                                                        const int* __restrict__ app_idx,
@@ -633,6 +636,28 @@ __global__ void __launch_bounds__(128) k_sort_appended(int cap, int* __restrict_
         }
       }
       if (lane < m) row[(size_t)(g + lane) * 32] = v;
+    } else if (m <= 32 * kRankRegs) {
+      // up to 32 kRankRegs entries: each lane holds kRankRegs of them, every
+      // entry's rank is the count of entries before it in (value, position)
+      // order, counted against all entries passed round the warp
+      int v[kRankRegs], rank[kRankRegs];
+#pragma unroll
+      for (int r = 0; r < kRankRegs; r++) {
+        const int e = r * 32 + lane;
+        v[r] = e < m ? row[(size_t)(g + e) * 32] : INT_MAX;
+        rank[r] = 0;
+      }
+      for (int r2 = 0; r2 < kRankRegs && r2 * 32 < m; r2++)
+        for (int src = 0; src < 32; src++) {
+          const int o = __shfl_sync(0xffffffffu, v[r2], src);
+          const int op = r2 * 32 + src;
+#pragma unroll
+          for (int r = 0; r < kRankRegs; r++) rank[r] += (o < v[r] || (o == v[r] && op < r * 32 + lane)) ? 1 : 0;
+        }
+      __syncwarp();
+#pragma unroll
+      for (int r = 0; r < kRankRegs; r++)
+        if (r * 32 + lane < m) row[(size_t)(g + rank[r]) * 32] = v[r];
     } else if (lane == 0) {
       for (int a = g + 1; a < c; a++) {
         const int v = row[(size_t)a * 32];
