@@ -151,3 +151,25 @@ def test_batched_lists_exact_with_a_few_large_h():
         bad = np.nonzero(counts[sl] != ref)[0]
         assert bad.size == 0, f"instance {k}: {bad.size} particles differ"
     eng.close()
+
+
+def test_long_appended_runs_are_ordered_deterministically():
+    # A blob of large-h particles: each smaller particle near it gets dozens
+    # of entries scattered into its list (runs longer than a warp), which the
+    # ordering pass must put in index order whatever order the scatter's
+    # atomics left them in.  The lists hold the exact neighbour sets, and two
+    # warm-ups (three right-hand sides each) from the same state agree bit for
+    # bit.
+    ic, prm = sc_.blast_3d(16, "cubic")
+    r2 = ic["x"] ** 2 + ic["y"] ** 2 + ic["z"] ** 2
+    ic = dict(ic, h=np.where(r2 < 0.18 ** 2, 3.0, 1.0) * ic["h"])
+    outs = []
+    for _ in range(2):
+        eng = _engine(ic, prm)
+        eng.cells_build()
+        _check(eng, prm, "large-h blob")
+        eng.warmup()
+        outs.append(eng.pa.pull("au", "av", "aw", "ae", "aBevolx", "rho", "h", "gid", order="gid"))
+        eng.close()
+    for k in outs[0]:
+        assert np.array_equal(outs[0][k], outs[1][k]), f"{k} differs between two identical runs"
