@@ -157,13 +157,19 @@ int dev_alloc(Ctx* c, T** p, int64_t count) {
   return MHD_OK;
 }
 
-// Persistent fields carried through the neighbour sort.
-int build_gather(const MhdState* src, MhdState* dst, GatherSet& g) {
+// Persistent fields carried through the neighbour sort.  With rhs_follows
+// (the sort of a right-hand side, whose prologue rewrites them before
+// anything reads them: DensityFromSmoothingLength, IdealGasEOS and
+// MagneticStateReconstruction) rho, p, cs and B are not carried.
+int build_gather(const MhdState* src, MhdState* dst, GatherSet& g, bool rhs_follows = false) {
   int k = 0;
-#define MHD_G_(n)          \
-  g.src[k] = src->n;       \
-  g.dst[k] = dst->n;       \
-  k++;
+#define MHD_G_(n)                                                                          \
+  if (!(rhs_follows && (&src->n == &src->rho || &src->n == &src->p || &src->n == &src->cs || \
+                        &src->n == &src->Bx || &src->n == &src->By || &src->n == &src->Bz))) { \
+    g.src[k] = src->n;                                                                     \
+    g.dst[k] = dst->n;                                                                     \
+    k++;                                                                                   \
+  }
   MHD_SORTED_FIELDS(MHD_G_)
 #undef MHD_G_
   g.nf = k;
@@ -313,13 +319,13 @@ int ensure_list_storage(Ctx* c, int cap) {
 
 // Sort src into dst, carry the previous accelerations into au_prev and build
 // the neighbour lists of the sorted particles.
-int sort_into(Ctx* c, const MhdState* src, MhdState* dst, int n, cudaStream_t st) {
+int sort_into(Ctx* c, const MhdState* src, MhdState* dst, int n, cudaStream_t st, bool rhs_follows) {
   {
     TimedScope ts(c, MHD_TIMING_CELLS, st);
     launch_sort_cells(c, src, n, st);
     GatherSet g;
     memset(&g, 0, sizeof g);
-    build_gather(src, dst, g);
+    build_gather(src, dst, g, rhs_follows);
     launch_gather(c, g, n, st);
     GatherSet a;
     memset(&a, 0, sizeof a);
@@ -545,7 +551,7 @@ int capture_density_loop(Ctx* c, MhdState* dst, int n, int first, cudaStream_t s
 int rhs_captured(Ctx* c, const MhdState* src, MhdState* dst, int n, cudaStream_t st) {
   int rc = plan_grid(c, src, n, st);
   if (rc != MHD_OK) return rc;
-  rc = sort_into(c, src, dst, n, st);
+  rc = sort_into(c, src, dst, n, st, true);
   if (rc != MHD_OK) return rc;
   CK(cudaMemsetAsync(&c->d_sc->n_unconverged[0], 0, sizeof(c->d_sc->n_unconverged), st));
   CK(cudaMemsetAsync(&c->d_sc->passes_done, 0, sizeof(int), st));
@@ -577,7 +583,7 @@ int step_fused(Ctx* c, const MhdState* cur, MhdState* nxt, int n, int mode, bool
     rc = rhs_captured(c, cur, nxt, n, st);
   } else {
     rc = plan_grid(c, cur, n, st);
-    if (rc == MHD_OK) rc = sort_into(c, cur, nxt, n, st);
+    if (rc == MHD_OK) rc = sort_into(c, cur, nxt, n, st, true);
     if (rc == MHD_OK) rc = density_iterate(c, nxt, n, nullptr, st);
     if (rc == MHD_OK) rc = force_pass(c, nxt, n, st);
   }
@@ -892,7 +898,7 @@ int mhd_cells_build(void* ctx, const MhdState* src, MhdState* dst, int64_t n, vo
   const cudaStream_t st = S(stream);
   int rc = plan_grid(c, src, (int)n, st);
   if (rc != MHD_OK) return rc;
-  return sort_into(c, src, dst, (int)n, st);
+  return sort_into(c, src, dst, (int)n, st, false);
 }
 
 int mhd_density_iterate(void* ctx, MhdState* s, int64_t n, MhdRhsStats* stats, void* stream) {
