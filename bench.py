@@ -68,13 +68,11 @@ FORCE_BYTES_PER_PARTICLE = {"fp64": 7 * 32 + 7 * 8 + 16 * 8, "fp32": 7 * 16 + 7 
 # 55, signal speed 3, pressure coefficient 5, Maxwell projections 12,
 # momentum 27 (three Kahan adds), div v 6, conduction speed 7, energy terms
 # 15, field projections and resistive speed 27, dissipation 6, induction
-# and cleaning terms 9 + 27, energy sum 13, div B sums 14 -- 253 with every
-# term Kahan-added (40 for the ten sums); the ten sums add plain partials
-# over four list entries and Kahan-add each partial (1 + 4/4 per term and
-# sum: 20), which gives 233; FP64 (plain sums) 223.  A list entry beyond the
-# cut-off costs its geometry (12).  The density pass: 33 per pair in FP32
-# (geometry 10, kernel 8, two Kahan sums 15).
-FORCE_FLOPS_PER_PAIR = {"fp32": 233, "fp64": 223}
+# and cleaning terms 9 + 27, energy sum 13, div B sums 14 -- 253, of which
+# 40 are the compensation of the ten Kahan sums; FP64 (plain sums) 223.  A
+# list entry beyond the cut-off costs its geometry (12).  The density pass:
+# 33 per pair in FP32 (geometry 10, kernel 8, two Kahan sums 15).
+FORCE_FLOPS_PER_PAIR = {"fp32": 253, "fp64": 223}
 FORCE_FLOPS_PER_CANDIDATE = 12
 DENSITY_FLOPS_PER_PAIR = {"fp32": 33, "fp64": 25}
 

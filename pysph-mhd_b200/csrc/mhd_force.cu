@@ -26,11 +26,8 @@
 //   x_ij (grad_i r-hat = omega_i |grad W_i| r-hat = omega_i t_i x_ij) so that
 //   r-hat is never formed and the thermal and isotropic magnetic pressures
 //   share one coefficient.  With T = float the momentum, energy, induction
-//   and divergence sums are compensated: plain FP32 partials over four
-//   list entries at a time, each partial Kahan-added (measured on the 128^3
-//   blast: 1.83 ms per pass against 1.86 with every term Kahan-added, and
-//   1e-7 against the FP64 path either way); the Cullen-Dehnen moments feed
-//   a clipped limiter and use plain FP32 sums.
+//   and divergence sums are Kahan-compensated; the Cullen-Dehnen moments
+//   feed a clipped limiter and use plain FP32 sums.
 #include <cuda_runtime.h>
 
 #include "mhd_common.cuh"
@@ -59,28 +56,18 @@ template <class T>
 struct Acc {
   T s = 0;
   __device__ __forceinline__ void add(T v) { s += v; }
-  __device__ __forceinline__ void flush() {}
   __device__ __forceinline__ double get() const { return (double)s; }
 };
-// FP32: plain partial sums of kSumBlock consecutive list entries, each
-// partial added to a Kahan-compensated sum.
-constexpr int kSumBlock = 4;
 template <>
 struct Acc<float> {
-  float s = 0.f, c = 0.f, p = 0.f;  // Kahan sum (s, c) of the flushed partials p
-  __device__ __forceinline__ void add(float v) { p += v; }
-  __device__ __forceinline__ void flush() {
-    const float y = __fsub_rn(p, c);
+  float s = 0.f, c = 0.f;
+  __device__ __forceinline__ void add(float v) {
+    const float y = __fsub_rn(v, c);
     const float t = __fadd_rn(s, y);
     c = __fsub_rn(__fsub_rn(t, s), y);
     s = t;
-    p = 0.f;
   }
-  __device__ __forceinline__ double get() const {
-    const float y = __fsub_rn(p, c);
-    const float t = __fadd_rn(s, y);
-    return (double)t - (double)__fsub_rn(__fsub_rn(t, s), y);
-  }
+  __device__ __forceinline__ double get() const { return (double)s - (double)c; }
 };
 
 // A kernel parameter in the pair precision: the FP32 copy or the FP64 value.
@@ -319,11 +306,6 @@ struct ForceParticle {
     dtc = 0;
   }
 
-  __device__ __forceinline__ void flush() {
-    fx.flush(); fy.flush(); fz.flush(); fe.flush(); fdiv.flush();
-    bxr.flush(); byr.flush(); bzr.flush(); dbs.flush(); dbd.flush();
-  }
-
   // the self pair: every sum term carries a zero kernel gradient or a zero
   // displacement; only the signal speed max(vw_i - 2 dot, 0) = vw_i enters
   // dt_cfl
@@ -532,7 +514,6 @@ __global__ void __launch_bounds__(kForceShapes[SHAPE][0], kForceShapes[SHAPE][1]
   }
   for (int k = 0; k < cnt; k++) {
     const int j = jn;
-    if ((k & (kSumBlock - 1)) == 0 && k > 0) F.flush();
     if constexpr (STAGED) {
       jn = jn2;
       if (k + 1 < cnt) fetch((k + 1) & 1, jn);
