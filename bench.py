@@ -931,14 +931,20 @@ def run_e2e(args, dev, barrier=lambda: None, dist=False, world=1):
     solver = app.solver
     solver.output_directory = None
     t0, dt0 = solver.t, solver.dt
-    # the run's inputs: the state the steps carry (the fields the neighbour
-    # sort permutes) and the rates of the last right-hand side, which the
-    # first predictor reads; every other property is written before it is
-    # read
-    from src import _abi
-
-    inputs = list(_abi.SORTED_FIELDS) + ["au", "av", "aw", "ae", "ah", "aBevolx", "aBevoly", "aBevolz", "apsi",
-                                         "alphaloc"]
+    # the run's inputs, what it reads before writing: the last right-hand
+    # side's dt_adapt (the first step size is their minimum) and rates, and
+    # what the predictor opening a chunk (initialize + stage1: positions, h,
+    # the evolved fields, alpha1 and c_s of the alpha switch, the particle
+    # type) and the sort of the right-hand side after it (mass and gid
+    # besides) read.  Every other property -- rho, p and B (the prologue's),
+    # the predicted fields, h0, omega, converged, rho_sum -- is written
+    # before it is read.  The timed run starts with the untimed run's end
+    # state in every property it does not push, so its outputs equalling
+    # the untimed run's, bit for bit (checked below), show none of them is
+    # read.
+    inputs = ["x", "y", "z", "h", "m", "gid", "itype", "u", "v", "w", "e", "Bevolx", "Bevoly", "Bevolz", "psi",
+              "alpha1", "cs", "au", "av", "aw", "ae", "ah", "aBevolx", "aBevoly", "aBevolz", "apsi", "alphaloc",
+              "dt_adapt"]
     host = {k: torch.empty(n, dtype=pa.properties[k].dtype, pin_memory=True) for k in inputs}
     for k in inputs:
         host[k].copy_(pa.properties[k])
@@ -963,6 +969,7 @@ def run_e2e(args, dev, barrier=lambda: None, dist=False, world=1):
         torch.cuda.synchronize()
 
     run_once()  # captures the chunk's graph
+    first = {k: v.clone() for k, v in out.items()}
     d2h[0] = 0
     h2d = sum(t.numel() * t.element_size() for t in host.values())
     barrier()
@@ -971,6 +978,9 @@ def run_e2e(args, dev, barrier=lambda: None, dist=False, world=1):
     run_once()
     el = time.perf_counter() - t_start
     steps = solver.count
+    for k in out:
+        if not torch.equal(out[k], first[k]):
+            raise RuntimeError(f"end-to-end run: {k} differs from the untimed run's (an input not pushed)")
     if dist:
         # every rank's replica, timed as the slowest rank
         import torch.distributed as tdist
@@ -983,8 +993,9 @@ def run_e2e(args, dev, barrier=lambda: None, dist=False, world=1):
     return {"value": world * n * steps / el, "unit": UNIT, "h2d_bytes_per_step": world * h2d / steps,
             "d2h_bytes_per_step": world * (d2h[0] + 8 * steps) / steps,
             "path": "MHDApplication (configs/mhdblast3d.toml) -> MHDSolver.solve, fused loop: pinned-host inputs "
-                    "(carried state + last rates) pushed, K steps in captured chunks with device dt, OUTPUT_PROPERTIES pulled at the dump "
-                    "every 20 steps; diagnostic outputs off"}
+                    "(the 28 properties the run reads before writing: state, type, last rates and dt_adapt) pushed, "
+                    "K steps in captured chunks with device dt, OUTPUT_PROPERTIES pulled at the dump every 20 steps "
+                    "(equal, bit for bit, to an untimed run's); diagnostic outputs off"}
 
 
 def main():
